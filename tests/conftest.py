@@ -1,0 +1,26 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def golden(name):
+    """A golden fixture written by the reference (tests/golden/make_golden.py)."""
+    import numpy as np
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = dict(zip([str(k) for k in z["meta_keys"]], [str(v) for v in z["meta_vals"]]))
+    return z, meta
+
+
+GOLDEN_CASES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
