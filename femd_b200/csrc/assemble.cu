@@ -1,0 +1,475 @@
+// assemble.cu -- K3: bilinear-form assembly into CSR values, K4: linear-form assembly into a
+// vector, on affine P_k triangles.
+//
+// Scheme (deterministic, no atomics).  Every matrix position p of row i is owned by one lane of
+// the sub-warp that owns row i.  The lane walks the row's (cell, local) list in increasing cell
+// order (the pattern's rc lists), finds through the scatter map which element entry (l, j) of
+// that cell lands on p, forms that entry and adds it.  Each value is therefore the sum of its
+// element contributions in increasing element order, starting from 0 -- the order of the
+// reference's row-owner scatter (include/femd/forms/assembly_2d.hpp:265-301) -- and is written
+// to HBM exactly once.  The Jacobi inverse diagonal (precond.hpp:82-91) is the epilogue of the
+// lane that owns the diagonal position.
+//
+// Element entries.  Per cell: J = [P1-P0, P2-P0], det J, J^{-1} (lagrange_space_2d.hpp:44-52),
+// w_q = rw_q |det J| (cache_2d.hpp:113-114).  Derivative code m of basis l at point q is
+// row_m(q,l) = R0 (m = 0), Ji0 Rxi + Ji2 Reta (m = 1), Ji1 Rxi + Ji3 Reta (m = 2)
+// (Cache2D::row, cache_2d.hpp:211-226).
+//   EXACT: Ke(l,j) = sum_t sum_q [(w_q c_t) row_a(q,l)] row_b(q,j), zero products skipped, in
+//          the reference's order with no fused multiply-adds (element_matrix_2d, :102-126).
+//   FAST:  constant-coefficient terms are contracted with reference tensors staged in shared
+//          memory, S^{rs}(l,j) = sum_q rw_q R_r(q,l) R_s(q,j) (r, s in value, d/dxi, d/deta):
+//          Ke(l,j) = |det J| sum_t c_t sum_{rs} A_{a_t r} A_{b_t s} S^{rs}(l,j); point
+//          coefficients are contracted point by point.
+// Coefficients given as closed forms or as a field are first evaluated at the points into a
+// scratch array [e nq + q] (the reference's coefficient arrays, assembler_2d.hpp:393-410).
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace femd {
+
+int build_scatter_map(femd_ctx ctx, femd_pattern p);
+
+static constexpr int MAX_TERMS = 8;
+static constexpr int MAX_NLOC = 28;    // P_6
+static constexpr int MAX_NQ = 64;
+
+struct TermSpec {
+    int nterms;
+    int a[MAX_TERMS], b[MAX_TERMS];
+    int is_const[MAX_TERMS];
+    double cval[MAX_TERMS];
+    const double *cpts[MAX_TERMS];
+};
+
+struct Geo {
+    double J0, J1, J2, J3, det;
+};
+
+__device__ __forceinline__ Geo load_geo_exact(const double *__restrict__ pts, const int *__restrict__ tris, int e)
+{
+    const int v0 = tris[3 * e], v1 = tris[3 * e + 1], v2 = tris[3 * e + 2];
+    const double x0 = pts[2 * v0], y0 = pts[2 * v0 + 1];
+    Geo g;
+    g.J0 = __dsub_rn(pts[2 * v1], x0);
+    g.J1 = __dsub_rn(pts[2 * v2], x0);
+    g.J2 = __dsub_rn(pts[2 * v1 + 1], y0);
+    g.J3 = __dsub_rn(pts[2 * v2 + 1], y0);
+    g.det = __dsub_rn(__dmul_rn(g.J0, g.J3), __dmul_rn(g.J1, g.J2));
+    return g;
+}
+
+// ---- coefficient evaluation at the points -------------------------------------------------
+// x = P0.x + J0 xi + J1 eta (lagrange_space_2d.hpp:86-87), no contraction.
+__global__ void k_coef_points(const double *__restrict__ pts, const int *__restrict__ tris, int ne, int nq,
+                              const double *__restrict__ qxi, const double *__restrict__ qeta, int kind, double p0,
+                              double p1, double p2, double p3, const double *__restrict__ field,
+                              const int *__restrict__ dofs, int nloc, const double *__restrict__ ref,
+                              double *__restrict__ out)
+{
+    const long long total = (long long)ne * nq;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int e = (int)(t / nq), q = (int)(t % nq);
+        double v;
+        if (kind == FEMD_COEF_FIELD) {
+            // Cache2D::eval_multi, value code (cache_2d.hpp:262-270): s = sum_l R_l loc_l
+            const double *R = ref + (size_t)q * 3 * nloc;
+            double s = 0.0;
+            for (int l = 0; l < nloc; ++l) {
+                const int d = dofs[(size_t)e * nloc + l];
+                const double c = d >= 0 ? field[d] : 0.0;
+                s = __dadd_rn(s, __dmul_rn(R[l], c));
+            }
+            v = s;
+        } else {
+            const Geo g = load_geo_exact(pts, tris, e);
+            const int v0 = tris[3 * e];
+            const double x = __dadd_rn(__dadd_rn(pts[2 * v0], __dmul_rn(g.J0, qxi[q])), __dmul_rn(g.J1, qeta[q]));
+            const double y = __dadd_rn(__dadd_rn(pts[2 * v0 + 1], __dmul_rn(g.J2, qxi[q])), __dmul_rn(g.J3, qeta[q]));
+            const double s = __dmul_rn(sin(__dmul_rn(p2, x)), sin(__dmul_rn(p3, y)));
+            if (kind == FEMD_COEF_SINSIN) v = __dadd_rn(p0, __dmul_rn(p1, s));
+            else v = __dadd_rn(__dmul_rn(p1, s), s);   // FEMD_COEF_SINSIN_HELM: p1 s + s
+        }
+        out[t] = v;
+    }
+}
+
+// ---- K3 ---------------------------------------------------------------------------------------
+// shared memory: ref tabulation [nq][3][nloc], then (FAST) S tensors [9][nloc][nloc]
+template <int MODE, int G>
+__global__ void __launch_bounds__(256) k_assemble_matrix(
+    const double *__restrict__ pts, const int *__restrict__ tris, const int *__restrict__ indptr,
+    const int *__restrict__ rc_ptr, const int *__restrict__ rc_code, const int *__restrict__ map,
+    const int *__restrict__ diag_pos, int nrows, int nloc, int nq, const double *__restrict__ g_ref,
+    const double *__restrict__ g_rw, const double *__restrict__ g_S, TermSpec ts, double *__restrict__ data,
+    double *__restrict__ inv, int *__restrict__ status)
+{
+    extern __shared__ double smem[];
+    double *sref = smem;                              // nq * 3 * nloc
+    double *srw = sref + nq * 3 * nloc;               // nq
+    double *sS = srw + nq;                            // 9 * nloc * nloc (FAST)
+    const int nref = nq * 3 * nloc;
+    for (int t = threadIdx.x; t < nref; t += blockDim.x) sref[t] = g_ref[t];
+    for (int t = threadIdx.x; t < nq; t += blockDim.x) srw[t] = g_rw[t];
+    if (MODE == FEMD_ASM_FAST)
+        for (int t = threadIdx.x; t < 9 * nloc * nloc; t += blockDim.x) sS[t] = g_S[t];
+    __syncthreads();
+
+    const int lane = threadIdx.x % G;
+    const int groups_per_block = blockDim.x / G;
+    const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+    for (int i = blockIdx.x * groups_per_block + threadIdx.x / G; i < nrows; i += gridDim.x * groups_per_block) {
+        const int rlo = indptr[i], len = indptr[i + 1] - rlo;
+        const int clo = rc_ptr[i], chi = rc_ptr[i + 1];
+        const int dpos = diag_pos ? diag_pos[i] : -1;
+        for (int c0 = 0; c0 < len; c0 += G) {
+            const int p = rlo + c0 + lane;
+            const bool valid = c0 + lane < len;
+            double acc = 0.0;
+            for (int c = clo; c < chi; ++c) {
+                const int code = rc_code[c];
+                const int e = code / nloc, l = code - e * nloc;
+                // the map row of (e, l): lane j < nloc holds the position of entry (l, j)
+                const int mj = lane < nloc ? map[(size_t)code * nloc + lane] : -2;
+                // the three vertices, loaded by lanes 0..2 and shared
+                double vx = 0.0, vy = 0.0;
+                if (lane < 3) {
+                    const int v = tris[3 * e + lane];
+                    vx = pts[2 * v];
+                    vy = pts[2 * v + 1];
+                }
+                const int gbase = (threadIdx.x & 31) / G * G;
+                const double x0 = __shfl_sync(gmask, vx, gbase + 0), y0 = __shfl_sync(gmask, vy, gbase + 0);
+                const double x1 = __shfl_sync(gmask, vx, gbase + 1), y1 = __shfl_sync(gmask, vy, gbase + 1);
+                const double x2 = __shfl_sync(gmask, vx, gbase + 2), y2 = __shfl_sync(gmask, vy, gbase + 2);
+                int myj = -1;
+                for (int j = 0; j < nloc; ++j) {
+                    const int pj = __shfl_sync(gmask, mj, gbase + j);
+                    if (pj == p) myj = j;
+                }
+                if (!valid || myj < 0) continue;
+                const double J0 = __dsub_rn(x1, x0), J1 = __dsub_rn(x2, x0);
+                const double J2 = __dsub_rn(y1, y0), J3 = __dsub_rn(y2, y0);
+                const double d = __dsub_rn(__dmul_rn(J0, J3), __dmul_rn(J1, J2));
+                const double ad = fabs(d);
+                double Ke = 0.0;
+                if (MODE == FEMD_ASM_EXACT) {
+                    const double Ji0 = __ddiv_rn(J3, d), Ji1 = __ddiv_rn(-J1, d);
+                    const double Ji2 = __ddiv_rn(-J2, d), Ji3 = __ddiv_rn(J0, d);
+                    for (int t = 0; t < ts.nterms; ++t) {
+                        const int ma = ts.a[t], mb = ts.b[t];
+                        for (int q = 0; q < nq; ++q) {
+                            const double w = __dmul_rn(srw[q], ad);
+                            const double ct = ts.is_const[t] ? ts.cval[t] : ts.cpts[t][(size_t)e * nq + q];
+                            const double s = __dmul_rn(w, ct);
+                            if (s == 0.0) continue;
+                            const double *R = sref + q * 3 * nloc;
+                            double ra, rb;
+                            if (ma == 0) ra = R[l];
+                            else {
+                                const double aa = ma == 1 ? Ji0 : Ji1, bb = ma == 1 ? Ji2 : Ji3;
+                                ra = __dadd_rn(__dmul_rn(aa, R[nloc + l]), __dmul_rn(bb, R[2 * nloc + l]));
+                            }
+                            const double sa = __dmul_rn(s, ra);
+                            if (sa == 0.0) continue;
+                            if (mb == 0) rb = R[myj];
+                            else {
+                                const double aa = mb == 1 ? Ji0 : Ji1, bb = mb == 1 ? Ji2 : Ji3;
+                                rb = __dadd_rn(__dmul_rn(aa, R[nloc + myj]), __dmul_rn(bb, R[2 * nloc + myj]));
+                            }
+                            Ke = __dadd_rn(Ke, __dmul_rn(sa, rb));
+                        }
+                    }
+                    acc = __dadd_rn(acc, Ke);
+                } else {
+                    const double rd = 1.0 / d;
+                    // A[m][r]: code m of the physical row in terms of reference row r (value, xi, eta)
+                    const double A[3][3] = {{1.0, 0.0, 0.0}, {0.0, J3 * rd, -J2 * rd}, {0.0, -J1 * rd, J0 * rd}};
+                    double G9[9];
+#pragma unroll
+                    for (int r = 0; r < 9; ++r) G9[r] = 0.0;
+                    for (int t = 0; t < ts.nterms; ++t) {
+                        const int ma = ts.a[t], mb = ts.b[t];
+                        if (ts.is_const[t]) {
+                            const double cs = ts.cval[t] * ad;
+#pragma unroll
+                            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                                for (int s = 0; s < 3; ++s) G9[3 * r + s] += cs * A[ma][r] * A[mb][s];
+                        } else {
+                            const double *cp = ts.cpts[t] + (size_t)e * nq;
+                            for (int q = 0; q < nq; ++q) {
+                                const double *R = sref + q * 3 * nloc;
+                                const double ra = A[ma][0] * R[l] + A[ma][1] * R[nloc + l] + A[ma][2] * R[2 * nloc + l];
+                                const double rb = A[mb][0] * R[myj] + A[mb][1] * R[nloc + myj] + A[mb][2] * R[2 * nloc + myj];
+                                Ke += (srw[q] * ad * cp[q]) * ra * rb;
+                            }
+                        }
+                    }
+                    const int lj = l * nloc + myj;
+#pragma unroll
+                    for (int r = 0; r < 9; ++r)
+                        if (G9[r] != 0.0) Ke += G9[r] * sS[r * nloc * nloc + lj];
+                    acc += Ke;
+                }
+            }
+            if (valid) {
+                data[p] = acc;
+                if (inv && p == dpos) {
+                    if (acc == 0.0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
+                    inv[i] = 1.0 / acc;
+                }
+            }
+        }
+        if (inv && lane == 0 && dpos < 0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
+    }
+}
+
+// ---- K4 ---------------------------------------------------------------------------------------
+// One thread per row; f_i = sum over the row's cells (increasing order) of fe(l), with
+// fe(l) = sum_t sum_q (w_q c_t) row_a(q, l) (assemble_vector_2d, assembly_2d.hpp:188-207).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_assemble_vector(
+    const double *__restrict__ pts, const int *__restrict__ tris, const int *__restrict__ rc_ptr,
+    const int *__restrict__ rc_code, int nrows, int nloc, int nq, const double *__restrict__ g_ref,
+    const double *__restrict__ g_rw, TermSpec ts, double *__restrict__ f)
+{
+    extern __shared__ double smem[];
+    double *sref = smem;
+    double *srw = sref + nq * 3 * nloc;
+    for (int t = threadIdx.x; t < nq * 3 * nloc; t += blockDim.x) sref[t] = g_ref[t];
+    for (int t = threadIdx.x; t < nq; t += blockDim.x) srw[t] = g_rw[t];
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x) {
+        double fi = 0.0;
+        for (int c = rc_ptr[i]; c < rc_ptr[i + 1]; ++c) {
+            const int code = rc_code[c];
+            const int e = code / nloc, l = code - e * nloc;
+            const Geo g = load_geo_exact(pts, tris, e);
+            const double ad = fabs(g.det);
+            double Ji0 = 0.0, Ji1 = 0.0, Ji2 = 0.0, Ji3 = 0.0;
+            bool need = false;
+            for (int t = 0; t < ts.nterms; ++t) need |= ts.a[t] != 0;
+            if (need) {
+                Ji0 = __ddiv_rn(g.J3, g.det); Ji1 = __ddiv_rn(-g.J1, g.det);
+                Ji2 = __ddiv_rn(-g.J2, g.det); Ji3 = __ddiv_rn(g.J0, g.det);
+            }
+            double fe = 0.0;
+            for (int t = 0; t < ts.nterms; ++t) {
+                const int ma = ts.a[t];
+                for (int q = 0; q < nq; ++q) {
+                    const double w = __dmul_rn(srw[q], ad);
+                    const double ct = ts.is_const[t] ? ts.cval[t] : ts.cpts[t][(size_t)e * nq + q];
+                    const double s = __dmul_rn(w, ct);
+                    if (s == 0.0) continue;
+                    const double *R = sref + q * 3 * nloc;
+                    double r;
+                    if (ma == 0) r = R[l];
+                    else {
+                        const double aa = ma == 1 ? Ji0 : Ji1, bb = ma == 1 ? Ji2 : Ji3;
+                        r = __dadd_rn(__dmul_rn(aa, R[nloc + l]), __dmul_rn(bb, R[2 * nloc + l]));
+                    }
+                    fe = __dadd_rn(fe, __dmul_rn(s, r));
+                }
+            }
+            fi = __dadd_rn(fi, fe);
+        }
+        f[i] = fi;
+    }
+}
+
+// ---- host side -----------------------------------------------------------------------------
+struct RuleDev {
+    DevBuf<double> ref, rw, S, xi, eta;
+};
+
+static int check_common(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p, int nterms,
+                        const int *a, const int *b, const femd_coef *coef, int mode)
+{
+    FEMD_CHECK_ARG(ctx && mesh && rule && p && a && coef, "assembly: NULL argument");
+    FEMD_CHECK_ARG(p->kind == KIND_PATTERN, "assembly: not a pattern handle");
+    FEMD_CHECK_ARG(p->cell_dofs.p != nullptr, "assembly: the pattern was not built from cells (cell_pattern)");
+    FEMD_CHECK_ARG(mode == FEMD_ASM_FAST || mode == FEMD_ASM_EXACT, "assembly: mode is FEMD_ASM_FAST or FEMD_ASM_EXACT");
+    FEMD_CHECK_ARG(nterms >= 1 && nterms <= MAX_TERMS, "assembly: 1..8 terms");
+    FEMD_CHECK_ARG(mesh->ncells == p->ncells, "assembly: the mesh and the pattern have different cell counts");
+    FEMD_CHECK_ARG(mesh->ncells == 0 || (mesh->points_dev && mesh->tris_dev), "assembly: mesh arrays are NULL");
+    FEMD_CHECK_ARG(rule->nloc == p->nloc && rule->nloc <= MAX_NLOC, "assembly: the rule's nloc differs from the pattern's");
+    FEMD_CHECK_ARG(rule->nq >= 1 && rule->nq <= MAX_NQ, "assembly: 1..64 quadrature points");
+    FEMD_CHECK_ARG(rule->ref_host && rule->w_host && rule->xi_host && rule->eta_host, "assembly: rule arrays are NULL");
+    for (int t = 0; t < nterms; ++t) {
+        FEMD_CHECK_ARG(a[t] >= 0 && a[t] <= 2, "assembly_2d: derivative code " + std::to_string(a[t]) + " is not in 0..2");
+        if (b) FEMD_CHECK_ARG(b[t] >= 0 && b[t] <= 2, "assembly_2d: derivative code " + std::to_string(b[t]) + " is not in 0..2");
+        const int k = coef[t].kind;
+        FEMD_CHECK_ARG(k >= FEMD_COEF_CONST && k <= FEMD_COEF_FIELD, "assembly: unknown coefficient kind");
+        if (k == FEMD_COEF_POINTS) FEMD_CHECK_ARG(coef[t].points_dev, "assembly: coefficient points array is NULL");
+        if (k == FEMD_COEF_FIELD) FEMD_CHECK_ARG(coef[t].field_dev, "assembly: coefficient field array is NULL");
+    }
+    return FEMD_OK;
+}
+
+// Upload the rule; in FAST mode also the reference tensors S^{rs}.
+static int upload_rule(const femd_rule *rule, bool want_S, RuleDev &R, cudaStream_t s)
+{
+    const int nq = rule->nq, nl = rule->nloc;
+    FEMD_TRY(R.ref.alloc((size_t)nq * 3 * nl));
+    FEMD_TRY(R.rw.alloc(nq));
+    FEMD_TRY(R.xi.alloc(nq));
+    FEMD_TRY(R.eta.alloc(nq));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(R.ref.p, rule->ref_host, (size_t)nq * 3 * nl * sizeof(double), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(R.rw.p, rule->w_host, nq * sizeof(double), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(R.xi.p, rule->xi_host, nq * sizeof(double), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(R.eta.p, rule->eta_host, nq * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (want_S) {
+        std::vector<double> S((size_t)9 * nl * nl, 0.0);
+        for (int r = 0; r < 3; ++r)
+            for (int sidx = 0; sidx < 3; ++sidx)
+                for (int l = 0; l < nl; ++l)
+                    for (int j = 0; j < nl; ++j) {
+                        double acc = 0.0;
+                        for (int q = 0; q < nq; ++q) {
+                            const double *Rq = rule->ref_host + (size_t)q * 3 * nl;
+                            acc += rule->w_host[q] * Rq[r * nl + l] * Rq[sidx * nl + j];
+                        }
+                        S[((size_t)(3 * r + sidx) * nl + l) * nl + j] = acc;
+                    }
+        FEMD_TRY(R.S.alloc(S.size()));
+        FEMD_TRY_CUDA(cudaMemcpyAsync(R.S.p, S.data(), S.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // S is a stack vector
+    }
+    return FEMD_OK;
+}
+
+// Evaluate closed-form and field coefficients into scratch arrays; fill the TermSpec.
+static int prepare_terms(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p, int nterms,
+                         const int *a, const int *b, const femd_coef *coef, const RuleDev &R, DevBuf<double> &scratch,
+                         TermSpec &ts)
+{
+    ts.nterms = nterms;
+    const size_t np = (size_t)mesh->ncells * rule->nq;
+    int nscratch = 0;
+    int owner[MAX_TERMS];
+    for (int t = 0; t < nterms; ++t) {
+        owner[t] = -1;
+        if (coef[t].kind >= FEMD_COEF_SINSIN) {
+            for (int u = 0; u < t; ++u)   // the same coefficient as an earlier term: share its array
+                if (coef[u].kind == coef[t].kind && coef[u].field_dev == coef[t].field_dev && coef[u].p[0] == coef[t].p[0] &&
+                    coef[u].p[1] == coef[t].p[1] && coef[u].p[2] == coef[t].p[2] && coef[u].p[3] == coef[t].p[3]) {
+                    owner[t] = owner[u];
+                    break;
+                }
+            if (owner[t] < 0) owner[t] = nscratch++;
+        }
+    }
+    if (nscratch) FEMD_TRY(scratch.alloc(np * nscratch));
+    bool done[MAX_TERMS] = {};
+    for (int t = 0; t < nterms; ++t) {
+        ts.a[t] = a[t];
+        ts.b[t] = b ? b[t] : 0;
+        ts.is_const[t] = coef[t].kind == FEMD_COEF_CONST;
+        ts.cval[t] = coef[t].value;
+        ts.cpts[t] = coef[t].kind == FEMD_COEF_POINTS ? coef[t].points_dev : nullptr;
+        if (owner[t] >= 0) {
+            double *dst = scratch.p + np * owner[t];
+            ts.cpts[t] = dst;
+            if (!done[owner[t]] && np) {
+                done[owner[t]] = true;
+                k_coef_points<<<grid_for(np, 256, 1u << 20), 256, 0, counted(ctx->stream)>>>(
+                    mesh->points_dev, mesh->tris_dev, mesh->ncells, rule->nq, R.xi.p, R.eta.p, coef[t].kind, coef[t].p[0],
+                    coef[t].p[1], coef[t].p[2], coef[t].p[3], coef[t].field_dev, p->cell_dofs.p, rule->nloc, R.ref.p, dst);
+                FEMD_TRY_CUDA(cudaGetLastError());
+            }
+        }
+    }
+    return FEMD_OK;
+}
+
+}  // namespace femd
+
+using namespace femd;
+
+extern "C" {
+
+int femd_cuda_assemble_matrix(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p, int nterms,
+                              const int *a, const int *b, const femd_coef *coef, int mode, femd_matrix K, int want_inv)
+{
+    clear_error();
+    FEMD_TRY(check_common(ctx, mesh, rule, p, nterms, a, b, coef, mode));
+    FEMD_CHECK_ARG(b != nullptr, "assemble_matrix_2d: b is NULL");
+    FEMD_CHECK_ARG(K && K->kind == KIND_MATRIX && K->pattern == p, "assemble_matrix_2d: K is not a matrix on this pattern");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    FEMD_TRY(build_scatter_map(ctx, p));
+    RuleDev R;
+    FEMD_TRY(upload_rule(rule, mode == FEMD_ASM_FAST, R, s));
+    DevBuf<double> scratch;
+    TermSpec ts;
+    FEMD_TRY(prepare_terms(ctx, mesh, rule, p, nterms, a, b, coef, R, scratch, ts));
+    FEMD_TRY(reset_status(ctx));
+    const int nl = rule->nloc, nq = rule->nq;
+    size_t shm = ((size_t)nq * 3 * nl + nq + (mode == FEMD_ASM_FAST ? 9 * nl * nl : 0)) * sizeof(double);
+    const int n = p->nrows;
+    if (n > 0) {
+        double *inv = nullptr;
+        if (want_inv) {
+            if (!K->inv.p) FEMD_TRY(K->inv.alloc((size_t)n));
+            inv = K->inv.p;
+        }
+        const bool wide = p->max_row_len > 16 || nl > 16;
+        const int G = wide ? 32 : 16;
+        const unsigned grid = grid_for((size_t)n, 256 / G, 1u << 22);
+#define FEMD_LAUNCH_ASM(M, GG)                                                                                        \
+    do {                                                                                                             \
+        cudaFuncSetAttribute(k_assemble_matrix<M, GG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);        \
+        k_assemble_matrix<M, GG><<<grid, 256, shm, counted(s)>>>(mesh->points_dev, mesh->tris_dev, p->indptr.p, p->rc_ptr.p,    \
+                                                        p->rc_code.p, p->map.p, p->diag_pos.p, n, nl, nq, R.ref.p,      \
+                                                        R.rw.p, R.S.p, ts, K->data.p, inv, ctx->status_dev);           \
+    } while (0)
+        if (mode == FEMD_ASM_EXACT) { if (wide) FEMD_LAUNCH_ASM(FEMD_ASM_EXACT, 32); else FEMD_LAUNCH_ASM(FEMD_ASM_EXACT, 16); }
+        else { if (wide) FEMD_LAUNCH_ASM(FEMD_ASM_FAST, 32); else FEMD_LAUNCH_ASM(FEMD_ASM_FAST, 16); }
+#undef FEMD_LAUNCH_ASM
+        FEMD_TRY_CUDA(cudaGetLastError());
+    }
+    K->f32_valid = false;
+    int flags = 0, bad = 0;
+    FEMD_TRY(read_status(ctx, &flags, &bad));   // also keeps R and scratch alive until the kernels finish
+    if (want_inv && (flags & ST_ZERODIAG)) {
+        set_error("Jacobi: zero diagonal entry in row " + std::to_string(bad));
+        return FEMD_EZERODIAG;
+    }
+    return FEMD_OK;
+}
+
+int femd_cuda_assemble_vector(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p, int nterms,
+                              const int *a, const femd_coef *coef, int mode, double *f_dev)
+{
+    clear_error();
+    FEMD_TRY(check_common(ctx, mesh, rule, p, nterms, a, nullptr, coef, mode));
+    FEMD_CHECK_ARG(p->nrows == 0 || f_dev, "assemble_vector_2d: f is NULL");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    RuleDev R;
+    FEMD_TRY(upload_rule(rule, false, R, s));
+    DevBuf<double> scratch;
+    TermSpec ts;
+    FEMD_TRY(prepare_terms(ctx, mesh, rule, p, nterms, a, nullptr, coef, R, scratch, ts));
+    const int nl = rule->nloc, nq = rule->nq, n = p->nrows;
+    const size_t shm = ((size_t)nq * 3 * nl + nq) * sizeof(double);
+    if (n > 0) {
+        if (mode == FEMD_ASM_EXACT) {
+            cudaFuncSetAttribute(k_assemble_vector<FEMD_ASM_EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            k_assemble_vector<FEMD_ASM_EXACT><<<grid_for((size_t)n, 256, 1u << 22), 256, shm, counted(s)>>>(
+                mesh->points_dev, mesh->tris_dev, p->rc_ptr.p, p->rc_code.p, n, nl, nq, R.ref.p, R.rw.p, ts, f_dev);
+        } else {
+            cudaFuncSetAttribute(k_assemble_vector<FEMD_ASM_FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            k_assemble_vector<FEMD_ASM_FAST><<<grid_for((size_t)n, 256, 1u << 22), 256, shm, counted(s)>>>(
+                mesh->points_dev, mesh->tris_dev, p->rc_ptr.p, p->rc_code.p, n, nl, nq, R.ref.p, R.rw.p, ts, f_dev);
+        }
+        FEMD_TRY_CUDA(cudaGetLastError());
+    }
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // R and scratch are released on return
+    return FEMD_OK;
+}
+
+}  // extern "C"

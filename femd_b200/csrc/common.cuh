@@ -1,0 +1,160 @@
+// common.cuh -- shared definitions of libfemd_cuda: handles, error handling, scans,
+// warp reductions.  Internal header (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/femd_cuda.h"
+
+namespace femd {
+
+// ---- errors -------------------------------------------------------------------------------
+void set_error(const std::string &msg);
+void clear_error();
+
+#define FEMD_TRY_CUDA(expr)                                                                      \
+    do {                                                                                         \
+        cudaError_t e_ = (expr);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            ::femd::set_error(std::string(#expr) + ": " + cudaGetErrorString(e_));               \
+            return e_ == cudaErrorMemoryAllocation ? FEMD_ENOMEM : FEMD_ECUDA;                   \
+        }                                                                                        \
+    } while (0)
+
+#define FEMD_CHECK_ARG(cond, msg)                                                                \
+    do {                                                                                         \
+        if (!(cond)) { ::femd::set_error(msg); return FEMD_EINVAL; }                             \
+    } while (0)
+
+#define FEMD_TRY(expr)                                                                           \
+    do {                                                                                         \
+        int s_ = (expr);                                                                         \
+        if (s_ != FEMD_OK) return s_;                                                            \
+    } while (0)
+
+// ---- handles ------------------------------------------------------------------------------
+enum HandleKind : uint32_t { KIND_PATTERN = 0x50415454u, KIND_MATRIX = 0x4d415452u, KIND_SOLVER = 0x534f4c56u,
+                             KIND_BATCH = 0x42415443u };
+
+struct HandleBase {
+    uint32_t kind;
+    explicit HandleBase(uint32_t k) : kind(k) {}
+    virtual ~HandleBase() {}
+};
+
+// A device buffer owned by a handle.
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    int alloc(size_t count)
+    {
+        release();
+        if (count == 0) return FEMD_OK;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            set_error(std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " + cudaGetErrorString(e));
+            return e == cudaErrorMemoryAllocation ? FEMD_ENOMEM : FEMD_ECUDA;
+        }
+        n = count;
+        return FEMD_OK;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+};
+
+struct Workspace;
+
+}  // namespace femd
+
+struct femd_ctx_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    // a small device status block: [0] error flags, [1] first bad row, [2..] spare
+    int *status_dev = nullptr;
+    int *status_host = nullptr;   // pinned
+};
+
+struct femd_pattern_s : femd::HandleBase {
+    femd_ctx ctx = nullptr;
+    int nrows = 0, ncols = 0, ncells = 0, nloc = 0;
+    long long nnz = 0;
+    femd::DevBuf<int> indptr, indices;
+    femd::DevBuf<int> cell_dofs;       // ncells x nloc (copy)
+    femd::DevBuf<int> rc_ptr, rc_code; // row -> (cell nloc + local), increasing cell order
+    femd::DevBuf<int> map;             // scatter map, ne nloc^2 (built on demand)
+    femd::DevBuf<int> diag_pos;        // position of (i, i), -1 when absent
+    int max_row_cells = 0, max_row_len = 0;
+    femd_pattern_s() : HandleBase(femd::KIND_PATTERN) {}
+};
+
+struct femd_matrix_s : femd::HandleBase {
+    femd_ctx ctx = nullptr;
+    femd_pattern pattern = nullptr;
+    femd::DevBuf<double> data, inv;
+    femd::DevBuf<float> data32, inv32;   // FP32 copies (mixed precision), built on demand
+    bool f32_valid = false;
+    int spmv_tpr = 0;                    // autotuned threads per row (0: not tuned)
+    femd_matrix_s() : HandleBase(femd::KIND_MATRIX) {}
+};
+
+namespace femd {
+
+// ---- small device helpers -----------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// exclusive scan of n ints in place on the stream; n+1 entries are written when total is
+// requested (out[n] = total).  Uses tmp (device) of scan_tmp_size(n) ints.
+size_t scan_tmp_ints(size_t n);
+int exclusive_scan_int(const int *in, int *out, size_t n, int *tmp, cudaStream_t s);
+
+// Kernel launches issued by this library in this process (graph launches count their nodes).
+void add_launches(long long n);
+// The launch-configuration stream argument of every kernel launch goes through counted(): it
+// counts the launch (unless the stream is being captured into a graph) and returns the stream.
+inline cudaStream_t counted(cudaStream_t s)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    if (cs == cudaStreamCaptureStatusNone) add_launches(1);
+    return s;
+}
+// Launch an instantiated graph and count its kernel nodes.
+inline cudaError_t launch_graph(cudaGraphExec_t exec, size_t nodes, cudaStream_t s)
+{
+    const cudaError_t e = cudaGraphLaunch(exec, s);
+    if (e == cudaSuccess) add_launches((long long)nodes);
+    return e;
+}
+
+inline unsigned grid_for(size_t work, unsigned block, unsigned cap = 1u << 30)
+{
+    size_t g = (work + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+// status flags written by kernels into ctx->status_dev[0]
+enum StatusFlag : int { ST_OUTSIDE = 1, ST_ZERODIAG = 2, ST_ROW_TOO_LONG = 4, ST_TIMEOUT = 8, ST_ABORT = 16 };
+
+int read_status(femd_ctx ctx, int *flags, int *bad_row);
+int reset_status(femd_ctx ctx);
+
+}  // namespace femd

@@ -1,0 +1,927 @@
+// krylov.cu -- K5: CSR SpMV (sub-warp per row) fused with p^T A p; K6: the fused Jacobi-PCG
+// update (x += a p, r -= a Ap, ||r||^2 and r^T D^-1 r in one pass) and direction update; the
+// whole CG loop runs on the device with no host round trip per iteration.
+//
+// Reference: krylov::cg_jacobi (include/femd/krylov/cg.hpp:296-350), cg_update_chunk_jacobi
+// (:99-171), detail_cg::finish (:222-237), CSRMatrix::apply (include/femd/sparse/csr.hpp:203-215).
+//
+// Reductions.  Every kernel that produces a dot product writes one partial per block; the
+// last block to finish (an atomic ticket, no waiting) adds the partials in block order and
+// updates the scalar state (alpha, beta, the stopping test).  The grid of each kernel depends
+// only on n, so the sums -- and the iterates -- have the same bits on every run.  Kernels of an
+// iteration that starts after the stopping test has fired return at once, so whole chunks of
+// iterations are queued (captured in a CUDA graph) and the host only polls between chunks.
+//
+// HBM bytes per FP64 iteration (n rows, nnz entries): SpMV 12 nnz + 4 (n+1) + 8 n (p) + 8 n (Ap);
+// update 40 n read + 16 n written; direction 24 n read + 8 n written.
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace femd {
+
+static constexpr int RED_BLOCK = 256;
+
+template <class T>
+struct CGState {
+    T rz, pAp, alpha, beta, rr;
+    double nb, tol_nb, rn, res64;          // FP64 scalars (norms of b and of the true residual)
+    double maxr;                           // mixed precision: largest ||r|| since the last reliable update
+    T rz_prev;                             // mixed precision: r.z before the last recurrence step
+    int it, done, breakdown, max_iter;
+    int want_ru, ru_count;
+    unsigned ticket;
+};
+
+// block reduction of NV values per thread into smem[v][0]; deterministic (fixed tree)
+template <class T, int NV>
+__device__ __forceinline__ void block_reduce(T (&v)[NV], T *sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        T x = warp_sum(v[k]);
+        if (lane == 0) sh[k * 32 + w] = x;
+    }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            T x = lane < nw ? sh[k * 32 + lane] : T(0);
+            x = warp_sum(x);
+            v[k] = x;
+        }
+    }
+}
+
+// Last-block ticket: returns true in the last block (all threads); partials visible to it.
+__device__ __forceinline__ bool last_block(unsigned *ticket)
+{
+    __shared__ bool amlast;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(ticket, 1u);
+        amlast = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    return amlast;
+}
+
+// Sum of NV partial arrays (each gridDim.x long, stride ld) in a fixed order by one block.
+template <class T, int NV>
+__device__ __forceinline__ void reduce_partials(const T *part, int np, int ld, T (&out)[NV], T *sh)
+{
+    T v[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = T(0);
+    for (int b = threadIdx.x; b < np; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] += ((volatile const T *)part)[k * ld + b];
+    block_reduce<T, NV>(v, sh);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = v[k];
+}
+
+// ---- SpMV: y = A x, TPR lanes per row; DOT adds x_i y_i into the block partial ------------
+template <class V, class T, int TPR, bool DOT>
+__global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indptr, const int *__restrict__ indices,
+                                                    const V *__restrict__ vals, const T *__restrict__ x,
+                                                    T *__restrict__ y, int n, T *__restrict__ part,
+                                                    CGState<T> *__restrict__ st)
+{
+    __shared__ T sh[32];
+    if (DOT && st->done) return;
+    const int lane = threadIdx.x % TPR;
+    constexpr int GPW = 32 / TPR;   // rows per warp per step
+    const int gwarp = (blockIdx.x * RED_BLOCK + threadIdx.x) >> 5, nwarp = (gridDim.x * RED_BLOCK) >> 5;
+    T dot = T(0);
+    // the loop bound is uniform across the warp, so the full-warp shuffles below are safe
+    for (int i0 = gwarp * GPW; i0 < n; i0 += nwarp * GPW) {
+        const int i = i0 + (threadIdx.x & 31) / TPR;
+        T s = T(0);
+        if (i < n) {
+            const int lo = indptr[i], hi = indptr[i + 1];
+            for (int q = lo + lane; q < hi; q += TPR) s += (T)vals[q] * __ldg(&x[indices[q]]);
+        }
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
+        if (lane == 0 && i < n) {
+            y[i] = s;
+            if (DOT) dot += x[i] * s;
+        }
+    }
+    if (!DOT) return;
+    T v[1] = {dot};
+    block_reduce<T, 1>(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    if (!last_block(&st->ticket)) return;
+    T tot[1];
+    reduce_partials<T, 1>(part, gridDim.x, 0, tot, sh);
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        const T pAp = tot[0];
+        st->pAp = pAp;
+        if (!(pAp > T(0))) { st->breakdown = 1; st->done = 1; }
+        else st->alpha = st->rz / pAp;
+    }
+}
+
+// ---- fused update: x += a p; r -= a Ap; rr = r.r; rz = r.(inv r) ------------------------------
+// JAC: with the Jacobi inverse diagonal; otherwise rz = rr (cg.hpp:330-331).
+template <class T, bool JAC>
+__global__ void __launch_bounds__(RED_BLOCK) k_cg_update(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p,
+                                                         const T *__restrict__ Ap, const T *__restrict__ inv, int n,
+                                                         T *__restrict__ part, CGState<T> *__restrict__ st,
+                                                         int mixed)
+{
+    __shared__ T sh[64];
+    if (st->done) return;
+    const T a = st->alpha;
+    T rr = T(0), rz = T(0);
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
+        const T ri = r[i] - a * Ap[i];
+        r[i] = ri;
+        x[i] = x[i] + a * p[i];
+        const T t = ri * ri;
+        rr += t;
+        if (JAC) rz += t * inv[i];
+    }
+    T v[2] = {rr, rz};
+    block_reduce<T, 2>(v, sh);
+    if (threadIdx.x == 0) { part[blockIdx.x] = v[0]; part[gridDim.x + blockIdx.x] = v[1]; }
+    if (!last_block(&st->ticket)) return;
+    T tot[2];
+    reduce_partials<T, 2>(part, gridDim.x, gridDim.x, tot, sh);
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        const T rrn = tot[0], rzn = JAC ? tot[1] : tot[0];
+        st->rr = rrn;
+        st->it += 1;
+        const double rn = sqrt((double)rrn);
+        st->rn = rn;
+        if (!mixed) {
+            if (rn <= st->tol_nb) { st->done = 1; return; }            // cg.hpp:334
+            if (st->it >= st->max_iter) { st->done = 1; return; }      // loop condition
+            st->beta = rzn / st->rz;                                   // cg.hpp:335-336
+            st->rz = rzn;
+            if (!(rzn > T(0))) { st->breakdown = 1; st->done = 1; }    // cg.hpp:324 at the next loop top
+        } else {
+            // mixed precision: ask for a reliable update when the recurrence residual has
+            // dropped by a decade since the last one, or looks converged
+            if (rn <= 0.1 * st->maxr || rn <= st->tol_nb || st->it >= st->max_iter) st->want_ru = 1;
+            st->rz_prev = st->rz;
+            st->beta = rzn / st->rz;
+            st->rz = rzn;
+            if (!(rzn > T(0))) st->want_ru = 1;
+        }
+    }
+}
+
+// ---- direction: p = inv r + beta p (or r + beta p) ------------------------------------------
+template <class T, bool JAC>
+__global__ void __launch_bounds__(RED_BLOCK) k_cg_direction(T *__restrict__ p, const T *__restrict__ r,
+                                                            const T *__restrict__ inv, int n,
+                                                            const CGState<T> *__restrict__ st)
+{
+    if (st->done) return;
+    const T b = st->beta;
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK)
+        p[i] = (JAC ? inv[i] * r[i] : r[i]) + b * p[i];
+}
+
+// ---- start: r = b - Ax; p = inv r; nb, ||r||, rz ------------------------------------------
+template <bool JAC>
+__global__ void __launch_bounds__(RED_BLOCK) k_cg_start(const double *__restrict__ b, const double *__restrict__ Ax,
+                                                        double *__restrict__ r, double *__restrict__ p,
+                                                        const double *__restrict__ inv, int n, double *__restrict__ part,
+                                                        CGState<double> *__restrict__ st, double tol)
+{
+    __shared__ double sh[96];
+    double bb = 0.0, rr = 0.0, rz = 0.0;
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
+        const double bi = b[i], ri = bi - Ax[i];
+        const double zi = JAC ? inv[i] * ri : ri;
+        r[i] = ri;
+        p[i] = zi;
+        bb += bi * bi;
+        rr += ri * ri;
+        rz += ri * zi;
+    }
+    double v[3] = {bb, rr, rz};
+    block_reduce<double, 3>(v, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = v[0];
+        part[gridDim.x + blockIdx.x] = v[1];
+        part[2 * gridDim.x + blockIdx.x] = v[2];
+    }
+    if (!last_block(&st->ticket)) return;
+    double tot[3];
+    reduce_partials<double, 3>(part, gridDim.x, gridDim.x, tot, sh);
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        const double nb = sqrt(tot[0]), rn = sqrt(tot[1]);
+        st->nb = nb;
+        st->tol_nb = tol * nb;
+        st->rn = rn;
+        st->maxr = rn;
+        st->rz = tot[2];
+        st->rr = tot[1];
+        st->it = 0;
+        st->breakdown = 0;
+        st->done = 0;
+        if (nb == 0.0) { st->done = 1; return; }                        // cg.hpp:306
+        if (rn <= tol * nb) { st->done = 1; return; }                   // cg.hpp:312
+        if (!(tot[2] > 0.0)) { st->breakdown = 1; st->done = 1; }       // cg.hpp:324
+    }
+}
+
+// ---- finish: r = b - Ax, ||r|| (cg.hpp:222-237) ---------------------------------------------
+__global__ void __launch_bounds__(RED_BLOCK) k_cg_finish(const double *__restrict__ b, const double *__restrict__ Ax,
+                                                         double *__restrict__ r, int n, double *__restrict__ part,
+                                                         CGState<double> *__restrict__ st)
+{
+    __shared__ double sh[32];
+    double rr = 0.0;
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
+        const double ri = b[i] - Ax[i];
+        r[i] = ri;
+        rr += ri * ri;
+    }
+    double v[1] = {rr};
+    block_reduce<double, 1>(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    if (!last_block(&st->ticket)) return;
+    double tot[1];
+    reduce_partials<double, 1>(part, gridDim.x, 0, tot, sh);
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        st->res64 = sqrt(tot[0]);
+    }
+}
+
+// ---- mixed precision kernels -----------------------------------------------------------------
+// x64 += d32; d32 = 0 (reliable update of the solution), when st32->want_ru
+__global__ void k_mixed_flush(double *__restrict__ x, float *__restrict__ d, int n, const CGState<float> *__restrict__ st)
+{
+    if (st->done || !st->want_ru) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] += (double)d[i];
+        d[i] = 0.0f;
+    }
+}
+
+// y = A64 x when st32->want_ru (the FP64 residual of the reliable update)
+template <int TPR>
+__global__ void __launch_bounds__(RED_BLOCK) k_mixed_spmv64(const int *__restrict__ indptr, const int *__restrict__ indices,
+                                                            const double *__restrict__ vals, const double *__restrict__ x,
+                                                            double *__restrict__ y, int n, const CGState<float> *__restrict__ st)
+{
+    if (st->done || !st->want_ru) return;
+    const int lane = threadIdx.x % TPR;
+    constexpr int GPW = 32 / TPR;
+    const int gwarp = (blockIdx.x * RED_BLOCK + threadIdx.x) >> 5, nwarp = (gridDim.x * RED_BLOCK) >> 5;
+    for (int i0 = gwarp * GPW; i0 < n; i0 += nwarp * GPW) {
+        const int i = i0 + (threadIdx.x & 31) / TPR;
+        double s = 0.0;
+        if (i < n)
+            for (int q = indptr[i] + lane; q < indptr[i + 1]; q += TPR) s += vals[q] * __ldg(&x[indices[q]]);
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
+        if (lane == 0 && i < n) y[i] = s;
+    }
+}
+
+// r64 = b - A x; r32 = r64; ||r64||^2, r32.(inv32 r32); then the convergence test on the FP64
+// residual and the restart of the recurrence from it.
+__global__ void __launch_bounds__(RED_BLOCK) k_mixed_residual(const double *__restrict__ b, const double *__restrict__ Ax,
+                                                              float *__restrict__ r32, const float *__restrict__ inv32, int n,
+                                                              double *__restrict__ part64, float *__restrict__ part32,
+                                                              CGState<float> *__restrict__ st)
+{
+    __shared__ double sh64[32];
+    __shared__ float sh32[32];
+    if (st->done || !st->want_ru) return;
+    double rr = 0.0;
+    float rz = 0.0f;
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
+        const double ri = b[i] - Ax[i];
+        const float rf = (float)ri;
+        r32[i] = rf;
+        rr += ri * ri;
+        rz += rf * rf * inv32[i];
+    }
+    double v[1] = {rr};
+    block_reduce<double, 1>(v, sh64);
+    float w[1] = {rz};
+    __syncthreads();
+    block_reduce<float, 1>(w, sh32);
+    if (threadIdx.x == 0) { part64[blockIdx.x] = v[0]; part32[blockIdx.x] = w[0]; }
+    if (!last_block(&st->ticket)) return;
+    double t64[1];
+    float t32[1];
+    reduce_partials<double, 1>(part64, gridDim.x, 0, t64, sh64);
+    __syncthreads();
+    reduce_partials<float, 1>(part32, gridDim.x, 0, t32, sh32);
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        st->want_ru = 0;
+        st->ru_count += 1;
+        const double rn = sqrt(t64[0]);
+        st->res64 = rn;
+        st->rn = rn;
+        st->maxr = rn;
+        if (rn <= st->tol_nb || st->it >= st->max_iter) { st->done = 1; return; }
+        // continue the recurrence from the true residual: beta from the refreshed r.z
+        const float rzn = t32[0];
+        if (!(rzn > 0.0f)) { st->breakdown = 1; st->done = 1; return; }
+        st->beta = rzn / st->rz_prev;
+        st->rz = rzn;
+    }
+}
+
+// x64 += d32 unconditionally (the correction still held when the loop stops)
+__global__ void k_mixed_flush_all(double *__restrict__ x, float *__restrict__ d, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] += (double)d[i];
+        d[i] = 0.0f;
+    }
+}
+
+// the FP32 recurrence starts from r32 = (float)(b - A x), p32 = inv32 r32, d32 = 0
+__global__ void k_mixed_init(const double *__restrict__ b, const double *__restrict__ Ax, float *__restrict__ r32,
+                             float *__restrict__ p32, float *__restrict__ d32, const float *__restrict__ inv32, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float rf = (float)(b[i] - Ax[i]);
+        r32[i] = rf;
+        p32[i] = inv32[i] * rf;
+        d32[i] = 0.0f;
+    }
+}
+
+__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+__global__ void k_jacobi_inv(const int *__restrict__ diag_pos, const double *__restrict__ data, double *__restrict__ inv,
+                             int n, int *__restrict__ status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int d = diag_pos[i];
+    const double a = d >= 0 ? data[d] : 0.0;
+    if (d < 0 || a == 0.0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
+    inv[i] = 1.0 / a;
+}
+
+__global__ void k_asym(const int *__restrict__ indptr, const int *__restrict__ indices, const double *__restrict__ v,
+                       int n, unsigned long long *__restrict__ out)
+{
+    // max |a_ij| and max |a_ij - a_ji| as the bit patterns of non-negative doubles (exact maxima)
+    unsigned long long big = 0, dif = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int q = indptr[i]; q < indptr[i + 1]; ++q) {
+            const int j = indices[q];
+            int lo = indptr[j], hi = indptr[j + 1];
+            const int end = hi;
+            while (lo < hi) {
+                const int mid = lo + ((hi - lo) >> 1);
+                if (indices[mid] < i) lo = mid + 1; else hi = mid;
+            }
+            const double m = (lo < end && indices[lo] == i) ? v[lo] : 0.0;
+            const unsigned long long a = __double_as_longlong(fabs(v[q]));
+            const unsigned long long d = __double_as_longlong(fabs(v[q] - m));
+            big = a > big ? a : big;
+            dif = d > dif ? d : dif;
+        }
+    atomicMax(out, big);
+    atomicMax(out + 1, dif);
+}
+
+__global__ void k_combine(double alpha, const double *__restrict__ A, double beta, const double *__restrict__ B,
+                          double *__restrict__ C, long long nnz)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += (long long)gridDim.x * blockDim.x)
+        C[q] = alpha * A[q] + beta * B[q];
+}
+
+// ---- host side -------------------------------------------------------------------------------
+unsigned red_grid(femd_ctx ctx, int n)
+{
+    // a fixed function of n (deterministic reductions): enough blocks to fill the GPU
+    const unsigned cap = (unsigned)ctx->sm_count * 8;
+    return grid_for((size_t)n, RED_BLOCK * 4, cap);
+}
+
+int pick_tpr(femd_matrix K)
+{
+    if (K->spmv_tpr) return K->spmv_tpr;
+    const double avg = K->pattern->nrows ? (double)K->pattern->nnz / K->pattern->nrows : 1.0;
+    return avg <= 6 ? 4 : avg <= 14 ? 8 : avg <= 28 ? 16 : 32;
+}
+
+template <class V, class T, bool DOT>
+static void launch_spmv(int tpr, unsigned grid, cudaStream_t s, const int *ip, const int *ix, const V *v, const T *x, T *y,
+                        int n, T *part, CGState<T> *st)
+{
+    switch (tpr) {
+    case 2: k_spmv<V, T, 2, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    case 4: k_spmv<V, T, 4, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    case 8: k_spmv<V, T, 8, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    case 16: k_spmv<V, T, 16, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    default: k_spmv<V, T, 32, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    }
+}
+
+unsigned spmv_grid(femd_ctx ctx, int n, int tpr)
+{
+    const int gpb = RED_BLOCK / tpr;
+    const unsigned cap = (unsigned)ctx->sm_count * 16;
+    return grid_for((size_t)n, gpb, cap);
+}
+
+// One CG solve (FP64) on device vectors.  Workspace: r, p, Ap (n each), partials, state.
+struct CGWork {
+    DevBuf<double> r, p, Ap, part;
+    DevBuf<CGState<double>> st;
+    CGState<double> *st_host = nullptr;
+    ~CGWork() { if (st_host) cudaFreeHost(st_host); }
+};
+
+static int cg_run(femd_ctx ctx, femd_matrix K, bool jac, const double *b, double *x, int max_iter, double tol,
+                  femd_cg_result *res)
+{
+    femd_pattern P = K->pattern;
+    const int n = P->nrows;
+    cudaStream_t s = ctx->stream;
+    CGWork W;
+    FEMD_TRY(W.r.alloc(n + 1));
+    FEMD_TRY(W.p.alloc(n + 1));
+    FEMD_TRY(W.Ap.alloc(n + 1));
+    const int tpr = pick_tpr(K);
+    const unsigned gs = spmv_grid(ctx, n, tpr), gr = red_grid(ctx, n);
+    FEMD_TRY(W.part.alloc(3 * (size_t)std::max(gs, gr) + 3));
+    FEMD_TRY(W.st.alloc(1));
+    FEMD_TRY_CUDA(cudaMallocHost(&W.st_host, sizeof(CGState<double>)));
+    FEMD_TRY_CUDA(cudaMemsetAsync(W.st.p, 0, sizeof(CGState<double>), s));
+    cudaEvent_t e0, e1;
+    FEMD_TRY_CUDA(cudaEventCreate(&e0));
+    FEMD_TRY_CUDA(cudaEventCreate(&e1));
+    FEMD_TRY_CUDA(cudaEventRecord(e0, s));
+    // start (cg.hpp:305-320)
+    launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x, W.Ap.p, n, nullptr, nullptr);
+    if (jac) k_cg_start<true><<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ap.p, W.r.p, W.p.p, K->inv.p, n, W.part.p, W.st.p, tol);
+    else k_cg_start<false><<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ap.p, W.r.p, W.p.p, nullptr, n, W.part.p, W.st.p, tol);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    // set max_iter on the device state (after start zeroed the counters)
+    {
+        CGState<double> init{};
+        (void)init;
+    }
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&W.st.p->max_iter, &max_iter, sizeof(int), cudaMemcpyHostToDevice, s));
+    // the loop, in chunks of CH iterations captured once in a CUDA graph
+    const int CH = n > (1 << 18) ? 8 : 32;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    FEMD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < CH; ++k) {
+        launch_spmv<double, double, true>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, W.p.p, W.Ap.p, n, W.part.p, W.st.p);
+        if (jac) {
+            k_cg_update<double, true><<<gr, RED_BLOCK, 0, counted(s)>>>(x, W.r.p, W.p.p, W.Ap.p, K->inv.p, n, W.part.p, W.st.p, 0);
+            k_cg_direction<double, true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.p.p, W.r.p, K->inv.p, n, W.st.p);
+        } else {
+            k_cg_update<double, false><<<gr, RED_BLOCK, 0, counted(s)>>>(x, W.r.p, W.p.p, W.Ap.p, nullptr, n, W.part.p, W.st.p, 0);
+            k_cg_direction<double, false><<<gr, RED_BLOCK, 0, counted(s)>>>(W.p.p, W.r.p, nullptr, n, W.st.p);
+        }
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) { set_error(std::string("cg: graph capture: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (ce != cudaSuccess) { cudaGraphDestroy(graph); set_error(std::string("cg: graph instantiate: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &nodes);
+    // poll the state between chunks; keep one chunk queued ahead
+    cudaEvent_t ev[2];
+    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    int status = FEMD_OK;
+    long long launched = 0;
+    const long long max_chunks = (long long)max_iter / CH + 2;
+    ce = launch_graph(exec, nodes, s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(W.st_host, W.st.p, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev[0], s);
+    launched = 1;
+    while (ce == cudaSuccess) {
+        // queue the next chunk before looking at the previous one
+        if (launched < max_chunks) {
+            ce = launch_graph(exec, nodes, s);
+            if (ce != cudaSuccess) break;
+        }
+        ce = cudaEventSynchronize(ev[(launched - 1) & 1]);
+        if (ce != cudaSuccess) break;
+        if (W.st_host->done) break;
+        if (launched >= max_chunks) break;
+        ce = cudaMemcpyAsync(W.st_host, W.st.p, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaEventRecord(ev[launched & 1], s);
+        ++launched;
+    }
+    if (ce != cudaSuccess) { set_error(std::string("cg: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; }
+    // finish (cg.hpp:222-237)
+    if (status == FEMD_OK) {
+        launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x, W.Ap.p, n, nullptr, nullptr);
+        k_cg_finish<<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ap.p, W.r.p, n, W.part.p, W.st.p);
+        cudaEventRecord(e1, s);
+        ce = cudaMemcpyAsync(W.st_host, W.st.p, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+        if (ce != cudaSuccess) { set_error(std::string("cg: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; }
+    }
+    if (status == FEMD_OK) {
+        const CGState<double> &S = *W.st_host;
+        if (S.nb == 0.0) {
+            cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), s);
+            cudaStreamSynchronize(s);
+            res->converged = 1; res->iterations = 0; res->residual = 0.0; res->breakdown = 0;
+        } else {
+            res->iterations = S.it;
+            res->breakdown = S.breakdown;
+            res->residual = S.res64 / S.nb;
+            int conv = !S.breakdown && res->residual <= tol * (1.0 + 1e-6) + 1e-15;
+            if (!conv && !S.breakdown && res->residual <= 10.0 * tol && S.it < max_iter) conv = 1;
+            res->converged = conv;
+        }
+        res->status = FEMD_OK;
+        res->outer = 0;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        res->seconds = ms * 1e-3;
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    return status;
+}
+
+static int ensure_f32(femd_ctx ctx, femd_matrix K)
+{
+    if (K->f32_valid) return FEMD_OK;
+    const long long nnz = K->pattern->nnz;
+    const int n = K->pattern->nrows;
+    if (!K->data32.p) FEMD_TRY(K->data32.alloc((size_t)nnz + 1));
+    if (!K->inv32.p) FEMD_TRY(K->inv32.alloc((size_t)n + 1));
+    if (nnz) k_to_f32<<<grid_for((size_t)nnz, 256, 1u << 20), 256, 0, counted(ctx->stream)>>>(K->data.p, K->data32.p, nnz);
+    if (n) k_to_f32<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(ctx->stream)>>>(K->inv.p, K->inv32.p, n);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    K->f32_valid = true;
+    return FEMD_OK;
+}
+
+// Mixed precision solve: inner FP32 Jacobi-PCG with reliable FP64 updates.
+static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b, double *x, int max_iter, double tol, femd_cg_result *res)
+{
+    femd_pattern P = K->pattern;
+    const int n = P->nrows;
+    cudaStream_t s = ctx->stream;
+    FEMD_TRY(ensure_f32(ctx, K));
+    DevBuf<double> Ax64, r64, part64;
+    DevBuf<float> r, p, Ap, d, part32;
+    DevBuf<CGState<float>> st;
+    DevBuf<CGState<double>> st64;
+    FEMD_TRY(Ax64.alloc(n + 1)); FEMD_TRY(r64.alloc(n + 1)); FEMD_TRY(r.alloc(n + 1)); FEMD_TRY(p.alloc(n + 1));
+    FEMD_TRY(Ap.alloc(n + 1)); FEMD_TRY(d.alloc(n + 1));
+    const int tpr = pick_tpr(K);
+    const unsigned gs = spmv_grid(ctx, n, tpr), gr = red_grid(ctx, n);
+    const size_t npart = 3 * (size_t)std::max(gs, gr) + 3;
+    FEMD_TRY(part64.alloc(npart)); FEMD_TRY(part32.alloc(npart));
+    FEMD_TRY(st.alloc(1)); FEMD_TRY(st64.alloc(1));
+    CGState<float> *sh = nullptr;
+    FEMD_TRY_CUDA(cudaMallocHost(&sh, sizeof(CGState<float>)));
+    struct FreeHost { CGState<float> *q; ~FreeHost() { cudaFreeHost(q); } } fh{sh};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    // FP64 start: r64 = b - A x, nb, ||r64||; the FP32 recurrence starts from (float) r64
+    FEMD_TRY_CUDA(cudaMemsetAsync(st64.p, 0, sizeof(CGState<double>), s));
+    launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, nullptr, nullptr);
+    k_cg_start<true><<<gr, RED_BLOCK, 0, counted(s)>>>(b, Ax64.p, r64.p, r64.p, K->inv.p, n, part64.p, st64.p, tol);
+    k_mixed_init<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(b, Ax64.p, r.p, p.p, d.p, K->inv32.p, n);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    CGState<double> s64;
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&s64, st64.p, sizeof(s64), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    if (s64.nb == 0.0) {
+        cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), s);
+        cudaStreamSynchronize(s);
+        *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
+        return FEMD_OK;
+    }
+    if (s64.done) {   // already converged at x0, or breakdown at the start
+        res->converged = !s64.breakdown; res->iterations = 0; res->residual = s64.rn / s64.nb;
+        res->breakdown = s64.breakdown; res->status = FEMD_OK; res->outer = 0; res->seconds = 0.0;
+        return FEMD_OK;
+    }
+    // FP32 state: rz = r32 . inv32 r32 is recomputed from the FP32 vectors by a reliable-update
+    // style kernel pass at the first chunk; seed it here from the FP64 start
+    CGState<float> s32{};
+    s32.rz = (float)s64.rz;
+    s32.nb = s64.nb;
+    s32.tol_nb = s64.tol_nb;
+    s32.rn = s64.rn;
+    s32.maxr = s64.rn;
+    s32.max_iter = max_iter;
+    FEMD_TRY_CUDA(cudaMemcpyAsync(st.p, &s32, sizeof(s32), cudaMemcpyHostToDevice, s));
+    const int CH = n > (1 << 18) ? 8 : 16;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    FEMD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < CH; ++k) {
+        launch_spmv<float, float, true>(tpr, gs, s, P->indptr.p, P->indices.p, K->data32.p, p.p, Ap.p, n, part32.p, st.p);
+        k_cg_update<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(d.p, r.p, p.p, Ap.p, K->inv32.p, n, part32.p, st.p, 1);
+        // a reliable update (when requested) before the direction update uses r
+        k_mixed_flush<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, d.p, n, st.p);
+        switch (tpr) {
+        case 4: k_mixed_spmv64<4><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
+        case 8: k_mixed_spmv64<8><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
+        case 16: k_mixed_spmv64<16><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
+        default: k_mixed_spmv64<32><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
+        }
+        k_mixed_residual<<<gr, RED_BLOCK, 0, counted(s)>>>(b, Ax64.p, r.p, K->inv32.p, n, part64.p, part32.p, st.p);
+        k_cg_direction<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(p.p, r.p, K->inv32.p, n, st.p);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) { set_error(std::string("pcg_mixed: graph capture: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (ce != cudaSuccess) { cudaGraphDestroy(graph); set_error(std::string("pcg_mixed: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &nodes);
+    const long long max_chunks = (long long)max_iter / CH + 2;
+    int status = FEMD_OK;
+    for (long long c = 0; c < max_chunks; ++c) {
+        ce = launch_graph(exec, nodes, s);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(sh, st.p, sizeof(CGState<float>), cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+        if (ce != cudaSuccess) { set_error(std::string("pcg_mixed: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; break; }
+        if (sh->done) break;
+    }
+    // final true residual in FP64 (cg.hpp:222-237)
+    if (status == FEMD_OK) {
+        // flush any correction still held in FP32 (when the loop ended on max_iter)
+        k_mixed_flush_all<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, d.p, n);
+        launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, nullptr, nullptr);
+        FEMD_TRY_CUDA(cudaMemsetAsync(st64.p, 0, sizeof(CGState<double>), s));
+        k_cg_finish<<<gr, RED_BLOCK, 0, counted(s)>>>(b, Ax64.p, Ax64.p, n, part64.p, st64.p);
+        cudaEventRecord(e1, s);
+        FEMD_TRY_CUDA(cudaMemcpyAsync(&s64, st64.p, sizeof(s64), cudaMemcpyDeviceToHost, s));
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+        res->iterations = sh->it;
+        res->breakdown = sh->breakdown;
+        res->residual = s64.res64 / sh->nb;
+        int conv = !sh->breakdown && res->residual <= tol * (1.0 + 1e-6) + 1e-15;
+        if (!conv && !sh->breakdown && res->residual <= 10.0 * tol && sh->it < max_iter) conv = 1;
+        res->converged = conv;
+        res->status = FEMD_OK;
+        res->outer = sh->ru_count;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        res->seconds = ms * 1e-3;
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    return status;
+}
+
+}  // namespace femd
+
+using namespace femd;
+
+static femd_matrix as_matrix(void *h)
+{
+    femd_matrix m = static_cast<femd_matrix>(h);
+    return (m && m->kind == KIND_MATRIX) ? m : nullptr;
+}
+
+extern "C" {
+
+int femd_cuda_matrix_create(femd_ctx ctx, femd_pattern p, femd_matrix *out)
+{
+    clear_error();
+    FEMD_CHECK_ARG(ctx && p && out && p->kind == KIND_PATTERN, "CSRMatrix: NULL or invalid argument");
+    *out = nullptr;
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    femd_matrix K = new femd_matrix_s();
+    K->ctx = ctx;
+    K->pattern = p;
+    int st = K->data.alloc((size_t)p->nnz + 1);
+    if (st == FEMD_OK) st = K->inv.alloc((size_t)p->nrows + 1);
+    if (st != FEMD_OK) { delete K; return st; }
+    cudaMemsetAsync(K->data.p, 0, ((size_t)p->nnz + 1) * sizeof(double), ctx->stream);
+    *out = K;
+    return FEMD_OK;
+}
+
+int femd_cuda_matrix_arrays(femd_matrix K, double **data_dev, double **inv_diag_dev)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(K, "matrix_arrays: not a matrix handle");
+    if (data_dev) *data_dev = K->data.p;
+    if (inv_diag_dev) *inv_diag_dev = K->inv.p;
+    K->f32_valid = false;   // the caller may write through these pointers
+    return FEMD_OK;
+}
+
+int femd_cuda_matrix_set_host(femd_matrix K, const double *data_host)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(K && data_host, "matrix_set_host: NULL argument");
+    FEMD_TRY_CUDA(cudaSetDevice(K->ctx->device));
+    if (K->pattern->nnz)
+        FEMD_TRY_CUDA(cudaMemcpyAsync(K->data.p, data_host, (size_t)K->pattern->nnz * sizeof(double), cudaMemcpyHostToDevice,
+                                      K->ctx->stream));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(K->ctx->stream));
+    K->f32_valid = false;
+    return FEMD_OK;
+}
+
+int femd_cuda_matrix_to_host(femd_matrix K, double *data_host)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(K && data_host, "matrix_to_host: NULL argument");
+    FEMD_TRY_CUDA(cudaSetDevice(K->ctx->device));
+    if (K->pattern->nnz)
+        FEMD_TRY_CUDA(cudaMemcpyAsync(data_host, K->data.p, (size_t)K->pattern->nnz * sizeof(double), cudaMemcpyDeviceToHost,
+                                      K->ctx->stream));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(K->ctx->stream));
+    return FEMD_OK;
+}
+
+int femd_cuda_matrix_jacobi(femd_ctx ctx, femd_matrix K)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K, "Jacobi: NULL argument");
+    FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "Jacobi: the matrix must be square");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    FEMD_TRY(reset_status(ctx));
+    const int n = K->pattern->nrows;
+    if (n) k_jacobi_inv<<<grid_for((size_t)n, 256), 256, 0, counted(ctx->stream)>>>(K->pattern->diag_pos.p, K->data.p, K->inv.p, n,
+                                                                           ctx->status_dev);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    int flags = 0, bad = 0;
+    FEMD_TRY(read_status(ctx, &flags, &bad));
+    K->f32_valid = false;
+    if (flags & ST_ZERODIAG) {
+        set_error("Jacobi: zero diagonal entry in row " + std::to_string(bad));
+        return FEMD_EZERODIAG;
+    }
+    return FEMD_OK;
+}
+
+int femd_cuda_matrix_inv_diag_to_host(femd_matrix K, double *inv_host)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(K && inv_host, "inv_diag_to_host: NULL argument");
+    FEMD_TRY_CUDA(cudaSetDevice(K->ctx->device));
+    if (K->pattern->nrows)
+        FEMD_TRY_CUDA(cudaMemcpyAsync(inv_host, K->inv.p, (size_t)K->pattern->nrows * sizeof(double), cudaMemcpyDeviceToHost,
+                                      K->ctx->stream));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(K->ctx->stream));
+    return FEMD_OK;
+}
+
+int femd_cuda_spmv(femd_ctx ctx, femd_matrix K, const double *x_dev, double *y_dev)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K, "matvec: NULL argument");
+    const int n = K->pattern->nrows;
+    FEMD_CHECK_ARG(n == 0 || (x_dev && y_dev), "matvec: NULL vector");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    if (n == 0) return FEMD_OK;
+    const int tpr = pick_tpr(K);
+    launch_spmv<double, double, false>(tpr, spmv_grid(ctx, n, tpr), ctx->stream, K->pattern->indptr.p, K->pattern->indices.p,
+                                       K->data.p, x_dev, y_dev, n, nullptr, nullptr);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    return FEMD_OK;
+}
+
+int femd_cuda_asymmetry(femd_ctx ctx, femd_matrix K, double *out)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K && out, "asymmetry: NULL argument");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    if (K->pattern->nrows != K->pattern->ncols) { *out = 1.0; return FEMD_OK; }
+    DevBuf<unsigned long long> m;
+    FEMD_TRY(m.alloc(2));
+    FEMD_TRY_CUDA(cudaMemsetAsync(m.p, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    const int n = K->pattern->nrows;
+    if (n) k_asym<<<grid_for((size_t)n, 256, (unsigned)ctx->sm_count * 8), 256, 0, counted(ctx->stream)>>>(
+        K->pattern->indptr.p, K->pattern->indices.p, K->data.p, n, m.p);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    unsigned long long h[2];
+    FEMD_TRY_CUDA(cudaMemcpyAsync(h, m.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    double big, dif;
+    memcpy(&big, &h[0], 8);
+    memcpy(&dif, &h[1], 8);
+    *out = big > 0.0 ? dif / big : 0.0;
+    return FEMD_OK;
+}
+
+int femd_cuda_combine(femd_ctx ctx, double alpha, femd_matrix A, double beta, femd_matrix B, femd_matrix C)
+{
+    clear_error();
+    A = as_matrix(A); B = as_matrix(B); C = as_matrix(C);
+    FEMD_CHECK_ARG(ctx && A && B && C, "combine: NULL argument");
+    FEMD_CHECK_ARG(A->pattern == B->pattern && A->pattern == C->pattern,
+                   "combine: A, B and C must share one pattern (CSRMatrix: shape mismatch in a sum)");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    const long long nnz = A->pattern->nnz;
+    if (nnz) k_combine<<<grid_for((size_t)nnz, 256, 1u << 20), 256, 0, counted(ctx->stream)>>>(alpha, A->data.p, beta, B->data.p, C->data.p, nnz);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    C->f32_valid = false;
+    return FEMD_OK;
+}
+
+int femd_cuda_cg_jacobi(femd_ctx ctx, femd_matrix K, int use_jacobi, const double *b_dev, double *x_dev, int max_iter,
+                        double tol, femd_cg_result *res)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K && res, "cg: NULL argument");
+    FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "cg: the matrix must be square");
+    const int n = K->pattern->nrows;
+    FEMD_CHECK_ARG(n == 0 || (b_dev && x_dev), "cg: NULL vector");
+    FEMD_CHECK_ARG(max_iter >= 0, "cg: max_iter must be >= 0");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
+    if (n == 0) return FEMD_OK;
+    return cg_run(ctx, K, use_jacobi != 0, b_dev, x_dev, max_iter, tol, res);
+}
+
+int femd_cuda_pcg_mixed(femd_ctx ctx, femd_matrix K, const double *b_dev, double *x_dev, int max_iter, double tol,
+                        femd_cg_result *res)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K && res, "pcg_mixed: NULL argument");
+    FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "pcg_mixed: the matrix must be square");
+    const int n = K->pattern->nrows;
+    FEMD_CHECK_ARG(n == 0 || (b_dev && x_dev), "pcg_mixed: NULL vector");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
+    if (n == 0) return FEMD_OK;
+    return mixed_run(ctx, K, b_dev, x_dev, max_iter, tol, res);
+}
+
+int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host, const int *indices_host, const double *data_host,
+                            const double *inv_host, const double *b_host, const double *x0_host, double *x_host,
+                            int max_iter, double tol, femd_cg_result *res)
+{
+    clear_error();
+    FEMD_CHECK_ARG(ctx && indptr_host && res && b_host && x_host, "cg: NULL argument");
+    FEMD_CHECK_ARG(n >= 0, "cg: negative size");
+    femd_pattern P = nullptr;
+    FEMD_TRY(femd_cuda_pattern_from_csr_host(ctx, n, n, indptr_host, indices_host, &P));
+    femd_matrix K = nullptr;
+    int st = femd_cuda_matrix_create(ctx, P, &K);
+    if (st) { femd_cuda_release(P); return st; }
+    DevBuf<double> b, x;
+    cudaStream_t s = ctx->stream;
+    const long long nnz = P->nnz;
+    st = b.alloc((size_t)n + 1);
+    if (!st) st = x.alloc((size_t)n + 1);
+    cudaError_t e = cudaSuccess;
+    if (!st) {
+        if (nnz) e = cudaMemcpyAsync(K->data.p, data_host, (size_t)nnz * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && inv_host) e = cudaMemcpyAsync(K->inv.p, inv_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b.p, b_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) {
+            if (x0_host) e = cudaMemcpyAsync(x.p, x0_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
+            else e = cudaMemsetAsync(x.p, 0, (size_t)n * sizeof(double), s);
+        }
+        if (e != cudaSuccess) { set_error(std::string("cg: ") + cudaGetErrorString(e)); st = FEMD_ECUDA; }
+    }
+    if (!st) st = femd_cuda_cg_jacobi(ctx, K, inv_host != nullptr, b.p, x.p, max_iter, tol, res);
+    if (!st && n) {
+        e = cudaMemcpyAsync(x_host, x.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { set_error(std::string("cg: ") + cudaGetErrorString(e)); st = FEMD_ECUDA; }
+    }
+    femd_cuda_release(K);
+    femd_cuda_release(P);
+    return st;
+}
+
+}  // extern "C"

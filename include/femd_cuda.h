@@ -1,0 +1,243 @@
+/*
+ * femd_cuda.h -- the C ABI of libfemd_cuda.so: FEMd's 2D Lagrange P_k triangle assembly into
+ * CSR and its Jacobi-preconditioned CG solve, on one NVIDIA B200 (sm_100a).
+ *
+ * This is the drop-in boundary.  Every entry point replaces one function of FEMd's own
+ * nanobind module `_femd` (python/src/femd_bindings*.cpp in the FEMd tree), named beside
+ * it, with the same argument meaning and the same error behaviour: where the reference
+ * throws std::invalid_argument the call returns FEMD_EINVAL, std::logic_error /
+ * std::runtime_error give FEMD_EOUTSIDE / FEMD_EZERODIAG, and the text of the reference's
+ * exception is available from femd_cuda_last_error().  CG non-convergence and breakdown are
+ * not errors (the reference reports them in its result tuple): they are fields of
+ * femd_cg_result and the call returns FEMD_OK.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Arrays named *_dev are device pointers (cudaMalloc'd or
+ *     any device-accessible memory of the context's device); arrays named *_host are host
+ *     pointers (pageable or pinned).  Index arrays are int32, values float64 unless named f32.
+ *   - Every call is asynchronous on the context's stream unless it returns a host value or
+ *     fills a host array, in which case it synchronizes that stream before returning.
+ *   - Handles (femd_pattern, femd_matrix, femd_solver) own device memory; release them with
+ *     femd_cuda_release().  Calls on different contexts may run concurrently from different
+ *     host threads; one context must not be used by two threads at once.
+ *   - femd_cuda_last_error() is per host thread.
+ */
+#ifndef FEMD_CUDA_H
+#define FEMD_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FEMD_API __attribute__((visibility("default")))
+#else
+#define FEMD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------------------- */
+#define FEMD_OK          0
+#define FEMD_EINVAL      1   /* bad argument (reference: std::invalid_argument -> ValueError) */
+#define FEMD_ENOMEM      2   /* device or host allocation failed */
+#define FEMD_ECUDA       3   /* a CUDA runtime error; femd_cuda_last_error() has its text */
+#define FEMD_EOUTSIDE    4   /* an element entry outside the pattern (reference: std::logic_error) */
+#define FEMD_EZERODIAG   5   /* Jacobi: zero diagonal entry (reference: std::invalid_argument) */
+#define FEMD_ETIMEOUT    6   /* a bounded device-side wait ran out (batched / served solves) */
+#define FEMD_EABORT      7   /* a host-requested abort stopped a batched solve */
+
+typedef struct femd_ctx_s *femd_ctx;
+typedef struct femd_pattern_s *femd_pattern;
+typedef struct femd_matrix_s *femd_matrix;
+
+/* Last error text of this host thread ("" when none). */
+FEMD_API const char *femd_cuda_last_error(void);
+/* Library version string. */
+FEMD_API const char *femd_cuda_version(void);
+/* Kernel launches this library has issued in this process (a launched CUDA graph counts its
+ * kernel nodes).  No reference counterpart: an instrumentation counter. */
+FEMD_API long long femd_cuda_kernel_launches(void);
+
+/* A context: one device and one stream (created, non-blocking).  device < 0: the current device. */
+FEMD_API int femd_cuda_ctx_create(int device, femd_ctx *out);
+FEMD_API int femd_cuda_ctx_destroy(femd_ctx ctx);
+/* The context's stream, as a cudaStream_t cast to void*. */
+FEMD_API void *femd_cuda_ctx_stream(femd_ctx ctx);
+/* Wait for all work queued on the context's stream. */
+FEMD_API int femd_cuda_ctx_sync(femd_ctx ctx);
+/* Release any handle created by this library (pattern, matrix, solver, batch). NULL is a no-op. */
+FEMD_API void femd_cuda_release(void *handle);
+
+/* ======================================================================================
+ * Sparsity pattern: K1.
+ * Replaces cell_pattern(T, S) (python/src/femd_bindings_2d.cpp:762) ->
+ * SparsityPattern::from_cells (include/femd/sparse/csr.hpp:84-125), for a square pattern
+ * whose rows and columns are numbered by the same cell->dof map (T == S).
+ * cell_dofs_dev: ncells x nloc, -1 for a constrained (eliminated) node.
+ * The result is bit-identical to the reference's indptr / indices.  The handle also keeps,
+ * for every row, the (cell, local index) pairs holding it in increasing cell order (the
+ * reference's cellof lists, csr.hpp:90-98), which the assembly kernels use.
+ * ====================================================================================== */
+FEMD_API int femd_cuda_pattern_from_cells(femd_ctx ctx, int nrows, int ncells, int nloc, const int *cell_dofs_dev,
+                                 femd_pattern *out);
+FEMD_API int femd_cuda_pattern_info(femd_pattern p, int *nrows, int *ncols, long long *nnz);
+/* Device views of the pattern's arrays (owned by the pattern). */
+FEMD_API int femd_cuda_pattern_arrays(femd_pattern p, const int **indptr_dev, const int **indices_dev);
+/* Copy indptr (nrows + 1) and indices (nnz) to host arrays; synchronizes. */
+FEMD_API int femd_cuda_pattern_to_host(femd_pattern p, int *indptr_host, int *indices_host);
+/* A pattern from existing CSR arrays (copied to the device; rows must be sorted and unique,
+ * as CSRMatrix.from_arrays requires, python/src/femd_bindings_2d.cpp:101-116). */
+FEMD_API int femd_cuda_pattern_from_csr_host(femd_ctx ctx, int nrows, int ncols, const int *indptr_host,
+                                    const int *indices_host, femd_pattern *out);
+
+/* ======================================================================================
+ * Scatter map: K2.
+ * Replaces scatter_map_2d(QT, QS, P, 0, 0) (include/femd/forms/assembly_2d.hpp:136-164):
+ * map_dev[(e nloc + i) nloc + j] = position of (dof(e,i), dof(e,j)) in the pattern's
+ * indices, -1 where either is constrained.  Returns FEMD_EOUTSIDE (the reference throws
+ * std::logic_error "assemble_matrix_2d: entry outside the pattern") if an entry is missing.
+ * The map is also kept inside the pattern (femd_cuda_pattern_map) for the assembly kernels.
+ * ====================================================================================== */
+FEMD_API int femd_cuda_scatter_map(femd_ctx ctx, femd_pattern p, int *map_dev);
+FEMD_API int femd_cuda_pattern_map(femd_pattern p, const int **map_dev);
+
+/* ======================================================================================
+ * Matrices: values on a pattern.
+ * Replaces CSRMatrix(pattern) (python/src/femd_bindings_2d.cpp:101) and the Jacobi
+ * preconditioner JacobiPreconditioner(K) (include/femd/sparse/precond.hpp:82-102), whose
+ * inverse diagonal the matrix keeps (computed by the assembly epilogue or by
+ * femd_cuda_matrix_jacobi).
+ * ====================================================================================== */
+FEMD_API int femd_cuda_matrix_create(femd_ctx ctx, femd_pattern p, femd_matrix *out);
+FEMD_API int femd_cuda_matrix_arrays(femd_matrix K, double **data_dev, double **inv_diag_dev);
+FEMD_API int femd_cuda_matrix_set_host(femd_matrix K, const double *data_host);
+FEMD_API int femd_cuda_matrix_to_host(femd_matrix K, double *data_host);
+/* inv_diag = 1 / a_ii; FEMD_EZERODIAG with "Jacobi: zero diagonal entry in row i"
+ * (precond.hpp:68-78) when some a_ii is 0 or missing. */
+FEMD_API int femd_cuda_matrix_jacobi(femd_ctx ctx, femd_matrix K);
+/* Copy of the inverse diagonal to the host (nrows); synchronizes. */
+FEMD_API int femd_cuda_matrix_inv_diag_to_host(femd_matrix K, double *inv_host);
+
+/* ======================================================================================
+ * Assembly: K3 (matrix) and K4 (vector).
+ * Replaces assemble_matrix_2d (python/src/femd_bindings_2d.cpp:810-816 ->
+ * include/femd/forms/assembly_2d.hpp:219-305) and assemble_vector_2d (:817-822 ->
+ * assembly_2d.hpp:173-211) on affine triangles, with the geometry read from the mesh
+ * (vertex coordinates and triangles) instead of per-point arrays: J = [P1-P0, P2-P0],
+ * w = rw |det J|, J^{-1} as in lagrange_space_2d.hpp:44-52 and cache_2d.hpp:110-118.
+ *
+ *   K  = sum_t integral c_t (D^{a_t} phi_i)(D^{b_t} phi_j)        codes 0 value, 1 d/dx, 2 d/dy
+ *   f  = sum_t integral c_t (D^{a_t} phi_i)
+ *
+ * The rule is the reference tabulation of the cell cache (Cache2D::ref: nq points x
+ * [phi, dphi/dxi, dphi/deta] x nloc, host array) with the reference points and weights.
+ * Coefficients: one femd_coef per term.  Each matrix entry and vector entry is summed in
+ * increasing cell order with no atomics (deterministic, the reference's order).
+ * mode FEMD_ASM_FAST contracts per-cell geometric factors with precomputed reference
+ * tensors; FEMD_ASM_EXACT forms every element entry with the reference's own operation
+ * order (element_matrix_2d, assembly_2d.hpp:102-126, no fused multiply-adds) and so gives
+ * the reference's bits for the same tabulation and coefficients.
+ * ====================================================================================== */
+#define FEMD_COEF_CONST   0   /* value */
+#define FEMD_COEF_POINTS  1   /* points_dev[e nq + q] (the reference's coefficient arrays) */
+#define FEMD_COEF_SINSIN  2   /* p0 + p1 sin(p2 x) sin(p3 y) */
+#define FEMD_COEF_SINSIN_HELM 3 /* p0 s + s, s = sin(p2 x) sin(p3 y) (the written sum of two terms) */
+#define FEMD_COEF_FIELD   4   /* a P_k field at the points: sum_l phi_l(q) field_dev[dof(e,l)] (Cache2D::eval_multi) */
+
+typedef struct {
+    int kind;
+    double value;
+    const double *points_dev;
+    const double *field_dev;
+    double p[4];
+} femd_coef;
+
+#define FEMD_ASM_FAST  0
+#define FEMD_ASM_EXACT 1
+
+typedef struct {
+    int nverts, ncells;
+    const double *points_dev;   /* nverts x 2 */
+    const int *tris_dev;        /* ncells x 3, counter-clockwise */
+} femd_mesh2d;
+
+typedef struct {
+    int k, nloc, nq;
+    const double *ref_host;     /* nq x 3 x nloc */
+    const double *xi_host, *eta_host, *w_host;   /* nq reference points and weights */
+} femd_rule;
+
+/* K (values overwritten) = the form; also refreshes K's inverse diagonal when want_inv. */
+FEMD_API int femd_cuda_assemble_matrix(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p,
+                              int nterms, const int *a, const int *b, const femd_coef *coef, int mode, femd_matrix K,
+                              int want_inv);
+/* f_dev (nrows entries, overwritten) = the rank-1 form; the pattern supplies the row lists. */
+FEMD_API int femd_cuda_assemble_vector(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p,
+                              int nterms, const int *a, const femd_coef *coef, int mode, double *f_dev);
+
+/* ======================================================================================
+ * Sparse kernels on a matrix.
+ * ====================================================================================== */
+/* y = K x: CSRMatrix::apply (include/femd/sparse/csr.hpp:203-215). */
+FEMD_API int femd_cuda_spmv(femd_ctx ctx, femd_matrix K, const double *x_dev, double *y_dev);
+/* max |a_ij - a_ji| / max |a_ij|: asymmetry (csr.hpp:632-645); synchronizes. */
+FEMD_API int femd_cuda_asymmetry(femd_ctx ctx, femd_matrix K, double *out);
+/* C = alpha A + beta B on one shared pattern: combine (csr.hpp:315-326). */
+FEMD_API int femd_cuda_combine(femd_ctx ctx, double alpha, femd_matrix A, double beta, femd_matrix B, femd_matrix C);
+
+/* ======================================================================================
+ * Jacobi-PCG: K5 (SpMV fused with p^T A p) and K6 (fused update with ||r||^2 and r^T D^-1 r).
+ * Replaces cg_solve(A, M, b, x0, max_iter, tol) (python/src/femd_bindings.cpp:799-833) with
+ * M a JacobiPreconditioner or None -> krylov::cg_jacobi (include/femd/krylov/cg.hpp:296-350)
+ * with the same stopping rule, final true residual, 10 tol acceptance and breakdown tests
+ * (cg.hpp:222-237).  The reductions are deterministic (fixed order, the same bits on every
+ * run) but not the reference's chunk order, so iteration counts may differ by a few.
+ * ====================================================================================== */
+typedef struct {
+    int converged;
+    int iterations;
+    double residual;      /* ||b - A x|| / ||b||, recomputed at the end */
+    int breakdown;        /* p^T A p <= 0 or r^T z <= 0 */
+    int status;           /* FEMD_OK, or FEMD_ETIMEOUT / FEMD_EABORT for bounded solves */
+    int outer;            /* refinement steps (mixed precision), 0 otherwise */
+    double seconds;       /* device time of the solve (CUDA events) */
+} femd_cg_result;
+
+/* x_dev: initial guess in, solution out.  use_jacobi 0: no preconditioner (M = None). */
+FEMD_API int femd_cuda_cg_jacobi(femd_ctx ctx, femd_matrix K, int use_jacobi, const double *b_dev, double *x_dev, int max_iter,
+                        double tol, femd_cg_result *res);
+/* The same with host CSR arrays and vectors (the exact data the reference binding holds):
+ * uploads A and b, solves, writes x back; inv_host may be NULL (no preconditioner) or the
+ * reference's JacobiPreconditioner.inverse_diagonal(). */
+FEMD_API int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host, const int *indices_host,
+                            const double *data_host, const double *inv_host, const double *b_host, const double *x0_host,
+                            double *x_host, int max_iter, double tol, femd_cg_result *res);
+
+/* Mixed precision: inner Jacobi-PCG on an FP32 copy of K with FP32 vectors and FP32
+ * accumulation; the residual r = b - A x is recomputed on the FP64 matrix and the solution
+ * updated in FP64 (reliable updates) until ||b - A x|| <= tol ||b||. */
+FEMD_API int femd_cuda_pcg_mixed(femd_ctx ctx, femd_matrix K, const double *b_dev, double *x_dev, int max_iter, double tol,
+                        femd_cg_result *res);
+
+/* ======================================================================================
+ * Host-side setup of the synthetic problems (the reference's own setup code runs on the
+ * host too).  No GPU work.
+ * ====================================================================================== */
+/* rectangle_mesh(x0,y0,x1,y1,nx,ny), diagonal "right" (include/femd/mesh/structured.hpp:338-351). */
+FEMD_API int femd_host_rectangle_mesh(double x0, double y0, double x1, double y1, int nx, int ny, double *points, int *tris);
+/* Continuous P_k numbering with every exterior edge Dirichlet (LagrangeSpace2D(m, k, {}, true),
+ * include/femd/fe/space_2d.hpp:390-526).  cell_dofs: ncells x nloc; returns dim via *dim. */
+FEMD_API int femd_host_lagrange_numbering(int nverts, int ncells, const int *tris, int k, int all_exterior, int *cell_dofs,
+                                 int *dim, int *raw_dim);
+/* TriangleQuadrature(degree) (include/femd/quadrature/triangle.hpp:24-58): returns nq (<= 64). */
+FEMD_API int femd_host_triangle_quadrature(int degree, double *xi, double *eta, double *w);
+/* The equispaced P_k basis and its reference derivatives at points: out[q][3][nloc]. */
+FEMD_API int femd_host_tabulate(int k, int nq, const double *xi, const double *eta, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FEMD_CUDA_H */

@@ -32,7 +32,7 @@
 //           poisson_vec   a = c grad.grad,            b read from --b (dim entries)
 //           heat          M = u v and K = grad.grad (both written), no solve
 //   options: --c <value> --tol <t> --f <file> --b <file> --nocg --chol --nodump
-//            --time <reps> --cg-sample <iters>
+//            --time <reps> --cg-sample <iters> --full-first (the first timed step runs CG to convergence)
 #include "femd/mesh/structured.hpp"
 #include "femd/fe/lagrange_space_2d.hpp"
 #include "femd/fe/cache_2d.hpp"
@@ -99,6 +99,7 @@ struct Opts {
     std::string fpath, bpath;
     bool cg = true, chol = false, dumpall = true;
     int time_reps = 0, cg_sample = 0;
+    bool full_first = false;
 };
 
 static std::vector<double> const_coeff(const Cache2D &Q, double v)
@@ -124,6 +125,7 @@ int main(int argc, char **argv)
         else if (a == "--nodump") o.dumpall = false;
         else if (a == "--time") o.time_reps = std::atoi(next().c_str());
         else if (a == "--cg-sample") o.cg_sample = std::atoi(next().c_str());
+        else if (a == "--full-first") o.full_first = true;
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     const std::string &dir = o.out;
@@ -265,7 +267,7 @@ int main(int argc, char **argv)
         std::vector<double> xs(static_cast<std::size_t>(n)), ys(static_cast<std::size_t>(n));
         for (int i = 0; i < n; ++i) xs[i] = 1.0 + 0.5 * std::sin(1.0 + 0.7 * i);
         double ts = now();
-        const int reps = o.time_reps > 0 ? 10 : 1;
+        const int reps = o.time_reps > 0 ? 3 : 1;
         for (int r = 0; r < reps; ++r) K.apply(xs.data(), ys.data());
         std::fprintf(meta, "t_spmv %.6f\n", (now() - ts) / reps);
         dump(dir, "spmv_y", ys);
@@ -311,7 +313,7 @@ int main(int argc, char **argv)
             K.apply(in.data(), out.data());
         };
         std::vector<double> x(static_cast<std::size_t>(n), 0.0);
-        const int cap = o.cg_sample > 0 ? o.cg_sample : maxiter;
+        const int cap = (o.cg_sample > 0 && !(o.full_first && rep == 0)) ? o.cg_sample : maxiter;
         double tc = now();
         krylov::CGResult r = krylov::cg_jacobi(op, J.inverse_diagonal().data(), x, bb, cap, o.tol);
         tc = now() - tc;
