@@ -69,6 +69,8 @@ SIGNATURES = {
     "femd_cuda_assemble_vector": (_I, [_P, C.POINTER(femd_mesh2d), C.POINTER(femd_rule), _P, _I, _P,
                                        C.POINTER(femd_coef), _I, _P]),
     "femd_cuda_spmv": (_I, [_P, _P, _P, _P]),
+    "femd_cuda_spmv_autotune": (_I, [_P, _P, _I, _PI, C.POINTER(C.c_double)]),
+    "femd_cuda_spmv_set_tpr": (_I, [_P, _I]),
     "femd_cuda_asymmetry": (_I, [_P, _P, C.POINTER(C.c_double)]),
     "femd_cuda_combine": (_I, [_P, _D, _P, _D, _P, _P]),
     "femd_cuda_cg_jacobi": (_I, [_P, _P, _I, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),

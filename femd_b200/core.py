@@ -375,6 +375,15 @@ class CSRMatrix(_Handle):
         check(lib.femd_cuda_spmv(self.ctx.h, self.h, _ptr(x), _ptr(y)))
         return y
 
+    def autotune_spmv(self, set_best: bool = True):
+        """Time the SpMV's threads-per-row variants on this matrix; returns (best, microseconds)."""
+        t, us = C.c_int(), C.c_double()
+        check(lib.femd_cuda_spmv_autotune(self.ctx.h, self.h, int(set_best), C.byref(t), C.byref(us)))
+        return t.value, us.value
+
+    def set_spmv_tpr(self, tpr: int):
+        check(lib.femd_cuda_spmv_set_tpr(self.h, int(tpr)))
+
     def asymmetry(self):
         out = C.c_double()
         check(lib.femd_cuda_asymmetry(self.ctx.h, self.h, C.byref(out)))

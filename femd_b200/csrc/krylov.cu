@@ -86,7 +86,11 @@ __device__ __forceinline__ void reduce_partials(const T *part, int np, int ld, T
 }
 
 // ---- SpMV: y = A x, TPR lanes per row; DOT adds x_i y_i into the block partial ------------
-template <class V, class T, int TPR, bool DOT>
+// Each lane takes the entries lo + lane, lo + lane + TPR, ... of its row, U at a time: the U
+// index and value loads are issued together, then the U gathers of x, then the U products
+// (memory-level parallelism for a latency-bound stream).  The lane's additions stay in entry
+// order, so U does not change the result; TPR does (the shuffle tree).
+template <class V, class T, int TPR, int U, bool DOT>
 __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indptr, const int *__restrict__ indices,
                                                     const V *__restrict__ vals, const T *__restrict__ x,
                                                     T *__restrict__ y, int n, T *__restrict__ part,
@@ -104,7 +108,24 @@ __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indp
         T s = T(0);
         if (i < n) {
             const int lo = indptr[i], hi = indptr[i + 1];
-            for (int q = lo + lane; q < hi; q += TPR) s += (T)vals[q] * __ldg(&x[indices[q]]);
+            for (int base = lo + lane; base < hi; base += U * TPR) {
+                int c[U];
+                V v[U];
+                T xv[U];
+                // the matrix is streamed once (evict-first loads); x is gathered through the
+                // read-only path and stays cached
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int q = base + u * TPR;
+                    c[u] = q < hi ? __ldcs(&indices[q]) : 0;
+                    v[u] = q < hi ? __ldcs(&vals[q]) : V(0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) xv[u] = base + u * TPR < hi ? __ldg(&x[c[u]]) : T(0);
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (base + u * TPR < hi) s += (T)v[u] * xv[u];
+            }
         }
 #pragma unroll
         for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
@@ -287,7 +308,7 @@ __global__ void __launch_bounds__(RED_BLOCK) k_mixed_spmv64(const int *__restric
         const int i = i0 + (threadIdx.x & 31) / TPR;
         double s = 0.0;
         if (i < n)
-            for (int q = indptr[i] + lane; q < indptr[i + 1]; q += TPR) s += vals[q] * __ldg(&x[indices[q]]);
+            for (int q = indptr[i] + lane; q < indptr[i + 1]; q += TPR) s += __ldcs(&vals[q]) * __ldg(&x[__ldcs(&indices[q])]);
 #pragma unroll
         for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
         if (lane == 0 && i < n) y[i] = s;
@@ -423,25 +444,42 @@ int pick_tpr(femd_matrix K)
 {
     if (K->spmv_tpr) return K->spmv_tpr;
     const double avg = K->pattern->nrows ? (double)K->pattern->nnz / K->pattern->nrows : 1.0;
-    return avg <= 6 ? 4 : avg <= 14 ? 8 : avg <= 28 ? 16 : 32;
+    const int tpr = avg <= 6 ? 4 : avg <= 14 ? 8 : avg <= 28 ? 16 : 32;
+    return tpr | (2 << 8);
 }
 
-template <class V, class T, bool DOT>
-static void launch_spmv(int tpr, unsigned grid, cudaStream_t s, const int *ip, const int *ix, const V *v, const T *x, T *y,
-                        int n, T *part, CGState<T> *st)
+// shape = threads per row (low byte) | loads in flight per lane (next byte)
+static inline int shape_tpr(int shape) { return shape & 0xff; }
+static inline int shape_u(int shape) { return (shape >> 8) ? (shape >> 8) : 1; }
+
+template <class V, class T, bool DOT, int U>
+static void launch_spmv_u(int tpr, unsigned grid, cudaStream_t s, const int *ip, const int *ix, const V *v, const T *x, T *y,
+                          int n, T *part, CGState<T> *st)
 {
     switch (tpr) {
-    case 2: k_spmv<V, T, 2, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
-    case 4: k_spmv<V, T, 4, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
-    case 8: k_spmv<V, T, 8, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
-    case 16: k_spmv<V, T, 16, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
-    default: k_spmv<V, T, 32, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    case 2: k_spmv<V, T, 2, U, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    case 4: k_spmv<V, T, 4, U, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    case 8: k_spmv<V, T, 8, U, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    case 16: k_spmv<V, T, 16, U, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
+    default: k_spmv<V, T, 32, U, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
     }
 }
 
-unsigned spmv_grid(femd_ctx ctx, int n, int tpr)
+template <class V, class T, bool DOT>
+static void launch_spmv(int shape, unsigned grid, cudaStream_t s, const int *ip, const int *ix, const V *v, const T *x, T *y,
+                        int n, T *part, CGState<T> *st)
 {
-    const int gpb = RED_BLOCK / tpr;
+    const int tpr = shape_tpr(shape);
+    switch (shape_u(shape)) {
+    case 2: launch_spmv_u<V, T, DOT, 2>(tpr, grid, s, ip, ix, v, x, y, n, part, st); break;
+    case 4: launch_spmv_u<V, T, DOT, 4>(tpr, grid, s, ip, ix, v, x, y, n, part, st); break;
+    default: launch_spmv_u<V, T, DOT, 1>(tpr, grid, s, ip, ix, v, x, y, n, part, st); break;
+    }
+}
+
+unsigned spmv_grid(femd_ctx ctx, int n, int shape)
+{
+    const int gpb = RED_BLOCK / shape_tpr(shape);
     const unsigned cap = (unsigned)ctx->sm_count * 16;
     return grid_for((size_t)n, gpb, cap);
 }
@@ -645,7 +683,8 @@ static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b, double *x, in
         k_cg_update<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(d.p, r.p, p.p, Ap.p, K->inv32.p, n, part32.p, st.p, 1);
         // a reliable update (when requested) before the direction update uses r
         k_mixed_flush<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, d.p, n, st.p);
-        switch (tpr) {
+        switch (shape_tpr(tpr)) {
+        case 2: k_mixed_spmv64<2><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
         case 4: k_mixed_spmv64<4><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
         case 8: k_mixed_spmv64<8><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
         case 16: k_mixed_spmv64<16><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
@@ -812,6 +851,65 @@ int femd_cuda_spmv(femd_ctx ctx, femd_matrix K, const double *x_dev, double *y_d
     launch_spmv<double, double, false>(tpr, spmv_grid(ctx, n, tpr), ctx->stream, K->pattern->indptr.p, K->pattern->indices.p,
                                        K->data.p, x_dev, y_dev, n, nullptr, nullptr);
     FEMD_TRY_CUDA(cudaGetLastError());
+    return FEMD_OK;
+}
+
+int femd_cuda_spmv_autotune(femd_ctx ctx, femd_matrix K, int set, int *tpr_out, double *us_out)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K, "spmv_autotune: NULL argument");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    const int n = K->pattern->nrows;
+    if (n == 0) { if (tpr_out) *tpr_out = pick_tpr(K); if (us_out) *us_out = 0.0; return FEMD_OK; }
+    DevBuf<double> x, y;
+    FEMD_TRY(x.alloc(K->pattern->ncols + 1));
+    FEMD_TRY(y.alloc(n + 1));
+    FEMD_TRY_CUDA(cudaMemsetAsync(x.p, 0, (K->pattern->ncols + 1) * sizeof(double), ctx->stream));
+    cudaEvent_t e0, e1;
+    FEMD_TRY_CUDA(cudaEventCreate(&e0));
+    FEMD_TRY_CUDA(cudaEventCreate(&e1));
+    // shapes: threads per row 2..32 x loads in flight per lane 1, 2, 4
+    std::vector<int> cand;
+    for (int t : {2, 4, 8, 16, 32})
+        for (int u : {1, 2, 4}) cand.push_back(t | (u << 8));
+    int best = pick_tpr(K);
+    float best_ms = 1e30f;
+    for (int c : cand) {
+        const unsigned g = spmv_grid(ctx, n, c);
+        for (int w = 0; w < 2; ++w)
+            launch_spmv<double, double, false>(c, g, ctx->stream, K->pattern->indptr.p, K->pattern->indices.p, K->data.p,
+                                               x.p, y.p, n, nullptr, nullptr);
+        cudaEventRecord(e0, ctx->stream);
+        const int reps = 5;
+        for (int r = 0; r < reps; ++r)
+            launch_spmv<double, double, false>(c, g, ctx->stream, K->pattern->indptr.p, K->pattern->indices.p, K->data.p,
+                                               x.p, y.p, n, nullptr, nullptr);
+        cudaEventRecord(e1, ctx->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); set_error(cudaGetErrorString(e)); return FEMD_ECUDA; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= reps;
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (set) K->spmv_tpr = best;
+    if (tpr_out) *tpr_out = best;
+    if (us_out) *us_out = best_ms * 1e3;
+    return FEMD_OK;
+}
+
+int femd_cuda_spmv_set_tpr(femd_matrix K, int tpr)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(K, "spmv_set_tpr: not a matrix handle");
+    const int t = shape_tpr(tpr), u = tpr >> 8;
+    FEMD_CHECK_ARG(tpr == 0 || ((t == 2 || t == 4 || t == 8 || t == 16 || t == 32) && (u == 0 || u == 1 || u == 2 || u == 4)),
+                   "spmv_set_tpr: shape = threads per row (0 heuristic, 2..32) | loads per lane (1, 2, 4) << 8");
+    K->spmv_tpr = tpr;
     return FEMD_OK;
 }
 

@@ -182,6 +182,14 @@ FEMD_API int femd_cuda_assemble_vector(femd_ctx ctx, const femd_mesh2d *mesh, co
  * ====================================================================================== */
 /* y = K x: CSRMatrix::apply (include/femd/sparse/csr.hpp:203-215). */
 FEMD_API int femd_cuda_spmv(femd_ctx ctx, femd_matrix K, const double *x_dev, double *y_dev);
+/* Autotuner of the SpMV (no reference counterpart: the reference's loop has no launch shape):
+ * times the launch shapes on K -- threads per row 2..32 (low byte) | loads in flight per lane
+ * 1, 2, 4 (next byte) -- and returns the fastest (and, with set != 0, keeps it for K's SpMV and
+ * CG).  Threads per row changes the summation order of a row, so a tuned matrix may give
+ * results that differ from an untuned one in the last bits; loads per lane does not. */
+FEMD_API int femd_cuda_spmv_autotune(femd_ctx ctx, femd_matrix K, int set, int *shape_out, double *us_out);
+/* Fix K's SpMV shape (0 = the built-in heuristic). */
+FEMD_API int femd_cuda_spmv_set_tpr(femd_matrix K, int shape);
 /* max |a_ij - a_ji| / max |a_ij|: asymmetry (csr.hpp:632-645); synchronizes. */
 FEMD_API int femd_cuda_asymmetry(femd_ctx ctx, femd_matrix K, double *out);
 /* C = alpha A + beta B on one shared pattern: combine (csr.hpp:315-326). */
