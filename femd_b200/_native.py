@@ -76,6 +76,7 @@ SIGNATURES = {
     "femd_cuda_cg_jacobi": (_I, [_P, _P, _I, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_cg_solve_host": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_pcg_mixed": (_I, [_P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
+    "femd_cuda_cg_jacobi_noalloc": (_I, [_P, _P, _I, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_host_rectangle_mesh": (_I, [_D, _D, _D, _D, _I, _I, _P, _P]),
     "femd_host_lagrange_numbering": (_I, [_I, _I, _P, _I, _I, _P, _PI, _PI]),
     "femd_host_triangle_quadrature": (_I, [_I, _P, _P, _P]),

@@ -15,6 +15,7 @@
 // HBM bytes per FP64 iteration (n rows, nnz entries): SpMV 12 nnz + 4 (n+1) + 8 n (p) + 8 n (Ap);
 // update 40 n read + 16 n written; direction 24 n read + 8 n written.
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1020,6 +1021,133 @@ int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host, const i
     femd_cuda_release(K);
     femd_cuda_release(P);
     return st;
+}
+
+}  // extern "C"
+
+// ==============================================================================================
+// Jacobi-PCG that allocates nothing.
+//
+// For callers that cannot call cudaMalloc while they solve: a solver embedded in a program whose
+// allocator already owns the device memory (a serving engine that reserved the HBM up front, or a
+// framework whose memory pool must not be bypassed), or a latency-bound loop where an allocation
+// and the device synchronization it may bring are not allowed.  The three work vectors, the
+// reduction partials and the scalar state of the solve live in one fixed static device array,
+// g_cg_scratch, sized for NOALLOC_MAX_ROWS rows; larger systems are rejected.  The kernels and
+// launch shapes are those of femd_cuda_cg_jacobi, so the iterates are the same.
+// ==============================================================================================
+namespace femd {
+
+static constexpr int NOALLOC_MAX_ROWS = 1 << 20;             // 1,048,576 rows
+static constexpr int NOALLOC_PART = 3 * 8192;                // reduction partials (3 per block)
+static constexpr size_t NOALLOC_STATE_DOUBLES = (sizeof(CGState<double>) + sizeof(double) - 1) / sizeof(double);
+static constexpr size_t NOALLOC_DOUBLES = 3 * (size_t)NOALLOC_MAX_ROWS + NOALLOC_PART + NOALLOC_STATE_DOUBLES;
+
+// about 25 MB per device, held by every GPU that loads the library until the process exits
+static __device__ __align__(256) double g_cg_scratch[NOALLOC_DOUBLES];
+
+static constexpr int NOALLOC_MAX_DEVICES = 64;
+static double *g_cg_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+static std::mutex g_cg_scratch_lock;
+
+// The device address of g_cg_scratch on the current device (host code cannot use the symbol
+// itself: on the host it names a stand-in, not device memory).  Looked up once per device.
+static int noalloc_scratch(int device, double **out)
+{
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) {
+        set_error("cg_jacobi_noalloc: device index " + std::to_string(device) + " is out of range");
+        return FEMD_EINVAL;
+    }
+    std::lock_guard<std::mutex> g(g_cg_scratch_lock);
+    if (!g_cg_scratch_addr[device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_cg_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error(std::string("cg_jacobi_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            return FEMD_ECUDA;
+        }
+        g_cg_scratch_addr[device] = static_cast<double *>(p);
+    }
+    *out = g_cg_scratch_addr[device];
+    return FEMD_OK;
+}
+
+}  // namespace femd
+
+extern "C" {
+
+int femd_cuda_cg_jacobi_noalloc(femd_ctx ctx, femd_matrix K, int use_jacobi, const double *b_dev, double *x_dev,
+                                int max_iter, double tol, femd_cg_result *res)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K && res, "cg_jacobi_noalloc: NULL argument");
+    FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "cg_jacobi_noalloc: the matrix must be square");
+    const int n = K->pattern->nrows;
+    FEMD_CHECK_ARG(n <= NOALLOC_MAX_ROWS, "cg_jacobi_noalloc: " + std::to_string(n) + " rows exceed the fixed scratch of " +
+                                              std::to_string(NOALLOC_MAX_ROWS) + " rows; use femd_cuda_cg_jacobi");
+    FEMD_CHECK_ARG(n == 0 || (b_dev && x_dev), "cg_jacobi_noalloc: NULL vector");
+    FEMD_CHECK_ARG(max_iter >= 0, "cg_jacobi_noalloc: max_iter must be >= 0");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
+    if (n == 0) return FEMD_OK;
+    double *base = nullptr;
+    FEMD_TRY(noalloc_scratch(ctx->device, &base));
+    const femd_pattern P = K->pattern;
+    const bool jac = use_jacobi != 0;
+    const int tpr = pick_tpr(K);
+    const unsigned gs = spmv_grid(ctx, n, tpr), gr = red_grid(ctx, n);
+    FEMD_CHECK_ARG(3 * (size_t)std::max(gs, gr) + 3 <= (size_t)NOALLOC_PART,
+                   "cg_jacobi_noalloc: the device has more blocks than the fixed reduction scratch holds");
+    double *r = base, *p = base + NOALLOC_MAX_ROWS, *Ap = base + 2 * (size_t)NOALLOC_MAX_ROWS;
+    double *part = base + 3 * (size_t)NOALLOC_MAX_ROWS;
+    CGState<double> *st = reinterpret_cast<CGState<double> *>(part + NOALLOC_PART);
+    cudaStream_t s = ctx->stream;
+    // the array keeps the previous call's contents: the state (with its reduction ticket) must
+    // start at zero; r, p, Ap and the partials are written before they are read
+    FEMD_TRY_CUDA(cudaMemsetAsync(st, 0, sizeof(CGState<double>), s));
+    launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x_dev, Ap, n, nullptr, nullptr);
+    if (jac) k_cg_start<true><<<gr, RED_BLOCK, 0, counted(s)>>>(b_dev, Ap, r, p, K->inv.p, n, part, st, tol);
+    else k_cg_start<false><<<gr, RED_BLOCK, 0, counted(s)>>>(b_dev, Ap, r, p, nullptr, n, part, st, tol);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&st->max_iter, &max_iter, sizeof(int), cudaMemcpyHostToDevice, s));
+    CGState<double> S;
+    const int CH = 16;
+    const long long max_chunks = (long long)max_iter / CH + 2;
+    for (long long c = 0; c < max_chunks; ++c) {
+        for (int k = 0; k < CH; ++k) {
+            launch_spmv<double, double, true>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, p, Ap, n, part, st);
+            if (jac) {
+                k_cg_update<double, true><<<gr, RED_BLOCK, 0, counted(s)>>>(x_dev, r, p, Ap, K->inv.p, n, part, st, 0);
+                k_cg_direction<double, true><<<gr, RED_BLOCK, 0, counted(s)>>>(p, r, K->inv.p, n, st);
+            } else {
+                k_cg_update<double, false><<<gr, RED_BLOCK, 0, counted(s)>>>(x_dev, r, p, Ap, nullptr, n, part, st, 0);
+                k_cg_direction<double, false><<<gr, RED_BLOCK, 0, counted(s)>>>(p, r, nullptr, n, st);
+            }
+        }
+        FEMD_TRY_CUDA(cudaGetLastError());
+        FEMD_TRY_CUDA(cudaMemcpyAsync(&S, st, sizeof(S), cudaMemcpyDeviceToHost, s));
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+        if (S.done) break;
+    }
+    // final true residual (cg.hpp:222-237)
+    launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x_dev, Ap, n, nullptr, nullptr);
+    k_cg_finish<<<gr, RED_BLOCK, 0, counted(s)>>>(b_dev, Ap, r, n, part, st);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&S, st, sizeof(S), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    if (S.nb == 0.0) {
+        FEMD_TRY_CUDA(cudaMemsetAsync(x_dev, 0, (size_t)n * sizeof(double), s));
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+        return FEMD_OK;
+    }
+    res->iterations = S.it;
+    res->breakdown = S.breakdown;
+    res->residual = S.res64 / S.nb;
+    int conv = !S.breakdown && res->residual <= tol * (1.0 + 1e-6) + 1e-15;
+    if (!conv && !S.breakdown && res->residual <= 10.0 * tol && S.it < max_iter) conv = 1;
+    res->converged = conv;
+    return FEMD_OK;
 }
 
 }  // extern "C"

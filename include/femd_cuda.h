@@ -229,6 +229,21 @@ FEMD_API int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host
 FEMD_API int femd_cuda_pcg_mixed(femd_ctx ctx, femd_matrix K, const double *b_dev, double *x_dev, int max_iter, double tol,
                         femd_cg_result *res);
 
+/* femd_cuda_cg_jacobi without any allocation.  It has no counterpart in the reference.
+ * For callers that cannot call cudaMalloc while they solve: a solver embedded in a program
+ * whose allocator already owns the device memory (a serving engine that reserved the HBM up
+ * front, a framework whose memory pool must not be bypassed), or a latency-bound loop where an
+ * allocation and the device synchronization it may bring are not allowed.  The caller passes
+ * b and x as before; the solver's work vectors, reduction partials and state live in one fixed
+ * static device array (about 25 MB, held by every GPU that loads the library until the process
+ * exits) sized for at most 1,048,576 rows -- larger systems are rejected with FEMD_EINVAL.
+ * The first call on a device looks up that array's device address; make it before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU (any stream or context
+ * of the same device) race and must be serialized.  Same kernels and iterates as
+ * femd_cuda_cg_jacobi; res->seconds is not measured (0). */
+FEMD_API int femd_cuda_cg_jacobi_noalloc(femd_ctx ctx, femd_matrix K, int use_jacobi, const double *b_dev, double *x_dev,
+                                         int max_iter, double tol, femd_cg_result *res);
+
 /* ======================================================================================
  * Host-side setup of the synthetic problems (the reference's own setup code runs on the
  * host too).  No GPU work.
