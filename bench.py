@@ -103,7 +103,7 @@ class Clocks:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
 
@@ -159,12 +159,22 @@ class Problem:
         self.setup_s = time.time() - t0
         self.n, self.nnz = self.V.dim, self.P.nnz
 
-    def step(self):
-        fb = self.fb
+    def step(self, phases=None):
+        fb, torch = self.fb, self.torch
+        s = self.ctx.stream
+        if phases is not None:
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record(s)
         fb.assemble_matrix_2d(self.Qa, self.Qa, [1, 2, 0], [1, 2, 0], [1.0, 1.0, 1.0], self.K)
         fb.assemble_vector_2d(self.Qf, [0], [self.coef_f], self.P, out=self.b)
         M = fb.JacobiPreconditioner(self.K)
+        if phases is not None:
+            ev[1].record(s)
         x, conv, its, res, brk = fb.cg_solve(self.K, M, self.b, None, max(1000, 10 * self.n), TOL)
+        if phases is not None:
+            ev[2].record(s)
+            ev[2].synchronize()
+            phases.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), fb.core.cg_solve.last.seconds * 1e3))
         if not conv:
             raise RuntimeError(f"CG did not converge: {its} iterations, residual {res:.2e}")
         return x, its, res
@@ -206,9 +216,10 @@ def ours(args, rank, world, dist):
     clk = Clocks(local)
     l0 = fb.lib.femd_cuda_kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    phases = []
     e0.record(s)
     for _ in range(args.steps):
-        x, its, res = pr.step()
+        x, its, res = pr.step(phases)
     e1.record(s)
     e1.synchronize()
     barrier()
@@ -217,6 +228,9 @@ def ours(args, rank, world, dist):
     t = e0.elapsed_time(e1) / 1e3
     t_all = _max_over_ranks(torch, dist, t)
     value = world * args.steps / t_all
+    phase_ms = {"assembly_ms": round(sum(p[0] for p in phases) / len(phases), 3),
+                "solve_ms": round(sum(p[1] for p in phases) / len(phases), 3),
+                "cg_device_ms": round(sum(p[2] for p in phases) / len(phases), 3)}
 
     # ---- end to end: host buffers through the public API
     pts_host = torch.from_numpy(pr.mesh.points).pin_memory()
@@ -268,7 +282,7 @@ def ours(args, rank, world, dist):
                                "Jacobi-PCG tol 1e-10", "n": pr.n, "nnz": pr.nnz, "cg_iterations": its,
                    "final_residual": res, "l2": "inputs larger than L2 (CSR 0.58 GB), no flush",
                    "parallelism": f"replicas x{world}", "setup_s": round(pr.setup_s, 2),
-                   "spmv_shape": pr.spmv_shape},
+                   "spmv_shape": pr.spmv_shape, "phases": phase_ms},
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(pr.mesh.points.nbytes),
                 "d2h_bytes_per_step": int(8 * pr.n)},
         "roofline": {"kernel": "k_spmv (FP64 CSR SpMV of the CG loop)", "bound": "hbm", "achieved": round(achieved, 1),

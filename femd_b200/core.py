@@ -68,6 +68,16 @@ class Context:
     def sync(self):
         check(lib.femd_cuda_ctx_sync(self.h))
 
+    def enter(self):
+        """Order the library's stream after the work torch has queued (inputs made by torch)."""
+        torch = _torch()
+        self._stream.wait_stream(torch.cuda.current_stream())
+
+    def leave(self):
+        """Order torch's current stream after the library's work (outputs read by torch)."""
+        torch = _torch()
+        torch.cuda.current_stream().wait_stream(self._stream)
+
     def close(self):
         if self.h:
             lib.femd_cuda_ctx_destroy(self.h)
@@ -296,6 +306,7 @@ def cell_pattern(test: LagrangeSpace2D, trial: LagrangeSpace2D, ctx=None) -> Spa
     ctx = ctx or context()
     dofs = test.cell_dofs_device(ctx)
     h = C.c_void_p()
+    ctx.enter()
     check(lib.femd_cuda_pattern_from_cells(ctx.h, test.dim, test.mesh.ncells, test.nloc, _ptr(dofs), C.byref(h)))
     P = SparsityPattern(h, ctx)
     P.ncells, P.nloc = test.mesh.ncells, test.nloc
@@ -309,6 +320,7 @@ def scatter_map_2d(pattern: SparsityPattern):
     torch = _torch()
     p = C.c_void_p()
     check(lib.femd_cuda_pattern_map(pattern.h, C.byref(p)))
+    pattern.ctx.leave()
     n = pattern.ncells * pattern.nloc * pattern.nloc
     return _wrap_device(p.value, n, torch.int32, pattern.ctx)
 
@@ -338,11 +350,13 @@ class CSRMatrix(_Handle):
         """The values as a torch float64 CUDA tensor view (no copy)."""
         torch = _torch()
         d, _ = self._arrays()
+        self.ctx.leave()
         return _wrap_device(d, self.nnz, torch.float64, self.ctx)
 
     def inv_tensor(self):
         torch = _torch()
         _, i = self._arrays()
+        self.ctx.leave()
         return _wrap_device(i, self.nrows, torch.float64, self.ctx)
 
     @property
@@ -372,7 +386,9 @@ class CSRMatrix(_Handle):
         if x.numel() != self.ncols:
             raise ValueError("matvec: length mismatch")
         y = torch.empty(self.nrows, dtype=torch.float64, device=x.device)
+        self.ctx.enter()
         check(lib.femd_cuda_spmv(self.ctx.h, self.h, _ptr(x), _ptr(y)))
+        self.ctx.leave()
         return y
 
     def autotune_spmv(self, set_best: bool = True):
@@ -505,15 +521,18 @@ def assemble_matrix_2d(QT: Cache2D, QS: Cache2D, a, b, coeffs, K: CSRMatrix, row
     bi = (C.c_int * len(b))(*b)
     mesh = V.mesh.c_struct(K.ctx)
     rule = QT.c_struct()
+    K.ctx.enter()
     check(lib.femd_cuda_assemble_matrix(K.ctx.h, C.byref(mesh), C.byref(rule), K.pattern.h, len(a), ai, bi, carr,
                                         N.ASM_EXACT if exact else N.ASM_FAST, K.h, int(bool(jacobi))))
+    K.ctx.leave()
     K._jacobi = bool(jacobi)
     del keep
     return K
 
 
-def assemble_vector_2d(Q: Cache2D, a, coeffs, pattern: SparsityPattern | None = None, *, exact=True, out=None):
-    """f_i = sum_t integral c_t D^a_t N_i (assembly_2d.hpp:173-211), as a float64 device tensor."""
+def assemble_vector_2d(Q: Cache2D, a, coeffs, pattern: SparsityPattern | None = None, *, exact=False, out=None):
+    """f_i = sum_t integral c_t D^a_t N_i (assembly_2d.hpp:173-211), as a float64 device tensor.
+    exact=True forms every element entry in the reference's operation order."""
     torch = _torch()
     V = Q.space
     P = pattern or V.pattern()
@@ -524,8 +543,10 @@ def assemble_vector_2d(Q: Cache2D, a, coeffs, pattern: SparsityPattern | None = 
     f = out if out is not None else torch.empty(V.dim, dtype=torch.float64, device=f"cuda:{P.ctx.device}")
     mesh = V.mesh.c_struct(P.ctx)
     rule = Q.c_struct()
+    P.ctx.enter()
     check(lib.femd_cuda_assemble_vector(P.ctx.h, C.byref(mesh), C.byref(rule), P.h, len(a), ai, carr,
                                         N.ASM_EXACT if exact else N.ASM_FAST, _ptr(f)))
+    P.ctx.leave()
     del keep
     return f
 
@@ -554,7 +575,7 @@ def cg_solve(A: CSRMatrix, M, b, x0, max_iter: int, tol: float, *, mixed: bool =
         # the preconditioner of another matrix: copy its inverse diagonal into A's slot
         A.inv_tensor().copy_(M.K.inv_tensor())
         A._jacobi = True
-    torch.cuda.current_stream().synchronize()
+    A.ctx.enter()
     res = N.femd_cg_result()
     if mixed:
         if M is None:
@@ -563,6 +584,7 @@ def cg_solve(A: CSRMatrix, M, b, x0, max_iter: int, tol: float, *, mixed: bool =
     else:
         check(lib.femd_cuda_cg_jacobi(A.ctx.h, A.h, int(M is not None), _ptr(bv), _ptr(x), int(max_iter), float(tol),
                                       C.byref(res)))
+    A.ctx.leave()
     cg_solve.last = res
     return x, bool(res.converged), int(res.iterations), float(res.residual), bool(res.breakdown)
 

@@ -280,10 +280,261 @@ __global__ void __launch_bounds__(256) k_assemble_vector(
     }
 }
 
+// ---- FAST path: K3a per-element factors, K3b row-owner accumulation ---------------------------
+// The physical derivative code m of a basis function is sum_r A[m][r] R_r, r = 0 value,
+// 1 d/dxi, 2 d/deta: A[0] = (1, 0, 0), A[1] = (0, Ji0, Ji2), A[2] = (0, Ji1, Ji3).  A matrix
+// form is then Ke(l, j) = sum_{(r,s)} [ F_rs S^{rs}(l, j) + sum_q H_{q,rs} R_r(q,l) R_s(q,j) ]
+// with, per cell,
+//   F_rs    = |det J| sum_{t constant} c_t A[a_t][r] A[b_t][s]          (constant coefficients)
+//   H_{q,rs} = rw_q |det J| sum_{t varying} c_t(q) A[a_t][r] A[b_t][s]   (coefficients at points)
+// and the reference tensors S^{rs}(l, j) = sum_q rw_q R_r(q,l) R_s(q,j) computed on the host.
+// K3a forms F and H once per cell (evaluating closed-form and field coefficients there), K3b
+// walks each row's cells in increasing order and adds the entries in shared memory.
+static constexpr int MAX_PAIRS = 9;
+static constexpr int FAST_BLOCK = 128;
+
+struct FastSpec {
+    int nterms;
+    int a[MAX_TERMS], b[MAX_TERMS];           // b unused for vectors
+    int kind[MAX_TERMS];
+    double cval[MAX_TERMS], p[MAX_TERMS][4];
+    const double *pts[MAX_TERMS];             // FEMD_COEF_POINTS arrays
+    const double *field[MAX_TERMS];           // FEMD_COEF_FIELD vectors
+    int npair, pr[MAX_PAIRS], ps[MAX_PAIRS];  // active (r, s) pairs (matrix) / active r (vector: ps unused)
+    int has_const, has_var, nf;               // factors per cell: npair (const) + nq npair (varying)
+    int vector;
+};
+
+__device__ __forceinline__ double amat(int m, int r, double Ji0, double Ji1, double Ji2, double Ji3)
+{
+    if (m == 0) return r == 0 ? 1.0 : 0.0;
+    if (r == 0) return 0.0;
+    if (m == 1) return r == 1 ? Ji0 : Ji2;
+    return r == 1 ? Ji1 : Ji3;
+}
+
+// coefficient of a varying term at point q of cell e (x, y the physical point)
+__device__ __forceinline__ double coef_at(const FastSpec &fs, int t, int e, int q, int nq, double x, double y,
+                                          const int *__restrict__ dofs, int nloc, const double *__restrict__ ref)
+{
+    switch (fs.kind[t]) {
+    case FEMD_COEF_POINTS: return fs.pts[t][(size_t)e * nq + q];
+    case FEMD_COEF_SINSIN: return fs.p[t][0] + fs.p[t][1] * (sin(fs.p[t][2] * x) * sin(fs.p[t][3] * y));
+    case FEMD_COEF_SINSIN_HELM: {
+        const double s = sin(fs.p[t][2] * x) * sin(fs.p[t][3] * y);
+        return fs.p[t][1] * s + s;
+    }
+    case FEMD_COEF_FIELD: {
+        const double *R = ref + (size_t)q * 3 * nloc;
+        double s = 0.0;
+        for (int l = 0; l < nloc; ++l) {
+            const int d = dofs[(size_t)e * nloc + l];
+            s += R[l] * (d >= 0 ? fs.field[t][d] : 0.0);
+        }
+        return s;
+    }
+    default: return fs.cval[t];
+    }
+}
+
+// K3a: one thread per cell.  tables: rw[nq], xi[nq], eta[nq], ref[nq][3][nloc].
+__global__ void __launch_bounds__(256) k_elem_factors(const double *__restrict__ pts, const int *__restrict__ tris, int ne,
+                                                      int nq, int nloc, const int *__restrict__ dofs,
+                                                      const double *__restrict__ tables, FastSpec fs,
+                                                      double *__restrict__ factors)
+{
+    const double *rw = tables, *qxi = tables + nq, *qeta = tables + 2 * nq, *ref = tables + 3 * nq;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) {
+        const int v0 = tris[3 * e], v1 = tris[3 * e + 1], v2 = tris[3 * e + 2];
+        const double x0 = pts[2 * v0], y0 = pts[2 * v0 + 1];
+        const double J0 = pts[2 * v1] - x0, J1 = pts[2 * v2] - x0, J2 = pts[2 * v1 + 1] - y0, J3 = pts[2 * v2 + 1] - y0;
+        const double d = J0 * J3 - J1 * J2, ad = fabs(d);
+        const double Ji0 = J3 / d, Ji1 = -J1 / d, Ji2 = -J2 / d, Ji3 = J0 / d;
+        double *F = factors + (size_t)e * fs.nf;
+        int o = 0;
+        if (fs.has_const) {
+            for (int k = 0; k < fs.npair; ++k) {
+                double acc = 0.0;
+                for (int t = 0; t < fs.nterms; ++t) {
+                    if (fs.kind[t] != FEMD_COEF_CONST) continue;
+                    const double ar = amat(fs.a[t], fs.pr[k], Ji0, Ji1, Ji2, Ji3);
+                    const double bs = fs.vector ? 1.0 : amat(fs.b[t], fs.ps[k], Ji0, Ji1, Ji2, Ji3);
+                    acc += fs.cval[t] * ar * bs;
+                }
+                F[o++] = ad * acc;
+            }
+        }
+        if (fs.has_var) {
+            for (int q = 0; q < nq; ++q) {
+                const double x = x0 + J0 * qxi[q] + J1 * qeta[q], y = y0 + J2 * qxi[q] + J3 * qeta[q];
+                double c[MAX_TERMS];
+                for (int t = 0; t < fs.nterms; ++t)
+                    c[t] = fs.kind[t] == FEMD_COEF_CONST ? 0.0 : coef_at(fs, t, e, q, nq, x, y, dofs, nloc, ref);
+                const double wq = rw[q] * ad;
+                for (int k = 0; k < fs.npair; ++k) {
+                    double acc = 0.0;
+                    for (int t = 0; t < fs.nterms; ++t) {
+                        if (fs.kind[t] == FEMD_COEF_CONST) continue;
+                        const double ar = amat(fs.a[t], fs.pr[k], Ji0, Ji1, Ji2, Ji3);
+                        const double bs = fs.vector ? 1.0 : amat(fs.b[t], fs.ps[k], Ji0, Ji1, Ji2, Ji3);
+                        acc += c[t] * ar * bs;
+                    }
+                    F[o++] = wq * acc;
+                }
+            }
+        }
+    }
+}
+
+// K3b: one thread per row, the row's values accumulated in shared memory (acc[k][thread]) in
+// increasing cell order, then written out by each warp as one contiguous, coalesced range.
+// smem: S[npair][nloc][nloc] (const part), R[nq][3][nloc] (varying part), acc[maxlen][FAST_BLOCK],
+// rlo[FAST_BLOCK + 4 per warp].
+__global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows(
+    const int *__restrict__ indptr, const int *__restrict__ rc_ptr, const int *__restrict__ rc_code,
+    const int *__restrict__ map, const int *__restrict__ diag_pos, int nrows, int nloc, int nq,
+    const double *__restrict__ factors, const double *__restrict__ g_S, const double *__restrict__ g_R, FastSpec fs,
+    int maxlen, double *__restrict__ data, double *__restrict__ inv, int *__restrict__ status)
+{
+    extern __shared__ double smem[];
+    const int nl2 = nloc * nloc;
+    double *sS = smem;                                        // npair * nl2 (const)
+    double *sR = sS + (fs.has_const ? fs.npair * nl2 : 0);    // nq * 3 * nloc (varying)
+    double *acc = sR + (fs.has_var ? nq * 3 * nloc : 0);      // maxlen * FAST_BLOCK
+    int *srlo = reinterpret_cast<int *>(acc + (size_t)maxlen * FAST_BLOCK);   // FAST_BLOCK + 1 per block... per warp 33
+    if (fs.has_const)
+        for (int t = threadIdx.x; t < fs.npair * nl2; t += blockDim.x) sS[t] = g_S[t];
+    if (fs.has_var)
+        for (int t = threadIdx.x; t < nq * 3 * nloc; t += blockDim.x) sR[t] = g_R[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int *wrlo = srlo + w * 33;
+    // the loop bound is uniform per warp: rows are handed out 32 at a time
+    for (int i0 = (blockIdx.x * FAST_BLOCK + w * 32); i0 < nrows; i0 += gridDim.x * FAST_BLOCK) {
+        const int i = i0 + lane;
+        const bool valid = i < nrows;
+        const int rlo = valid ? indptr[i] : 0;
+        const int len = valid ? indptr[i + 1] - rlo : 0;
+        double *a = acc + threadIdx.x;                        // a[k * FAST_BLOCK]
+        for (int k = 0; k < len; ++k) a[k * FAST_BLOCK] = 0.0;
+        if (valid) {
+            for (int c = rc_ptr[i]; c < rc_ptr[i + 1]; ++c) {
+                const int code = rc_code[c];
+                const int e = code / nloc, l = code - e * nloc;
+                const double *F = factors + (size_t)e * fs.nf;
+                double Fc[MAX_PAIRS];
+                if (fs.has_const)
+                    for (int k = 0; k < fs.npair; ++k) Fc[k] = F[k];
+                const double *H = F + (fs.has_const ? fs.npair : 0);
+                const int *mrow = map + (size_t)code * nloc;
+                for (int j = 0; j < nloc; ++j) {
+                    const int pos = mrow[j];
+                    if (pos < 0) continue;
+                    double v = 0.0;
+                    if (fs.has_const)
+                        for (int k = 0; k < fs.npair; ++k) v += Fc[k] * sS[k * nl2 + l * nloc + j];
+                    if (fs.has_var)
+                        for (int q = 0; q < nq; ++q) {
+                            const double *R = sR + q * 3 * nloc;
+                            for (int k = 0; k < fs.npair; ++k)
+                                v += H[q * fs.npair + k] * R[fs.pr[k] * nloc + l] * R[fs.ps[k] * nloc + j];
+                        }
+                    a[(pos - rlo) * FAST_BLOCK] += v;
+                }
+            }
+            if (inv) {
+                const int dp = diag_pos[i];
+                if (dp < 0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
+                else {
+                    const double dv = a[(dp - rlo) * FAST_BLOCK];
+                    if (dv == 0.0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
+                    inv[i] = 1.0 / dv;
+                }
+            }
+        }
+        // coalesced write-out of the warp's 32 rows: positions [first, last)
+        wrlo[lane] = valid ? rlo : (i0 < nrows ? indptr[nrows] : 0);
+        if (lane == 31) wrlo[32] = valid ? rlo + len : indptr[nrows];
+        __syncwarp();
+        const int first = wrlo[0], last = wrlo[32];
+        for (int p = first + lane; p < last; p += 32) {
+            int lo = 0, hi = 31;          // the row t with wrlo[t] <= p < wrlo[t + 1]
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (wrlo[mid] <= p) lo = mid; else hi = mid - 1;
+            }
+            data[p] = acc[(size_t)(p - wrlo[lo]) * FAST_BLOCK + w * 32 + lo];
+        }
+        __syncwarp();
+    }
+}
+
+// K4 FAST: one thread per row, f_i = sum over the row's cells (increasing order) of
+// sum_k F_k R_{r_k}(l) (constant) + sum_q sum_k H_{q,k} R_{r_k}(q, l) (varying), where the
+// constant part uses the tabulation integrated against the weights (Sv^{r}(l) = sum_q rw_q R_r(q,l)).
+__global__ void __launch_bounds__(256) k_assemble_vector_fast(const int *__restrict__ rc_ptr, const int *__restrict__ rc_code,
+                                                              int nrows, int nloc, int nq, const double *__restrict__ factors,
+                                                              const double *__restrict__ g_Sv, const double *__restrict__ g_R,
+                                                              FastSpec fs, double *__restrict__ f)
+{
+    extern __shared__ double smem[];
+    double *sSv = smem;                        // 3 * nloc
+    double *sR = sSv + 3 * nloc;               // nq * 3 * nloc
+    for (int t = threadIdx.x; t < 3 * nloc; t += blockDim.x) sSv[t] = g_Sv[t];
+    for (int t = threadIdx.x; t < nq * 3 * nloc; t += blockDim.x) sR[t] = g_R[t];
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x) {
+        double fi = 0.0;
+        for (int c = rc_ptr[i]; c < rc_ptr[i + 1]; ++c) {
+            const int code = rc_code[c];
+            const int e = code / nloc, l = code - e * nloc;
+            const double *F = factors + (size_t)e * fs.nf;
+            double v = 0.0;
+            int o = 0;
+            if (fs.has_const)
+                for (int k = 0; k < fs.npair; ++k) v += F[o++] * sSv[fs.pr[k] * nloc + l];
+            if (fs.has_var)
+                for (int q = 0; q < nq; ++q)
+                    for (int k = 0; k < fs.npair; ++k) v += F[o++] * sR[(q * 3 + fs.pr[k]) * nloc + l];
+            fi += v;
+        }
+        f[i] = fi;
+    }
+}
+
 // ---- host side -----------------------------------------------------------------------------
 struct RuleDev {
     DevBuf<double> ref, rw, S, xi, eta;
 };
+
+// Active (r, s) pairs of a form, and the factor count per cell.
+static void fast_spec(int nterms, const int *a, const int *b, const femd_coef *coef, int nq, bool vector, FastSpec &fs)
+{
+    fs = FastSpec{};
+    fs.nterms = nterms;
+    fs.vector = vector ? 1 : 0;
+    bool act[3][3] = {};
+    for (int t = 0; t < nterms; ++t) {
+        fs.a[t] = a[t];
+        fs.b[t] = b ? b[t] : 0;
+        fs.kind[t] = coef[t].kind;
+        fs.cval[t] = coef[t].value;
+        for (int u = 0; u < 4; ++u) fs.p[t][u] = coef[t].p[u];
+        fs.pts[t] = coef[t].points_dev;
+        fs.field[t] = coef[t].field_dev;
+        if (coef[t].kind == FEMD_COEF_CONST) fs.has_const = 1; else fs.has_var = 1;
+        for (int r = 0; r < 3; ++r)
+            for (int s = 0; s < 3; ++s) {
+                const bool ra = a[t] == 0 ? r == 0 : r != 0;
+                const bool sb = vector ? s == 0 : (b[t] == 0 ? s == 0 : s != 0);
+                if (ra && sb) act[r][s] = true;
+            }
+    }
+    for (int r = 0; r < 3; ++r)
+        for (int s = 0; s < 3; ++s)
+            if (act[r][s]) { fs.pr[fs.npair] = r; fs.ps[fs.npair] = s; ++fs.npair; }
+    fs.nf = (fs.has_const ? fs.npair : 0) + (fs.has_var ? nq * fs.npair : 0);
+}
 
 static int check_common(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p, int nterms,
                         const int *a, const int *b, const femd_coef *coef, int mode)
@@ -385,6 +636,90 @@ static int prepare_terms(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
     return FEMD_OK;
 }
 
+static constexpr int FAST_MAX_ROW = 96;   // longest row the shared-memory accumulator holds
+
+// FAST assembly of a matrix (K non-null) or a vector (f non-null).  Tables and factors live in
+// the pattern's workspace; no allocation once the workspace has its size.
+static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p, int nterms,
+                         const int *a, const int *b, const femd_coef *coef, femd_matrix K, int want_inv, double *f)
+{
+    cudaStream_t s = ctx->stream;
+    const bool vector = K == nullptr;
+    const int nq = rule->nq, nl = rule->nloc, nl2 = nl * nl, n = p->nrows, ne = p->ncells;
+    FastSpec fs;
+    fast_spec(nterms, a, b, coef, nq, vector, fs);
+    // host tables: [rw | xi | eta | ref (nq 3 nl) | S (npair nl^2) or Sv (3 nl)]
+    const size_t nref = (size_t)nq * 3 * nl;
+    const size_t nS = vector ? (size_t)3 * nl : (size_t)fs.npair * nl2;
+    std::vector<double> tab(3 * (size_t)nq + nref + nS, 0.0);
+    for (int q = 0; q < nq; ++q) { tab[q] = rule->w_host[q]; tab[nq + q] = rule->xi_host[q]; tab[2 * nq + q] = rule->eta_host[q]; }
+    std::copy(rule->ref_host, rule->ref_host + nref, tab.begin() + 3 * nq);
+    double *S = tab.data() + 3 * nq + nref;
+    if (vector) {
+        for (int r = 0; r < 3; ++r)
+            for (int l = 0; l < nl; ++l) {
+                double acc = 0.0;
+                for (int q = 0; q < nq; ++q) acc += rule->w_host[q] * rule->ref_host[((size_t)q * 3 + r) * nl + l];
+                S[r * nl + l] = acc;
+            }
+    } else {
+        for (int k = 0; k < fs.npair; ++k)
+            for (int l = 0; l < nl; ++l)
+                for (int j = 0; j < nl; ++j) {
+                    double acc = 0.0;
+                    for (int q = 0; q < nq; ++q) {
+                        const double *Rq = rule->ref_host + (size_t)q * 3 * nl;
+                        acc += rule->w_host[q] * Rq[fs.pr[k] * nl + l] * Rq[fs.ps[k] * nl + j];
+                    }
+                    S[(size_t)k * nl2 + l * nl + j] = acc;
+                }
+    }
+    if (p->ws_tables.n < tab.size()) FEMD_TRY(p->ws_tables.alloc(tab.size()));
+    if (p->ws_factors.n < (size_t)ne * fs.nf + 1) FEMD_TRY(p->ws_factors.alloc((size_t)ne * fs.nf + 1));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(p->ws_tables.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    const double *d_ref = p->ws_tables.p + 3 * nq, *d_S = d_ref + nref;
+    if (ne)
+        k_elem_factors<<<grid_for((size_t)ne, 256, 1u << 22), 256, 0, counted(s)>>>(
+            mesh->points_dev, mesh->tris_dev, ne, nq, nl, p->cell_dofs.p, p->ws_tables.p, fs, p->ws_factors.p);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    if (vector) {
+        const size_t shm = (3 * (size_t)nl + nref) * sizeof(double);
+        if (n) {
+            cudaFuncSetAttribute(k_assemble_vector_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            k_assemble_vector_fast<<<grid_for((size_t)n, 256, 1u << 22), 256, shm, counted(s)>>>(
+                p->rc_ptr.p, p->rc_code.p, n, nl, nq, p->ws_factors.p, d_S, d_ref, fs, f);
+        }
+        FEMD_TRY_CUDA(cudaGetLastError());
+        return FEMD_OK;
+    }
+    FEMD_TRY(reset_status(ctx));
+    double *inv = nullptr;
+    if (want_inv) {
+        if (!K->inv.p) FEMD_TRY(K->inv.alloc((size_t)n + 1));
+        inv = K->inv.p;
+    }
+    const int maxlen = std::max(p->max_row_len, 1);
+    const size_t shm = ((fs.has_const ? (size_t)fs.npair * nl2 : 0) + (fs.has_var ? nref : 0) + (size_t)maxlen * FAST_BLOCK) *
+                           sizeof(double) + (FAST_BLOCK / 32) * 33 * sizeof(int);
+    if (n) {
+        cudaFuncSetAttribute(k_assemble_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        k_assemble_rows<<<grid_for((size_t)n, FAST_BLOCK, 1u << 22), FAST_BLOCK, shm, counted(s)>>>(
+            p->indptr.p, p->rc_ptr.p, p->rc_code.p, p->map.p, p->diag_pos.p, n, nl, nq, p->ws_factors.p, d_S, d_ref, fs,
+            maxlen, K->data.p, inv, ctx->status_dev);
+    }
+    FEMD_TRY_CUDA(cudaGetLastError());
+    K->f32_valid = false;
+    if (want_inv) {
+        int flags = 0, bad = 0;
+        FEMD_TRY(read_status(ctx, &flags, &bad));
+        if (flags & ST_ZERODIAG) {
+            set_error("Jacobi: zero diagonal entry in row " + std::to_string(bad));
+            return FEMD_EZERODIAG;
+        }
+    }
+    return FEMD_OK;
+}
+
 }  // namespace femd
 
 using namespace femd;
@@ -401,6 +736,8 @@ int femd_cuda_assemble_matrix(femd_ctx ctx, const femd_mesh2d *mesh, const femd_
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     FEMD_TRY(build_scatter_map(ctx, p));
+    if (mode == FEMD_ASM_FAST && p->max_row_len <= FAST_MAX_ROW)
+        return fast_assemble(ctx, mesh, rule, p, nterms, a, b, coef, K, want_inv, nullptr);
     RuleDev R;
     FEMD_TRY(upload_rule(rule, mode == FEMD_ASM_FAST, R, s));
     DevBuf<double> scratch;
@@ -449,6 +786,7 @@ int femd_cuda_assemble_vector(femd_ctx ctx, const femd_mesh2d *mesh, const femd_
     FEMD_CHECK_ARG(p->nrows == 0 || f_dev, "assemble_vector_2d: f is NULL");
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
+    if (mode == FEMD_ASM_FAST) return fast_assemble(ctx, mesh, rule, p, nterms, a, nullptr, coef, nullptr, 0, f_dev);
     RuleDev R;
     FEMD_TRY(upload_rule(rule, false, R, s));
     DevBuf<double> scratch;

@@ -95,6 +95,9 @@ struct femd_pattern_s : femd::HandleBase {
     femd::DevBuf<int> map;             // scatter map, ne nloc^2 (built on demand)
     femd::DevBuf<int> diag_pos;        // position of (i, i), -1 when absent
     int max_row_cells = 0, max_row_len = 0;
+    // assembly workspace, grown on demand and reused across calls (no allocation per call
+    // once it has its size): per-element factors, the rule's tables
+    femd::DevBuf<double> ws_factors, ws_tables;
     femd_pattern_s() : HandleBase(femd::KIND_PATTERN) {}
 };
 
@@ -105,7 +108,12 @@ struct femd_matrix_s : femd::HandleBase {
     femd::DevBuf<float> data32, inv32;   // FP32 copies (mixed precision), built on demand
     bool f32_valid = false;
     int spmv_tpr = 0;                    // autotuned threads per row (0: not tuned)
+    // the solver workspace of this matrix (vectors, pinned state, captured CUDA graphs), kept
+    // between solves so that a solve allocates nothing once it has run once
+    void *solver_ws = nullptr;
+    void (*solver_ws_free)(void *) = nullptr;
     femd_matrix_s() : HandleBase(femd::KIND_MATRIX) {}
+    ~femd_matrix_s() override { if (solver_ws_free) solver_ws_free(solver_ws); }
 };
 
 namespace femd {

@@ -15,6 +15,7 @@
 // HBM bytes per FP64 iteration (n rows, nnz entries): SpMV 12 nnz + 4 (n+1) + 8 n (p) + 8 n (Ap);
 // update 40 n read + 16 n written; direction 24 n read + 8 n written.
 #include <cmath>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -485,98 +486,162 @@ unsigned spmv_grid(femd_ctx ctx, int n, int shape)
     return grid_for((size_t)n, gpb, cap);
 }
 
-// One CG solve (FP64) on device vectors.  Workspace: r, p, Ap (n each), partials, state.
-struct CGWork {
-    DevBuf<double> r, p, Ap, part;
+// The solver workspace of a matrix: vectors, reduction partials, device and pinned host state,
+// events, and the CUDA graphs of a chunk of iterations.  The graphs run on the workspace's own
+// solution and right-hand-side vectors (wx, wb), so their pointers never change and a graph is
+// captured once per matrix; a solve copies b and x0 in and x out.  After the first solve on a
+// matrix, a solve makes no allocation, capture or instantiation.
+struct SolverWS {
+    int n = 0, shape = 0;
+    unsigned gs = 0, gr = 0;
+    // FP64
+    DevBuf<double> r, p, Ap, part, wx, wb;
     DevBuf<CGState<double>> st;
     CGState<double> *st_host = nullptr;
-    ~CGWork() { if (st_host) cudaFreeHost(st_host); }
+    int *maxit_host = nullptr;
+    cudaGraphExec_t x64[2] = {nullptr, nullptr};
+    size_t nodes64[2] = {0, 0};
+    int ch64 = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, ev[2] = {nullptr, nullptr};
+    // mixed precision
+    bool mixed_ready = false;
+    DevBuf<double> Ax64, r64, part64;
+    DevBuf<float> r32, p32, Ap32, d32, part32;
+    DevBuf<CGState<float>> st32;
+    CGState<float> *st32_host = nullptr;
+    cudaGraphExec_t xm = nullptr;
+    size_t nodesm = 0;
+    int chm = 0;
+    ~SolverWS()
+    {
+        for (auto &g : x64) if (g) cudaGraphExecDestroy(g);
+        if (xm) cudaGraphExecDestroy(xm);
+        for (cudaEvent_t e : {e0, e1, ev[0], ev[1]}) if (e) cudaEventDestroy(e);
+        if (st_host) cudaFreeHost(st_host);
+        if (maxit_host) cudaFreeHost(maxit_host);
+        if (st32_host) cudaFreeHost(st32_host);
+    }
 };
 
+static void solver_ws_free(void *w) { delete static_cast<SolverWS *>(w); }
+
+static int get_ws(femd_ctx ctx, femd_matrix K, SolverWS **out)
+{
+    const int n = K->pattern->nrows, shape = pick_tpr(K);
+    SolverWS *W = static_cast<SolverWS *>(K->solver_ws);
+    if (W && W->n == n && W->shape == shape) { *out = W; return FEMD_OK; }
+    if (W) { solver_ws_free(W); K->solver_ws = nullptr; K->solver_ws_free = nullptr; }
+    W = new SolverWS();
+    std::unique_ptr<SolverWS> guard(W);
+    W->n = n;
+    W->shape = shape;
+    W->gs = spmv_grid(ctx, n, shape);
+    W->gr = red_grid(ctx, n);
+    for (DevBuf<double> *b : {&W->r, &W->p, &W->Ap, &W->wx, &W->wb}) FEMD_TRY(b->alloc((size_t)n + 1));
+    FEMD_TRY(W->part.alloc(3 * (size_t)std::max(W->gs, W->gr) + 3));
+    FEMD_TRY(W->st.alloc(1));
+    FEMD_TRY_CUDA(cudaMallocHost(&W->st_host, sizeof(CGState<double>)));
+    FEMD_TRY_CUDA(cudaMallocHost(&W->maxit_host, sizeof(int)));
+    FEMD_TRY_CUDA(cudaEventCreate(&W->e0));
+    FEMD_TRY_CUDA(cudaEventCreate(&W->e1));
+    FEMD_TRY_CUDA(cudaEventCreateWithFlags(&W->ev[0], cudaEventDisableTiming));
+    FEMD_TRY_CUDA(cudaEventCreateWithFlags(&W->ev[1], cudaEventDisableTiming));
+    W->ch64 = n > (1 << 18) ? 8 : 32;
+    K->solver_ws = guard.release();
+    K->solver_ws_free = solver_ws_free;
+    *out = W;
+    return FEMD_OK;
+}
+
+// Capture CH iterations of the FP64 loop on the workspace vectors (once per matrix and variant).
+static int capture_cg64(femd_ctx ctx, femd_matrix K, SolverWS &W, bool jac)
+{
+    if (W.x64[jac]) return FEMD_OK;
+    femd_pattern P = K->pattern;
+    cudaStream_t s = ctx->stream;
+    const int n = W.n;
+    cudaGraph_t graph = nullptr;
+    FEMD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < W.ch64; ++k) {
+        launch_spmv<double, double, true>(W.shape, W.gs, s, P->indptr.p, P->indices.p, K->data.p, W.p.p, W.Ap.p, n, W.part.p,
+                                          W.st.p);
+        if (jac) {
+            k_cg_update<double, true><<<W.gr, RED_BLOCK, 0, counted(s)>>>(W.wx.p, W.r.p, W.p.p, W.Ap.p, K->inv.p, n, W.part.p,
+                                                                          W.st.p, 0);
+            k_cg_direction<double, true><<<W.gr, RED_BLOCK, 0, counted(s)>>>(W.p.p, W.r.p, K->inv.p, n, W.st.p);
+        } else {
+            k_cg_update<double, false><<<W.gr, RED_BLOCK, 0, counted(s)>>>(W.wx.p, W.r.p, W.p.p, W.Ap.p, nullptr, n, W.part.p,
+                                                                           W.st.p, 0);
+            k_cg_direction<double, false><<<W.gr, RED_BLOCK, 0, counted(s)>>>(W.p.p, W.r.p, nullptr, n, W.st.p);
+        }
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) { set_error(std::string("cg: graph capture: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
+    ce = cudaGraphInstantiate(&W.x64[jac], graph, 0);
+    cudaGraphGetNodes(graph, nullptr, &W.nodes64[jac]);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) { W.x64[jac] = nullptr; set_error(std::string("cg: graph instantiate: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
+    return FEMD_OK;
+}
+
+// One FP64 CG solve (cg.hpp:296-350) on the matrix's workspace.
 static int cg_run(femd_ctx ctx, femd_matrix K, bool jac, const double *b, double *x, int max_iter, double tol,
                   femd_cg_result *res)
 {
     femd_pattern P = K->pattern;
     const int n = P->nrows;
     cudaStream_t s = ctx->stream;
-    CGWork W;
-    FEMD_TRY(W.r.alloc(n + 1));
-    FEMD_TRY(W.p.alloc(n + 1));
-    FEMD_TRY(W.Ap.alloc(n + 1));
-    const int tpr = pick_tpr(K);
-    const unsigned gs = spmv_grid(ctx, n, tpr), gr = red_grid(ctx, n);
-    FEMD_TRY(W.part.alloc(3 * (size_t)std::max(gs, gr) + 3));
-    FEMD_TRY(W.st.alloc(1));
-    FEMD_TRY_CUDA(cudaMallocHost(&W.st_host, sizeof(CGState<double>)));
+    SolverWS *Wp = nullptr;
+    FEMD_TRY(get_ws(ctx, K, &Wp));
+    SolverWS &W = *Wp;
+    FEMD_TRY(capture_cg64(ctx, K, W, jac));
+    const unsigned gs = W.gs, gr = W.gr;
+    const int CH = W.ch64;
+    *W.maxit_host = max_iter;
+    FEMD_TRY_CUDA(cudaEventRecord(W.e0, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.wb.p, b, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.wx.p, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     FEMD_TRY_CUDA(cudaMemsetAsync(W.st.p, 0, sizeof(CGState<double>), s));
-    cudaEvent_t e0, e1;
-    FEMD_TRY_CUDA(cudaEventCreate(&e0));
-    FEMD_TRY_CUDA(cudaEventCreate(&e1));
-    FEMD_TRY_CUDA(cudaEventRecord(e0, s));
     // start (cg.hpp:305-320)
-    launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x, W.Ap.p, n, nullptr, nullptr);
-    if (jac) k_cg_start<true><<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ap.p, W.r.p, W.p.p, K->inv.p, n, W.part.p, W.st.p, tol);
-    else k_cg_start<false><<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ap.p, W.r.p, W.p.p, nullptr, n, W.part.p, W.st.p, tol);
+    launch_spmv<double, double, false>(W.shape, gs, s, P->indptr.p, P->indices.p, K->data.p, W.wx.p, W.Ap.p, n, nullptr, nullptr);
+    if (jac) k_cg_start<true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.wb.p, W.Ap.p, W.r.p, W.p.p, K->inv.p, n, W.part.p, W.st.p, tol);
+    else k_cg_start<false><<<gr, RED_BLOCK, 0, counted(s)>>>(W.wb.p, W.Ap.p, W.r.p, W.p.p, nullptr, n, W.part.p, W.st.p, tol);
     FEMD_TRY_CUDA(cudaGetLastError());
-    // set max_iter on the device state (after start zeroed the counters)
-    {
-        CGState<double> init{};
-        (void)init;
-    }
-    FEMD_TRY_CUDA(cudaMemcpyAsync(&W.st.p->max_iter, &max_iter, sizeof(int), cudaMemcpyHostToDevice, s));
-    // the loop, in chunks of CH iterations captured once in a CUDA graph
-    const int CH = n > (1 << 18) ? 8 : 32;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    FEMD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < CH; ++k) {
-        launch_spmv<double, double, true>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, W.p.p, W.Ap.p, n, W.part.p, W.st.p);
-        if (jac) {
-            k_cg_update<double, true><<<gr, RED_BLOCK, 0, counted(s)>>>(x, W.r.p, W.p.p, W.Ap.p, K->inv.p, n, W.part.p, W.st.p, 0);
-            k_cg_direction<double, true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.p.p, W.r.p, K->inv.p, n, W.st.p);
-        } else {
-            k_cg_update<double, false><<<gr, RED_BLOCK, 0, counted(s)>>>(x, W.r.p, W.p.p, W.Ap.p, nullptr, n, W.part.p, W.st.p, 0);
-            k_cg_direction<double, false><<<gr, RED_BLOCK, 0, counted(s)>>>(W.p.p, W.r.p, nullptr, n, W.st.p);
-        }
-    }
-    cudaError_t ce = cudaStreamEndCapture(s, &graph);
-    if (ce != cudaSuccess) { set_error(std::string("cg: graph capture: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
-    ce = cudaGraphInstantiate(&exec, graph, 0);
-    if (ce != cudaSuccess) { cudaGraphDestroy(graph); set_error(std::string("cg: graph instantiate: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
-    size_t nodes = 0;
-    cudaGraphGetNodes(graph, nullptr, &nodes);
-    // poll the state between chunks; keep one chunk queued ahead
-    cudaEvent_t ev[2];
-    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    // max_iter on the device state (after start zeroed the counters)
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&W.st.p->max_iter, W.maxit_host, sizeof(int), cudaMemcpyHostToDevice, s));
+    // the loop, in chunks of CH iterations (one graph launch each); poll the state between
+    // chunks, keeping one chunk queued ahead
     int status = FEMD_OK;
     long long launched = 0;
     const long long max_chunks = (long long)max_iter / CH + 2;
-    ce = launch_graph(exec, nodes, s);
+    cudaGraphExec_t exec = W.x64[jac];
+    const size_t nodes = W.nodes64[jac];
+    cudaError_t ce = launch_graph(exec, nodes, s);
     if (ce == cudaSuccess) ce = cudaMemcpyAsync(W.st_host, W.st.p, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s);
-    if (ce == cudaSuccess) ce = cudaEventRecord(ev[0], s);
+    if (ce == cudaSuccess) ce = cudaEventRecord(W.ev[0], s);
     launched = 1;
     while (ce == cudaSuccess) {
-        // queue the next chunk before looking at the previous one
         if (launched < max_chunks) {
             ce = launch_graph(exec, nodes, s);
             if (ce != cudaSuccess) break;
         }
-        ce = cudaEventSynchronize(ev[(launched - 1) & 1]);
+        ce = cudaEventSynchronize(W.ev[(launched - 1) & 1]);
         if (ce != cudaSuccess) break;
         if (W.st_host->done) break;
         if (launched >= max_chunks) break;
         ce = cudaMemcpyAsync(W.st_host, W.st.p, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s);
-        if (ce == cudaSuccess) ce = cudaEventRecord(ev[launched & 1], s);
+        if (ce == cudaSuccess) ce = cudaEventRecord(W.ev[launched & 1], s);
         ++launched;
     }
     if (ce != cudaSuccess) { set_error(std::string("cg: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; }
     // finish (cg.hpp:222-237)
     if (status == FEMD_OK) {
-        launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x, W.Ap.p, n, nullptr, nullptr);
-        k_cg_finish<<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ap.p, W.r.p, n, W.part.p, W.st.p);
-        cudaEventRecord(e1, s);
+        launch_spmv<double, double, false>(W.shape, gs, s, P->indptr.p, P->indices.p, K->data.p, W.wx.p, W.Ap.p, n, nullptr,
+                                           nullptr);
+        k_cg_finish<<<gr, RED_BLOCK, 0, counted(s)>>>(W.wb.p, W.Ap.p, W.r.p, n, W.part.p, W.st.p);
         ce = cudaMemcpyAsync(W.st_host, W.st.p, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(x, W.wx.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (ce == cudaSuccess) ce = cudaEventRecord(W.e1, s);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
         if (ce != cudaSuccess) { set_error(std::string("cg: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; }
     }
@@ -597,13 +662,9 @@ static int cg_run(femd_ctx ctx, femd_matrix K, bool jac, const double *b, double
         res->status = FEMD_OK;
         res->outer = 0;
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventElapsedTime(&ms, W.e0, W.e1);
         res->seconds = ms * 1e-3;
     }
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    cudaEventDestroy(ev[0]); cudaEventDestroy(ev[1]);
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
     return status;
 }
 
@@ -621,41 +682,83 @@ static int ensure_f32(femd_ctx ctx, femd_matrix K)
     return FEMD_OK;
 }
 
-// Mixed precision solve: inner FP32 Jacobi-PCG with reliable FP64 updates.
-static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b, double *x, int max_iter, double tol, femd_cg_result *res)
+// The mixed-precision buffers of the workspace and the graph of a chunk (once per matrix).
+static int prepare_mixed(femd_ctx ctx, femd_matrix K, SolverWS &W)
+{
+    if (W.mixed_ready) return FEMD_OK;
+    femd_pattern P = K->pattern;
+    cudaStream_t s = ctx->stream;
+    const int n = W.n;
+    const size_t npart = 3 * (size_t)std::max(W.gs, W.gr) + 3;
+    for (DevBuf<double> *b : {&W.Ax64, &W.r64}) FEMD_TRY(b->alloc((size_t)n + 1));
+    for (DevBuf<float> *b : {&W.r32, &W.p32, &W.Ap32, &W.d32}) FEMD_TRY(b->alloc((size_t)n + 1));
+    FEMD_TRY(W.part64.alloc(npart));
+    FEMD_TRY(W.part32.alloc(npart));
+    FEMD_TRY(W.st32.alloc(1));
+    FEMD_TRY_CUDA(cudaMallocHost(&W.st32_host, sizeof(CGState<float>)));
+    W.chm = n > (1 << 18) ? 8 : 16;
+    const unsigned gs = W.gs, gr = W.gr;
+    double *x = W.wx.p;
+    const double *b = W.wb.p;
+    cudaGraph_t graph = nullptr;
+    FEMD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < W.chm; ++k) {
+        launch_spmv<float, float, true>(W.shape, gs, s, P->indptr.p, P->indices.p, K->data32.p, W.p32.p, W.Ap32.p, n,
+                                        W.part32.p, W.st32.p);
+        k_cg_update<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.d32.p, W.r32.p, W.p32.p, W.Ap32.p, K->inv32.p, n, W.part32.p,
+                                                                   W.st32.p, 1);
+        // a reliable update (when requested) before the direction update uses r
+        k_mixed_flush<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, W.d32.p, n, W.st32.p);
+        switch (shape_tpr(W.shape)) {
+        case 2: k_mixed_spmv64<2><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+        case 4: k_mixed_spmv64<4><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+        case 8: k_mixed_spmv64<8><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+        case 16: k_mixed_spmv64<16><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+        default: k_mixed_spmv64<32><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+        }
+        k_mixed_residual<<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ax64.p, W.r32.p, K->inv32.p, n, W.part64.p, W.part32.p, W.st32.p);
+        k_cg_direction<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.p32.p, W.r32.p, K->inv32.p, n, W.st32.p);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) { set_error(std::string("pcg_mixed: graph capture: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
+    ce = cudaGraphInstantiate(&W.xm, graph, 0);
+    cudaGraphGetNodes(graph, nullptr, &W.nodesm);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) { W.xm = nullptr; set_error(std::string("pcg_mixed: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
+    W.mixed_ready = true;
+    return FEMD_OK;
+}
+
+// Mixed precision solve: inner FP32 Jacobi-PCG with reliable FP64 updates, on the workspace.
+static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b_in, double *x_out, int max_iter, double tol,
+                     femd_cg_result *res)
 {
     femd_pattern P = K->pattern;
     const int n = P->nrows;
     cudaStream_t s = ctx->stream;
     FEMD_TRY(ensure_f32(ctx, K));
-    DevBuf<double> Ax64, r64, part64;
-    DevBuf<float> r, p, Ap, d, part32;
-    DevBuf<CGState<float>> st;
-    DevBuf<CGState<double>> st64;
-    FEMD_TRY(Ax64.alloc(n + 1)); FEMD_TRY(r64.alloc(n + 1)); FEMD_TRY(r.alloc(n + 1)); FEMD_TRY(p.alloc(n + 1));
-    FEMD_TRY(Ap.alloc(n + 1)); FEMD_TRY(d.alloc(n + 1));
-    const int tpr = pick_tpr(K);
-    const unsigned gs = spmv_grid(ctx, n, tpr), gr = red_grid(ctx, n);
-    const size_t npart = 3 * (size_t)std::max(gs, gr) + 3;
-    FEMD_TRY(part64.alloc(npart)); FEMD_TRY(part32.alloc(npart));
-    FEMD_TRY(st.alloc(1)); FEMD_TRY(st64.alloc(1));
-    CGState<float> *sh = nullptr;
-    FEMD_TRY_CUDA(cudaMallocHost(&sh, sizeof(CGState<float>)));
-    struct FreeHost { CGState<float> *q; ~FreeHost() { cudaFreeHost(q); } } fh{sh};
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0); cudaEventCreate(&e1);
-    cudaEventRecord(e0, s);
+    SolverWS *Wp = nullptr;
+    FEMD_TRY(get_ws(ctx, K, &Wp));
+    SolverWS &W = *Wp;
+    FEMD_TRY(prepare_mixed(ctx, K, W));
+    const unsigned gs = W.gs, gr = W.gr;
+    double *x = W.wx.p;
+    const double *b = W.wb.p;
+    CGState<double> *st64 = W.st.p;
+    cudaEventRecord(W.e0, s);
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.wb.p, b_in, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.wx.p, x_out, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     // FP64 start: r64 = b - A x, nb, ||r64||; the FP32 recurrence starts from (float) r64
-    FEMD_TRY_CUDA(cudaMemsetAsync(st64.p, 0, sizeof(CGState<double>), s));
-    launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, nullptr, nullptr);
-    k_cg_start<true><<<gr, RED_BLOCK, 0, counted(s)>>>(b, Ax64.p, r64.p, r64.p, K->inv.p, n, part64.p, st64.p, tol);
-    k_mixed_init<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(b, Ax64.p, r.p, p.p, d.p, K->inv32.p, n);
+    FEMD_TRY_CUDA(cudaMemsetAsync(st64, 0, sizeof(CGState<double>), s));
+    launch_spmv<double, double, false>(W.shape, gs, s, P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, nullptr, nullptr);
+    k_cg_start<true><<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ax64.p, W.r64.p, W.r64.p, K->inv.p, n, W.part64.p, st64, tol);
+    k_mixed_init<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(b, W.Ax64.p, W.r32.p, W.p32.p, W.d32.p, K->inv32.p, n);
     FEMD_TRY_CUDA(cudaGetLastError());
-    CGState<double> s64;
-    FEMD_TRY_CUDA(cudaMemcpyAsync(&s64, st64.p, sizeof(s64), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.st_host, st64, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s));
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    const CGState<double> s64 = *W.st_host;
     if (s64.nb == 0.0) {
-        cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), s);
+        cudaMemsetAsync(x_out, 0, (size_t)n * sizeof(double), s);
         cudaStreamSynchronize(s);
         *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
         return FEMD_OK;
@@ -665,75 +768,51 @@ static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b, double *x, in
         res->breakdown = s64.breakdown; res->status = FEMD_OK; res->outer = 0; res->seconds = 0.0;
         return FEMD_OK;
     }
-    // FP32 state: rz = r32 . inv32 r32 is recomputed from the FP32 vectors by a reliable-update
-    // style kernel pass at the first chunk; seed it here from the FP64 start
-    CGState<float> s32{};
+    // FP32 state seeded from the FP64 start
+    CGState<float> &s32 = *W.st32_host;
+    s32 = CGState<float>{};
     s32.rz = (float)s64.rz;
     s32.nb = s64.nb;
     s32.tol_nb = s64.tol_nb;
     s32.rn = s64.rn;
     s32.maxr = s64.rn;
     s32.max_iter = max_iter;
-    FEMD_TRY_CUDA(cudaMemcpyAsync(st.p, &s32, sizeof(s32), cudaMemcpyHostToDevice, s));
-    const int CH = n > (1 << 18) ? 8 : 16;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    FEMD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < CH; ++k) {
-        launch_spmv<float, float, true>(tpr, gs, s, P->indptr.p, P->indices.p, K->data32.p, p.p, Ap.p, n, part32.p, st.p);
-        k_cg_update<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(d.p, r.p, p.p, Ap.p, K->inv32.p, n, part32.p, st.p, 1);
-        // a reliable update (when requested) before the direction update uses r
-        k_mixed_flush<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, d.p, n, st.p);
-        switch (shape_tpr(tpr)) {
-        case 2: k_mixed_spmv64<2><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
-        case 4: k_mixed_spmv64<4><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
-        case 8: k_mixed_spmv64<8><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
-        case 16: k_mixed_spmv64<16><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
-        default: k_mixed_spmv64<32><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, st.p); break;
-        }
-        k_mixed_residual<<<gr, RED_BLOCK, 0, counted(s)>>>(b, Ax64.p, r.p, K->inv32.p, n, part64.p, part32.p, st.p);
-        k_cg_direction<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(p.p, r.p, K->inv32.p, n, st.p);
-    }
-    cudaError_t ce = cudaStreamEndCapture(s, &graph);
-    if (ce != cudaSuccess) { set_error(std::string("pcg_mixed: graph capture: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
-    ce = cudaGraphInstantiate(&exec, graph, 0);
-    if (ce != cudaSuccess) { cudaGraphDestroy(graph); set_error(std::string("pcg_mixed: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
-    size_t nodes = 0;
-    cudaGraphGetNodes(graph, nullptr, &nodes);
-    const long long max_chunks = (long long)max_iter / CH + 2;
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.st32.p, W.st32_host, sizeof(CGState<float>), cudaMemcpyHostToDevice, s));
+    const long long max_chunks = (long long)max_iter / W.chm + 2;
     int status = FEMD_OK;
+    cudaError_t ce = cudaSuccess;
     for (long long c = 0; c < max_chunks; ++c) {
-        ce = launch_graph(exec, nodes, s);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(sh, st.p, sizeof(CGState<float>), cudaMemcpyDeviceToHost, s);
+        ce = launch_graph(W.xm, W.nodesm, s);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(W.st32_host, W.st32.p, sizeof(CGState<float>), cudaMemcpyDeviceToHost, s);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
         if (ce != cudaSuccess) { set_error(std::string("pcg_mixed: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; break; }
-        if (sh->done) break;
+        if (W.st32_host->done) break;
     }
     // final true residual in FP64 (cg.hpp:222-237)
     if (status == FEMD_OK) {
+        const CGState<float> sh = *W.st32_host;
         // flush any correction still held in FP32 (when the loop ended on max_iter)
-        k_mixed_flush_all<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, d.p, n);
-        launch_spmv<double, double, false>(tpr, gs, s, P->indptr.p, P->indices.p, K->data.p, x, Ax64.p, n, nullptr, nullptr);
-        FEMD_TRY_CUDA(cudaMemsetAsync(st64.p, 0, sizeof(CGState<double>), s));
-        k_cg_finish<<<gr, RED_BLOCK, 0, counted(s)>>>(b, Ax64.p, Ax64.p, n, part64.p, st64.p);
-        cudaEventRecord(e1, s);
-        FEMD_TRY_CUDA(cudaMemcpyAsync(&s64, st64.p, sizeof(s64), cudaMemcpyDeviceToHost, s));
+        k_mixed_flush_all<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, W.d32.p, n);
+        launch_spmv<double, double, false>(W.shape, gs, s, P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, nullptr,
+                                           nullptr);
+        FEMD_TRY_CUDA(cudaMemsetAsync(st64, 0, sizeof(CGState<double>), s));
+        k_cg_finish<<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ax64.p, W.Ax64.p, n, W.part64.p, st64);
+        FEMD_TRY_CUDA(cudaMemcpyAsync(x_out, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        cudaEventRecord(W.e1, s);
+        FEMD_TRY_CUDA(cudaMemcpyAsync(W.st_host, st64, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s));
         FEMD_TRY_CUDA(cudaStreamSynchronize(s));
-        res->iterations = sh->it;
-        res->breakdown = sh->breakdown;
-        res->residual = s64.res64 / sh->nb;
-        int conv = !sh->breakdown && res->residual <= tol * (1.0 + 1e-6) + 1e-15;
-        if (!conv && !sh->breakdown && res->residual <= 10.0 * tol && sh->it < max_iter) conv = 1;
+        res->iterations = sh.it;
+        res->breakdown = sh.breakdown;
+        res->residual = W.st_host->res64 / sh.nb;
+        int conv = !sh.breakdown && res->residual <= tol * (1.0 + 1e-6) + 1e-15;
+        if (!conv && !sh.breakdown && res->residual <= 10.0 * tol && sh.it < max_iter) conv = 1;
         res->converged = conv;
         res->status = FEMD_OK;
-        res->outer = sh->ru_count;
+        res->outer = sh.ru_count;
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventElapsedTime(&ms, W.e0, W.e1);
         res->seconds = ms * 1e-3;
     }
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
     return status;
 }
 
