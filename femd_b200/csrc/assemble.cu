@@ -301,6 +301,7 @@ struct FastSpec {
     const double *pts[MAX_TERMS];             // FEMD_COEF_POINTS arrays
     const double *field[MAX_TERMS];           // FEMD_COEF_FIELD vectors
     int npair, pr[MAX_PAIRS], ps[MAX_PAIRS];  // active (r, s) pairs (matrix) / active r (vector: ps unused)
+    int psym[MAX_PAIRS];                      // pair k stands for (r, s) and (s, r) of a symmetric form
     int has_const, has_var, nf;               // factors per cell: npair (const) + nq npair (varying)
     int vector;
 };
@@ -348,8 +349,8 @@ __global__ void __launch_bounds__(256) k_elem_factors(const double *__restrict__
         const int v0 = tris[3 * e], v1 = tris[3 * e + 1], v2 = tris[3 * e + 2];
         const double x0 = pts[2 * v0], y0 = pts[2 * v0 + 1];
         const double J0 = pts[2 * v1] - x0, J1 = pts[2 * v2] - x0, J2 = pts[2 * v1 + 1] - y0, J3 = pts[2 * v2 + 1] - y0;
-        const double d = J0 * J3 - J1 * J2, ad = fabs(d);
-        const double Ji0 = J3 / d, Ji1 = -J1 / d, Ji2 = -J2 / d, Ji3 = J0 / d;
+        const double d = J0 * J3 - J1 * J2, ad = fabs(d), rd = 1.0 / d;
+        const double Ji0 = J3 * rd, Ji1 = -J1 * rd, Ji2 = -J2 * rd, Ji3 = J0 * rd;
         double *F = factors + (size_t)e * fs.nf;
         int o = 0;
         if (fs.has_const) {
@@ -469,6 +470,161 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows(
     }
 }
 
+// ---- K3d: one thread per row over the pair offsets ----------------------------------------------
+// As K3b, with the scatter map replaced by the row-local byte offsets (a quarter of the bytes),
+// the next pair's code, offsets and factors loaded while the current pair's entries are formed,
+// and the row written back from the shared-memory accumulator.
+template <int NLOC, int NPAIR>
+__global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows_off(
+    const int *__restrict__ indptr, const int *__restrict__ rc_ptr, const int *__restrict__ rc_code,
+    const unsigned char *__restrict__ pair_off, const int *__restrict__ diag_pos, int nrows, int nq,
+    const double *__restrict__ factors, const double *__restrict__ g_S, const double *__restrict__ g_R, FastSpec fs,
+    int maxlen, double *__restrict__ data, double *__restrict__ inv, int *__restrict__ status)
+{
+    extern __shared__ double smem[];
+    constexpr int NL2 = NLOC * NLOC;
+    constexpr int OFFS = (NLOC + 3) / 4 * 4;
+    constexpr int NW = OFFS / 4;                             // 32-bit words of offsets per pair
+    double *sS = smem;
+    double *sR = sS + (fs.has_const ? NPAIR * NL2 : 0);
+    double *acc = sR + (fs.has_var ? nq * 3 * NLOC : 0);
+    if (fs.has_const)
+        for (int t = threadIdx.x; t < NPAIR * NL2; t += blockDim.x) sS[t] = g_S[t];
+    if (fs.has_var)
+        for (int t = threadIdx.x; t < nq * 3 * NLOC; t += blockDim.x) sR[t] = g_R[t];
+    __syncthreads();
+    const int cst = fs.has_const ? NPAIR : 0;
+    const unsigned *offw = reinterpret_cast<const unsigned *>(pair_off);
+    // per warp: the first position of each of its 32 rows (+ the end), and for every position of
+    // the warp's range the lane that owns it -- for the coalesced write-out below
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int *wrlo = reinterpret_cast<int *>(acc + (size_t)maxlen * FAST_BLOCK) + w * 33;
+    unsigned char *owner = reinterpret_cast<unsigned char *>(reinterpret_cast<int *>(acc + (size_t)maxlen * FAST_BLOCK) +
+                                                             (FAST_BLOCK / 32) * 33) + (size_t)w * 32 * maxlen;
+    for (int i0 = blockIdx.x * FAST_BLOCK + w * 32; i0 < nrows; i0 += gridDim.x * FAST_BLOCK) {
+    const int i = i0 + lane;
+    const bool valid = i < nrows;
+    const int rlo = valid ? indptr[i] : 0, len = valid ? indptr[i + 1] - rlo : 0;
+    double *a = acc + threadIdx.x;
+    for (int k = 0; k < len; ++k) a[k * FAST_BLOCK] = 0.0;
+    if (valid) {
+        const int c0 = rc_ptr[i], c1 = rc_ptr[i + 1];
+        int code = 0;
+        unsigned ow[NW];
+        double Fc[NPAIR];
+        if (c0 < c1) {
+            code = __ldcs(&rc_code[c0]);
+#pragma unroll
+            for (int ww = 0; ww < NW; ++ww) ow[ww] = __ldcs(&offw[(size_t)c0 * NW + ww]);
+            const double *F = factors + (size_t)(code / NLOC) * fs.nf;
+#pragma unroll
+            for (int k = 0; k < NPAIR; ++k) Fc[k] = fs.has_const ? __ldg(&F[k]) : 0.0;
+        }
+        for (int c = c0; c < c1; ++c) {
+            const int cur = code;
+            unsigned oq[NW];
+            double Fq[NPAIR];
+#pragma unroll
+            for (int ww = 0; ww < NW; ++ww) oq[ww] = ow[ww];
+#pragma unroll
+            for (int k = 0; k < NPAIR; ++k) Fq[k] = Fc[k];
+            if (c + 1 < c1) {                                 // the next pair's loads
+                code = __ldcs(&rc_code[c + 1]);
+#pragma unroll
+                for (int ww = 0; ww < NW; ++ww) ow[ww] = __ldcs(&offw[(size_t)(c + 1) * NW + ww]);
+                const double *F = factors + (size_t)(code / NLOC) * fs.nf;
+#pragma unroll
+                for (int k = 0; k < NPAIR; ++k) Fc[k] = fs.has_const ? __ldg(&F[k]) : 0.0;
+            }
+            const int e = cur / NLOC, l = cur - e * NLOC;
+            double v[NLOC];
+#pragma unroll
+            for (int j = 0; j < NLOC; ++j) {
+                double s = 0.0;
+                if (fs.has_const) {
+#pragma unroll
+                    for (int k = 0; k < NPAIR; ++k) s += Fq[k] * sS[k * NL2 + l * NLOC + j];
+                }
+                v[j] = s;
+            }
+            if (fs.has_var) {
+                const double *H = factors + (size_t)e * fs.nf + cst;
+                for (int q = 0; q < nq; ++q) {
+                    const double *R = sR + q * 3 * NLOC;
+#pragma unroll
+                    for (int k = 0; k < NPAIR; ++k) {
+                        const double h = H[q * NPAIR + k] * R[fs.pr[k] * NLOC + l];
+                        const double *Rs = R + fs.ps[k] * NLOC;
+#pragma unroll
+                        for (int j = 0; j < NLOC; ++j) v[j] += h * Rs[j];
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NLOC; ++j) {
+                const unsigned o = (oq[j >> 2] >> (8 * (j & 3))) & 0xffu;
+                if (o != 0xffu) a[o * FAST_BLOCK] += v[j];
+            }
+        }
+        if (inv) {
+            const int dp = diag_pos[i];
+            if (dp < 0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
+            else {
+                const double dv = a[(dp - rlo) * FAST_BLOCK];
+                if (dv == 0.0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
+                inv[i] = 1.0 / dv;
+            }
+        }
+    }
+    // coalesced write-out: the warp's rows are contiguous in HBM, [wrlo[0], wrlo[32]); each
+    // position is written by consecutive lanes (full sectors, no partial-sector merges in L2)
+    const int end_all = indptr[min(i0 + 32, nrows)];
+    wrlo[lane] = valid ? rlo : end_all;
+    if (lane == 31) wrlo[32] = end_all;
+    __syncwarp();
+    const int first = wrlo[0];
+    for (int k = 0; k < len; ++k) owner[rlo - first + k] = (unsigned char)lane;
+    __syncwarp();
+    for (int p = first + lane; p < wrlo[32]; p += 32) {
+        const int t = owner[p - first];
+        data[p] = acc[(size_t)(p - wrlo[t]) * FAST_BLOCK + w * 32 + t];
+    }
+    __syncwarp();
+    }
+}
+
+// The pair offsets: for rc index c (row i, cell entry code = cell nloc + l), byte j of
+// off[c * OFFS + j] = position of (i, dof(cell, j)) minus indptr[i], 255 where constrained.
+// OFFS = nloc rounded up to a multiple of 4, so a pair's offsets load as whole 32-bit words.
+__global__ void k_pair_offsets(const int *__restrict__ rc_ptr, const int *__restrict__ rc_code,
+                               const int *__restrict__ indptr, const int *__restrict__ map, int nrows, int nloc, int offs,
+                               unsigned char *__restrict__ off)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x) {
+        const int rlo = indptr[i];
+        for (int c = rc_ptr[i]; c < rc_ptr[i + 1]; ++c) {
+            const int code = rc_code[c];
+            for (int j = 0; j < offs; ++j) {
+                const int m = j < nloc ? map[(size_t)code * nloc + j] : -1;
+                off[(size_t)c * offs + j] = m < 0 ? (unsigned char)255 : (unsigned char)(m - rlo);
+            }
+        }
+    }
+}
+
+static int build_pair_offsets(femd_ctx ctx, femd_pattern p)
+{
+    if (p->pair_off.p) return FEMD_OK;
+    const int offs = (p->nloc + 3) / 4 * 4;
+    const size_t npairs = (size_t)p->ncells * p->nloc;
+    FEMD_TRY(p->pair_off.alloc(npairs * offs + 4));
+    if (p->nrows)
+        k_pair_offsets<<<grid_for((size_t)p->nrows, 256, 1u << 20), 256, 0, counted(ctx->stream)>>>(
+            p->rc_ptr.p, p->rc_code.p, p->indptr.p, p->map.p, p->nrows, p->nloc, offs, p->pair_off.p);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    return FEMD_OK;
+}
+
 // K4 FAST: one thread per row, f_i = sum over the row's cells (increasing order) of
 // sum_k F_k R_{r_k}(l) (constant) + sum_q sum_k H_{q,k} R_{r_k}(q, l) (varying), where the
 // constant part uses the tabulation integrated against the weights (Sv^{r}(l) = sum_q rw_q R_r(q,l)).
@@ -530,9 +686,25 @@ static void fast_spec(int nterms, const int *a, const int *b, const femd_coef *c
                 if (ra && sb) act[r][s] = true;
             }
     }
+    // a symmetric form with constant coefficients (every term (a, b) has its mirror (b, a) with
+    // the same coefficient) has F_rs = F_sr on every cell: (r, s) and (s, r) share one factor
+    bool symmetric = !vector && !fs.has_var;
+    for (int t = 0; t < nterms && symmetric; ++t) {
+        if (a[t] == b[t]) continue;
+        bool found = false;
+        for (int u = 0; u < nterms && !found; ++u)
+            found = a[u] == b[t] && b[u] == a[t] && coef[u].kind == coef[t].kind && coef[u].value == coef[t].value;
+        symmetric = found;
+    }
     for (int r = 0; r < 3; ++r)
-        for (int s = 0; s < 3; ++s)
-            if (act[r][s]) { fs.pr[fs.npair] = r; fs.ps[fs.npair] = s; ++fs.npair; }
+        for (int s = 0; s < 3; ++s) {
+            if (!act[r][s]) continue;
+            if (symmetric && s < r && act[s][r]) continue;     // merged into (s, r)
+            fs.pr[fs.npair] = r;
+            fs.ps[fs.npair] = s;
+            fs.psym[fs.npair] = symmetric && r != s && act[s][r];
+            ++fs.npair;
+        }
     fs.nf = (fs.has_const ? fs.npair : 0) + (fs.has_var ? nq * fs.npair : 0);
 }
 
@@ -670,6 +842,7 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
                     for (int q = 0; q < nq; ++q) {
                         const double *Rq = rule->ref_host + (size_t)q * 3 * nl;
                         acc += rule->w_host[q] * Rq[fs.pr[k] * nl + l] * Rq[fs.ps[k] * nl + j];
+                        if (fs.psym[k]) acc += rule->w_host[q] * Rq[fs.ps[k] * nl + l] * Rq[fs.pr[k] * nl + j];
                     }
                     S[(size_t)k * nl2 + l * nl + j] = acc;
                 }
@@ -702,10 +875,30 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
     const size_t shm = ((fs.has_const ? (size_t)fs.npair * nl2 : 0) + (fs.has_var ? nref : 0) + (size_t)maxlen * FAST_BLOCK) *
                            sizeof(double) + (FAST_BLOCK / 32) * 33 * sizeof(int);
     if (n) {
-        cudaFuncSetAttribute(k_assemble_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-        k_assemble_rows<<<grid_for((size_t)n, FAST_BLOCK, 1u << 22), FAST_BLOCK, shm, counted(s)>>>(
-            p->indptr.p, p->rc_ptr.p, p->rc_code.p, p->map.p, p->diag_pos.p, n, nl, nq, p->ws_factors.p, d_S, d_ref, fs,
-            maxlen, K->data.p, inv, ctx->status_dev);
+        const unsigned grid = grid_for((size_t)n, FAST_BLOCK, 1u << 22);
+        bool done = false;
+        const size_t sho = ((fs.has_const ? (size_t)fs.npair * nl2 : 0) + (fs.has_var ? nref : 0) +
+                            (size_t)maxlen * FAST_BLOCK) * sizeof(double) +
+                           (FAST_BLOCK / 32) * 33 * sizeof(int) + (size_t)FAST_BLOCK * maxlen;
+#define FEMD_ROWS_OFF(NL, NP)                                                                                          \
+        if (!done && nl == NL && fs.npair == NP && maxlen < 255) {                                                     \
+            FEMD_TRY(build_pair_offsets(ctx, p));                                                                      \
+            cudaFuncSetAttribute(k_assemble_rows_off<NL, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sho); \
+            k_assemble_rows_off<NL, NP><<<grid, FAST_BLOCK, sho, counted(s)>>>(                                        \
+                p->indptr.p, p->rc_ptr.p, p->rc_code.p, p->pair_off.p, p->diag_pos.p, n, nq, p->ws_factors.p, d_S,     \
+                d_ref, fs, maxlen, K->data.p, inv, ctx->status_dev);                                                   \
+            done = true;                                                                                               \
+        }
+        FEMD_ROWS_OFF(3, 1) FEMD_ROWS_OFF(3, 3) FEMD_ROWS_OFF(3, 4) FEMD_ROWS_OFF(3, 5)
+        FEMD_ROWS_OFF(6, 1) FEMD_ROWS_OFF(6, 3) FEMD_ROWS_OFF(6, 4) FEMD_ROWS_OFF(6, 5)
+        FEMD_ROWS_OFF(10, 1) FEMD_ROWS_OFF(10, 3) FEMD_ROWS_OFF(10, 4) FEMD_ROWS_OFF(10, 5)
+#undef FEMD_ROWS_OFF
+        if (!done) {
+            cudaFuncSetAttribute(k_assemble_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+            k_assemble_rows<<<grid, FAST_BLOCK, shm, counted(s)>>>(p->indptr.p, p->rc_ptr.p, p->rc_code.p, p->map.p,
+                                                                   p->diag_pos.p, n, nl, nq, p->ws_factors.p, d_S, d_ref,
+                                                                   fs, maxlen, K->data.p, inv, ctx->status_dev);
+        }
     }
     FEMD_TRY_CUDA(cudaGetLastError());
     K->f32_valid = false;

@@ -98,6 +98,13 @@ struct femd_pattern_s : femd::HandleBase {
     // assembly workspace, grown on demand and reused across calls (no allocation per call
     // once it has its size): per-element factors, the rule's tables
     femd::DevBuf<double> ws_factors, ws_tables;
+    // the scatter map inverted: for every matrix position, its element entries
+    // (cell nloc^2 + l nloc + j) in increasing cell order (built on the first FAST assembly)
+    femd::DevBuf<int> contrib_ptr, contrib;
+    // for every (row, cell) pair of the rc lists, the offsets within the row of the cell's nloc
+    // columns (uint8, 255 = constrained): the scatter map in the rows' own order, a quarter of
+    // its size (built on the first FAST assembly when every row is shorter than 255)
+    femd::DevBuf<unsigned char> pair_off;
     femd_pattern_s() : HandleBase(femd::KIND_PATTERN) {}
 };
 
