@@ -11,3 +11,4 @@ from .krylov import KrylovInfo, cg  # noqa: F401
 from ._native import FemdError, lib  # noqa: F401
 
 __version__ = "0.1.0"
+from .batch import Batch  # noqa: F401,E402

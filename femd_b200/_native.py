@@ -77,6 +77,11 @@ SIGNATURES = {
     "femd_cuda_cg_solve_host": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_pcg_mixed": (_I, [_P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_cg_jacobi_noalloc": (_I, [_P, _P, _I, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
+    "femd_cuda_batch_create": (_I, [_P, _I, _P, _I, C.POINTER(_P)]),
+    "femd_cuda_batch_solve": (_I, [_P, _P, _P, _P, _I, _D, _I, C.POINTER(femd_cg_result)]),
+    "femd_cuda_batch_abort": (_I, [_P]),
+    "femd_cuda_batch_info": (_I, [_P, _PI, _PI, _PI, _PI]),
+    "femd_cuda_batch_debug": (_I, [_P, _I, C.c_longlong]),
     "femd_host_rectangle_mesh": (_I, [_D, _D, _D, _D, _I, _I, _P, _P]),
     "femd_host_lagrange_numbering": (_I, [_I, _I, _P, _I, _I, _P, _PI, _PI]),
     "femd_host_triangle_quadrature": (_I, [_I, _P, _P, _P]),

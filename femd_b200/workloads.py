@@ -1,0 +1,55 @@
+"""The synthetic workloads of the benchmark configurations, built through femd_b200.
+
+Every input comes from a seed (numpy's default_rng); no dataset is read.
+
+    poisson_batch(seed, nprob)   many independent Poisson problems: rectangle_mesh(0,0,1,1,N,N),
+                                 N uniform in {16, ..., 256}, P_k with k uniform in {1, 2, 3},
+                                 a = c grad.grad with c log-uniform in [0.1, 10], the load
+                                 vector's dof values N(0, 1)
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import core as fb
+
+PI = math.pi
+
+
+class SpaceCache:
+    """Meshes, spaces, caches and patterns shared by every problem on the same (N, k)."""
+
+    def __init__(self):
+        self.spaces = {}
+
+    def get(self, N, k, form="gradgrad"):
+        key = (N, k)
+        s = self.spaces.get(key)
+        if s is None:
+            m = fb.rectangle_mesh(0, 0, 1, 1, N, N)
+            V = fb.LagrangeSpace2D(m, k, bc="dirichlet")
+            s = self.spaces[key] = dict(mesh=m, V=V, P=V.pattern(), Q={})
+        q = s["Q"].get(form)
+        if q is None:
+            q = s["Q"][form] = s["V"].cache(fb.quad_degree(form, k))
+        return s, q
+
+
+def poisson_batch_spec(seed=0, nprob=256, nmin=16, nmax=256):
+    rng = np.random.default_rng(seed)
+    N = rng.integers(nmin, nmax + 1, nprob)
+    k = rng.integers(1, 4, nprob)
+    c = np.exp(rng.uniform(np.log(0.1), np.log(10.0), nprob))
+    return [dict(N=int(N[i]), k=int(k[i]), c=float(c[i]), seed=int(seed) * 100003 + i) for i in range(nprob)]
+
+
+def build_poisson(spec, cache: SpaceCache):
+    """One problem of the batch: the assembled matrix (with its Jacobi inverse) and the load vector."""
+    import torch
+    s, Q = cache.get(spec["N"], spec["k"], "gradgrad")
+    K = fb.CSRMatrix(s["P"])
+    fb.assemble_matrix_2d(Q, Q, [1, 2], [1, 2], [spec["c"], spec["c"]], K)
+    b = np.random.default_rng(spec["seed"]).standard_normal(s["V"].dim)
+    return K, torch.as_tensor(b).cuda()

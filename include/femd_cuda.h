@@ -245,6 +245,33 @@ FEMD_API int femd_cuda_cg_jacobi_noalloc(femd_ctx ctx, femd_matrix K, int use_ja
                                          int max_iter, double tol, femd_cg_result *res);
 
 /* ======================================================================================
+ * Batched solves: K7.  Many independent Jacobi-PCG solves in ONE persistent cooperative
+ * launch.  No single reference counterpart: it runs the reference's cg_jacobi
+ * (include/femd/krylov/cg.hpp:296-350, stopping rule and final true residual included) for
+ * every system of the batch at once.  Each problem gets a team of thread blocks sized from its
+ * nonzeros (nnz_per_block, 0 = 65536); the members meet at software barriers with bounded
+ * waits (FEMD_ETIMEOUT when one runs out; every block then returns).  A problem's result does
+ * not depend on the rest of the batch: its reductions are ordered by the problem alone.
+ * mixed != 0: FP32 matrix copy, vectors and accumulation, with FP64 reliable updates
+ * (r = b - A x on the FP64 matrix, x updated in FP64) until ||b - A x|| <= tol ||b||.
+ * ====================================================================================== */
+typedef struct femd_batch_s *femd_batch;
+FEMD_API int femd_cuda_batch_create(femd_ctx ctx, int nprob, const femd_matrix *mats, int nnz_per_block, femd_batch *out);
+/* b_dev[p], x_dev[p]: device vectors of problem p (x: initial guess in, solution out).
+ * max_iter <= 0: max(1000, 10 n) per problem.  results[p] per problem; res.seconds = the launch. */
+FEMD_API int femd_cuda_batch_solve(femd_ctx ctx, femd_batch B, const double *const *b_dev, double *const *x_dev,
+                                   int max_iter, double tol, int mixed, femd_cg_result *results);
+/* Ask a running batch solve to stop (safe from another host thread): FEMD_EABORT. */
+FEMD_API int femd_cuda_batch_abort(femd_batch B);
+/* Problems, resident blocks, team slots and each problem's team size (team_out: nprob ints). */
+FEMD_API int femd_cuda_batch_info(femd_batch B, int *nprob, int *grid, int *nslots, int *team_out);
+/* Failure-detection hook for tests: the next solves make problem ghost_problem (-1: none) wait
+ * at its barriers for one team member that never comes, and bound every wait by spin_limit
+ * spins (<= 0: the default, a few seconds).  The solve then returns FEMD_ETIMEOUT and the
+ * context stays usable.  No reference counterpart. */
+FEMD_API int femd_cuda_batch_debug(femd_batch B, int ghost_problem, long long spin_limit);
+
+/* ======================================================================================
  * Host-side setup of the synthetic problems (the reference's own setup code runs on the
  * host too).  No GPU work.
  * ====================================================================================== */
