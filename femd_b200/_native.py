@@ -82,6 +82,13 @@ SIGNATURES = {
     "femd_cuda_batch_abort": (_I, [_P]),
     "femd_cuda_batch_info": (_I, [_P, _PI, _PI, _PI, _PI]),
     "femd_cuda_batch_debug": (_I, [_P, _I, C.c_longlong]),
+    "femd_cuda_batch_configure": (_I, [_P, _I, _I, _I]),
+    "femd_cuda_batch_params": (_I, [_P, _PI, _PI, _PI, _PI]),
+    "femd_cuda_batch_tune": (_I, [_P, _P, _P, _P, _I, _D, _I, _PI, C.POINTER(C.c_double)]),
+    "femd_cuda_batch_add": (_I, [_P, _P, _PI]),
+    "femd_cuda_batch_remove": (_I, [_P, _I]),
+    "femd_cuda_batch_arm": (_I, [_P, _I, _P, _P, _I, _D]),
+    "femd_cuda_batch_step": (_I, [_P, _P, _I, _I, _PI, _PI, C.POINTER(femd_cg_result)]),
     "femd_host_rectangle_mesh": (_I, [_D, _D, _D, _D, _I, _I, _P, _P]),
     "femd_host_lagrange_numbering": (_I, [_I, _I, _P, _I, _I, _P, _PI, _PI]),
     "femd_host_triangle_quadrature": (_I, [_I, _P, _P, _P]),

@@ -1,4 +1,11 @@
-"""Batched Jacobi-PCG: many independent systems in one persistent launch (femd_cuda_batch_*)."""
+"""Batched Jacobi-PCG: many independent systems in one persistent launch (femd_cuda_batch_*).
+
+A Batch holds member systems (CSR matrices with their Jacobi inverse diagonals).  solve() runs
+every member to completion in one cooperative launch; arm() / step() advance armed members a
+bounded number of iterations per launch, so members can join and leave between launches (the
+continuous batching of femd_b200.serve).  A member's iterates depend on the member and the
+launch shape alone: the same bits alone or in any mix.
+"""
 from __future__ import annotations
 
 import ctypes as C
@@ -9,23 +16,30 @@ from . import _native as N
 from .core import CSRMatrix, _as_device, _torch, check, context, lib
 
 
+def _result(r: N.femd_cg_result) -> dict:
+    return dict(converged=bool(r.converged), iterations=int(r.iterations), residual=float(r.residual),
+                breakdown=bool(r.breakdown), status=int(r.status), reliable_updates=int(r.outer),
+                seconds=float(r.seconds))
+
+
 class Batch:
-    """A fixed set of matrices (each with its Jacobi inverse diagonal) solved together.
+    """Member systems solved together, FP64 or mixed precision (FP32 inner iteration, FP64
+    reliable updates)."""
 
-    solve() runs every system's Jacobi-PCG in one cooperative launch, FP64 or mixed precision
-    (FP32 inner iteration, FP64 reliable updates).  A system's result does not depend on the
-    other systems of the batch."""
-
-    def __init__(self, mats: list[CSRMatrix], nnz_per_block: int = 0, ctx=None):
+    def __init__(self, mats: list[CSRMatrix] = (), nnz_per_block: int = 0, ctx=None):
         from .core import JacobiPreconditioner
         self.ctx = ctx or context()
-        self.mats = list(mats)
-        for K in self.mats:
+        mats = list(mats)
+        for K in mats:
             JacobiPreconditioner(K)             # the inverse diagonal, checked (zero diagonal -> ValueError)
-        arr = (C.c_void_p * len(mats))(*[K.h.value for K in self.mats])
+        arr = (C.c_void_p * max(len(mats), 1))(*[K.h.value for K in mats])
         h = C.c_void_p()
         check(lib.femd_cuda_batch_create(self.ctx.h, len(mats), arr, int(nnz_per_block), C.byref(h)))
         self.h = h
+        self.members = {i: K for i, K in enumerate(mats)}   # id -> matrix (kept alive while a member)
+        self.mats = mats
+        self.last_status = N.FEMD_OK
+        self._armed = {}                                    # id -> (b, x) kept alive while armed
 
     def __del__(self):
         try:
@@ -35,39 +49,111 @@ class Batch:
         except Exception:
             pass
 
+    # ---- shape -------------------------------------------------------------------------
     def info(self):
         n, g, s = C.c_int(), C.c_int(), C.c_int()
-        teams = np.empty(len(self.mats), dtype=np.int32)
+        teams = np.empty(max(len(self.members), 1), dtype=np.int32)
         check(lib.femd_cuda_batch_info(self.h, C.byref(n), C.byref(g), C.byref(s), teams.ctypes.data_as(C.POINTER(C.c_int))))
-        return dict(nprob=n.value, grid=g.value, slots=s.value, teams=teams)
+        return dict(nprob=n.value, grid=g.value, slots=s.value, teams=teams[:n.value])
 
-    def solve(self, bs, xs=None, *, tol=1e-10, max_iter=0, mixed=True):
-        """bs: right-hand sides (device tensors or arrays); xs: initial guesses (default 0), overwritten.
-        Returns (xs, results), results a list of dicts (converged, iterations, residual, breakdown,
-        status, reliable_updates) and the launch time."""
+    def configure(self, block=256, nnz_per_block=65536, nnz_per_thread=4):
+        """Set the launch shape (femd_cuda_batch_configure)."""
+        check(lib.femd_cuda_batch_configure(self.h, int(block), int(nnz_per_block), int(nnz_per_thread)))
+
+    def params(self):
+        b, n, t, g = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib.femd_cuda_batch_params(self.h, C.byref(b), C.byref(n), C.byref(t), C.byref(g)))
+        return dict(block=b.value, nnz_per_block=n.value, nnz_per_thread=t.value, graph=g.value)
+
+    # ---- fixed batch -------------------------------------------------------------------
+    def _vectors(self, bs, xs):
         torch = _torch()
+        mats = [self.members[i] for i in sorted(self.members)]
         bs = [_as_device(b, self.ctx) for b in bs]
-        if len(bs) != len(self.mats):
-            raise ValueError("batch: one right-hand side per matrix")
+        if len(bs) != len(mats):
+            raise ValueError("batch: one right-hand side per member")
         if xs is None:
-            xs = [torch.zeros(K.nrows, dtype=torch.float64, device=b.device) for K, b in zip(self.mats, bs)]
-        for K, b, x in zip(self.mats, bs, xs):
+            xs = [torch.zeros(K.nrows, dtype=torch.float64, device=b.device) for K, b in zip(mats, bs)]
+        for K, b, x in zip(mats, bs, xs):
             if b.numel() != K.nrows or x.numel() != K.nrows:
                 raise ValueError("batch: vector length differs from its matrix")
         bp = (C.c_void_p * len(bs))(*[b.data_ptr() for b in bs])
         xp = (C.c_void_p * len(xs))(*[x.data_ptr() for x in xs])
+        return bs, xs, bp, xp
+
+    def tune(self, bs, *, tol=1e-10, max_iter=0, mixed=True):
+        """Autotune the launch shape on these right-hand sides (femd_cuda_batch_tune); returns the
+        chosen params and the best time in seconds."""
+        bs, xs, bp, xp = self._vectors(bs, None)
+        best = (C.c_int * 3)()
+        sec = C.c_double()
+        self.ctx.enter()
+        st = lib.femd_cuda_batch_tune(self.ctx.h, self.h, bp, xp, int(max_iter), float(tol), int(bool(mixed)), best,
+                                      C.byref(sec))
+        self.ctx.leave()
+        check(st)
+        return self.params(), sec.value
+
+    def solve(self, bs, xs=None, *, tol=1e-10, max_iter=0, mixed=True):
+        """Solve every member (in id order) to completion in one launch.  bs: right-hand sides;
+        xs: initial guesses (default 0), overwritten.  Returns (xs, results) with one dict per
+        member (converged, iterations, residual, breakdown, status, reliable_updates, seconds)."""
+        bs, xs, bp, xp = self._vectors(bs, xs)
         res = (N.femd_cg_result * len(bs))()
         self.ctx.enter()
         st = lib.femd_cuda_batch_solve(self.ctx.h, self.h, bp, xp, int(max_iter), float(tol), int(bool(mixed)), res)
         self.ctx.leave()
-        out = [dict(converged=bool(r.converged), iterations=int(r.iterations), residual=float(r.residual),
-                    breakdown=bool(r.breakdown), status=int(r.status), reliable_updates=int(r.outer),
-                    seconds=float(r.seconds)) for r in res]
         self.last_status = st
         if st not in (N.FEMD_OK, N.FEMD_ETIMEOUT, N.FEMD_EABORT):
             check(st)
-        return xs, out
+        return xs, [_result(r) for r in res]
 
+    # ---- dynamic membership --------------------------------------------------------------
+    def add(self, K: CSRMatrix) -> int:
+        """Add a member; returns its id."""
+        from .core import JacobiPreconditioner
+        JacobiPreconditioner(K)
+        i = C.c_int()
+        check(lib.femd_cuda_batch_add(self.h, K.h, C.byref(i)))
+        self.members[i.value] = K
+        return i.value
+
+    def remove(self, i: int):
+        check(lib.femd_cuda_batch_remove(self.h, int(i)))
+        self.members.pop(i, None)
+        self._armed.pop(i, None)
+
+    def arm(self, i: int, b, x, *, tol=1e-10, max_iter=0):
+        """Start a solve of member i on the next steps (b, x: float64 device tensors; x holds the
+        initial guess and receives the solution)."""
+        K = self.members[i]
+        if b.numel() != K.nrows or x.numel() != K.nrows:
+            raise ValueError("batch: vector length differs from its matrix")
+        self.ctx.enter()
+        st = lib.femd_cuda_batch_arm(self.h, int(i), b.data_ptr(), x.data_ptr(), int(max_iter), float(tol))
+        self.ctx.leave()
+        check(st)
+        self._armed[i] = (b, x)
+
+    def step(self, iters: int, *, mixed=True):
+        """One launch advancing every armed member by at most iters iterations.  Returns
+        [(id, result dict)] of the members that finished."""
+        n = max(len(self._armed), 1)
+        ids = (C.c_int * n)()
+        res = (N.femd_cg_result * n)()
+        nf = C.c_int()
+        self.ctx.enter()
+        st = lib.femd_cuda_batch_step(self.ctx.h, self.h, int(iters), int(bool(mixed)), C.byref(nf), ids, res)
+        self.ctx.leave()
+        self.last_status = st
+        if st not in (N.FEMD_OK, N.FEMD_ETIMEOUT, N.FEMD_EABORT):
+            check(st)
+        out = [(int(ids[k]), _result(res[k])) for k in range(nf.value)]
+        for i, _ in out:
+            self._armed.pop(i, None)
+        return out
+
+    # ---- control -----------------------------------------------------------------------
     def abort(self):
         lib.femd_cuda_batch_abort(self.h)
 

@@ -1,20 +1,39 @@
 // batch.cu -- K7: many independent Jacobi-PCG solves in one persistent, cooperative launch.
 //
-// Every problem p gets a team of T_p thread blocks (T_p from its size alone).  Blocks take
-// (problem, member) slots from a queue, largest teams first; a member owns a contiguous range of
-// the problem's rows.  The members of a team meet at software barriers (a counter per problem,
-// waited on with a bounded spin: a wait that runs out sets FEMD_ETIMEOUT and every block
-// returns).  Dot products are summed per block, then across the team's members in member order,
-// so a problem's iterates depend on the problem alone -- the same bits alone or in any mix.
+// A batch is a set of member systems (CSR matrices with their Jacobi inverse diagonals).  Every
+// member gets a team of T thread blocks (T from its size and the batch's launch shape only).
+// Blocks take (member, team rank) slots from a queue, largest teams first; a rank owns a
+// contiguous range of the member's rows.  The ranks of a team meet at software barriers (a
+// counter per member, waited on with a bounded spin: a wait that runs out sets FEMD_ETIMEOUT and
+// every block returns).  Dot products are summed per block, then across the team in one fixed
+// order, so a member's iterates depend on the member and the launch shape alone -- the same bits
+// alone or in any mix.
 //
-// The launch is cooperative (all blocks resident), so a team whose members are still busy
-// elsewhere only delays; at most one team is incomplete at any time (slots are taken in order),
-// so every team completes.
+// The launch is cooperative (all blocks resident), so a team whose ranks are still busy
+// elsewhere only delays; at most one team is incomplete at any time (slots are taken in order and
+// no team is larger than half the grid), so every team completes.
 //
-// Modes: FP64 Jacobi-PCG (cg.hpp:296-350 semantics) or mixed precision (FP32 matrix copy,
-// vectors and reductions; FP64 residual b - A x and solution update at reliable updates).
+// Solves are resumable: a launch advances every armed member by at most `iters` iterations and
+// saves its scalars (BState) for the next launch.  One launch with iters = max_iter solves a
+// fixed batch; short launches with members joining and leaving between them are the continuous
+// batching of the request loop.
+//
+// SpMV: CSR-stream over precomputed chunks of whole rows (at most BB x NPT nonzeros): the block
+// loads the chunk's column indices and values coalesced, gathers, stores the products in shared
+// memory (two buffers, one barrier per chunk), and one thread per row sums its products in order.
+//
+// One iteration is two team reductions.  The search direction is never written before the SpMV
+// that needs it: the SpMV forms p_j = z_j + beta p_j (one fused multiply-add, the same one the
+// row's owner stores) from the previous direction, held in a second buffer.
+//
+// Modes: FP64 Jacobi-PCG (cg.hpp:296-350 semantics, final true residual included) or mixed
+// precision: FP32 matrix copy (made by each rank from the FP64 values when the solve starts),
+// FP32 vectors and SpMV accumulation; FP64 residual b - A x on the FP64 matrix and FP64 solution
+// update at reliable updates.
 #include <algorithm>
+#include <climits>
 #include <cmath>
+#include <cstring>
 #include <memory>
 #include <numeric>
 #include <string>
@@ -24,29 +43,38 @@
 
 namespace femd {
 
-static constexpr int BB = 256;                 // threads per block
-static constexpr long long SPIN_LIMIT = 1ll << 25;   // default bound: x ~64 ns sleeps, a few seconds at most
+static constexpr long long SPIN_LIMIT = 1ll << 25;   // default bound of a barrier wait (spins of ~0.5 us)
+
+enum : int { BS_STARTED = 1, BS_DONE = 2, BS_BREAKDOWN = 4, BS_CONVERGED = 8 };
+
+// a member's solver scalars, kept in device memory between launches
+struct BState {
+    double rz, beta, maxr, nb, res;
+    int it, rus, flags, status;
+};
 
 struct BProb {
-    int n, tpr, team, max_iter;
+    int n, team, max_iter, nch;
     double tol;
     const int *indptr, *indices;
-    const float *A32, *inv32;
+    const int *crow, *cq;  // chunk c = rows [crow[c], crow[c+1]) = nonzeros [cq[c], cq[c+1])
     const double *A64, *inv64;
+    float *A32, *inv32;
     const double *b;
     double *x;
-    float *r32, *p32, *Ap32, *d32;
-    double *r64, *p64, *Ap64;
+    float *r32, *z32, *pa32, *pb32, *Ap32, *d32;
+    double *r64, *z64, *pa64, *pb64, *Ap64;
     double *part;          // 8 kinds x team
     unsigned *bar;
-    int *res_i;            // [0] iterations [1] converged [2] breakdown [3] status [4] reliable updates
-    double *res_d;         // [0] residual
+    BState *st;
 };
 
 struct BQueue {
     unsigned next;
     int flag;              // FEMD_ETIMEOUT / FEMD_EABORT seen by any block
     long long spin_limit;  // the bound of every barrier wait (spins)
+    int nslots;
+    int iters;             // iterations per member in this launch
 };
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
@@ -56,28 +84,43 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
     return v;
 }
 
-// team barrier: returns false when the batch has to stop (timeout or abort)
-__device__ bool team_barrier(const BProb &P, unsigned &phase, BQueue *q, volatile const int *abort_flag)
+__device__ __forceinline__ float pdir(const float *z, const float *p, float beta, int j) { return __fmaf_rn(beta, p[j], z[j]); }
+__device__ __forceinline__ double pdir(const double *z, const double *p, double beta, int j) { return __fma_rn(beta, p[j], z[j]); }
+
+// team barrier: false when the batch has to stop (timeout or abort).  lead_sync: the block has
+// not synchronised since its last global writes.
+__device__ bool team_barrier(const BProb &P, unsigned &phase, BQueue *q, volatile const int *abort_flag, bool lead_sync)
 {
     __shared__ int s_ok;
-    __syncthreads();
+    const bool check = (phase & 15) == 0;
+    if (P.team == 1 && !check) {
+        if (lead_sync) __syncthreads();
+        ++phase;
+        return true;
+    }
+    if (lead_sync) __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
         if (P.team > 1) {
             __threadfence();
             atomicAdd(P.bar, 1u);
             const unsigned target = (phase + 1) * (unsigned)P.team;
+            const long long lim = q->spin_limit;
             long long spins = 0;
             while (ld_acquire(P.bar) < target) {
-                if (((spins & 1023) == 0) && *(volatile int *)&q->flag) { ok = 0; break; }
-                if (++spins > q->spin_limit) { atomicCAS(&q->flag, 0, FEMD_ETIMEOUT); ok = 0; break; }
-                __nanosleep(64);
+                if (((++spins) & 255) == 0) {
+                    if (*(volatile int *)&q->flag) { ok = 0; break; }
+                    if (spins > lim) { atomicCAS(&q->flag, 0, FEMD_ETIMEOUT); ok = 0; break; }
+                }
+                __nanosleep(32);
             }
             __threadfence();
         }
-        // the host's abort flag (mapped host memory, a PCIe read): every 64th barrier
-        if (abort_flag && (phase & 63) == 0 && *abort_flag) atomicCAS(&q->flag, 0, FEMD_EABORT);
-        if (*(volatile int *)&q->flag) ok = 0;
+        if (check) {
+            // the host's abort flag (mapped host memory, a PCIe read): every 64th barrier
+            if (abort_flag && (phase & 63) == 0 && *abort_flag) atomicCAS(&q->flag, 0, FEMD_EABORT);
+            if (*(volatile int *)&q->flag) ok = 0;
+        }
         s_ok = ok;
     }
     __syncthreads();
@@ -85,35 +128,46 @@ __device__ bool team_barrier(const BProb &P, unsigned &phase, BQueue *q, volatil
     return s_ok != 0;
 }
 
-template <class T>
-__device__ __forceinline__ T block_sum(T v, T *sh)
+// the block's reduction scratch, one row per kind: consecutive reductions of the same kind are
+// always separated by a reduction of another kind (and its __syncthreads)
+struct RedSmem {
+    double warp[8][16];
+    double tot[8];
+};
+__device__ __forceinline__ RedSmem &red_smem()
 {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    __syncthreads();
-    if (lane == 0) sh[w] = v;
-    __syncthreads();
-    T s = T(0);
-    for (int k = 0; k < BB / 32; ++k) s += sh[k];
+    __shared__ RedSmem s;
     return s;
 }
 
-// team reduction of NV values of kind base..base+NV-1: each member writes its block sum, the team
-// meets, and warp 0 of every member sums the T partials in one fixed order (lane-strided, then a
-// shuffle tree), so the result depends on T and the partials only
-template <int NV>
+// team reduction of NV values of kinds base..base+NV-1: block sums, each rank writes its own,
+// the team meets, and warp 0 of every rank sums the T partials in one fixed order (lane-strided,
+// then a shuffle tree), so the result depends on T and the partials only
+template <int NV, int BB>
 __device__ bool team_reduce(const BProb &P, int m, int base, double (&v)[NV], unsigned &phase, BQueue *q,
                             volatile const int *abort_flag)
 {
-    __shared__ double sh[BB / 32];
-    __shared__ double tot[NV];
+    static_assert(BB / 32 <= 16, "at most 16 warps per block");
+    RedSmem &S = red_smem();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) S.warp[base + k][threadIdx.x >> 5] = v[k];
+    }
+    __syncthreads();
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-        v[k] = block_sum<double>(v[k], sh);
-        if (threadIdx.x == 0) P.part[(base + k) * P.team + m] = v[k];
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < BB / 32; ++w) s += S.warp[base + k][w];
+        v[k] = s;
     }
-    if (!team_barrier(P, phase, q, abort_flag)) return false;
+    if (P.team > 1 && threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) P.part[(base + k) * P.team + m] = v[k];
+    }
+    if (!team_barrier(P, phase, q, abort_flag, false)) return false;
     if (P.team == 1) return true;
     if (threadIdx.x < 32) {
         const volatile double *part = P.part;
@@ -121,233 +175,272 @@ __device__ bool team_reduce(const BProb &P, int m, int base, double (&v)[NV], un
         for (int k = 0; k < NV; ++k) {
             double s = 0.0;
             for (int u = threadIdx.x; u < P.team; u += 32) s += part[(base + k) * P.team + u];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (threadIdx.x == 0) tot[k] = s;
+            s = warp_sum(s);
+            if (threadIdx.x == 0) S.tot[base + k] = s;
         }
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = tot[k];
+    for (int k = 0; k < NV; ++k) v[k] = S.tot[base + k];
     return true;
 }
 
-// y = A x on rows [r0, r1) with TPR lanes per row; returns this thread's share of x.y.  x and y are
-// written during the launch (by this team's members), so they take plain coherent loads: no
-// __restrict__, which would let the compiler use the non-coherent read-only path
-template <class V, class X, int TPR>
-__device__ __forceinline__ double spmv_rows(const int *__restrict__ ip, const int *__restrict__ ix, const V *__restrict__ A,
-                                            const X *x, X *y, int r0, int r1)
+// CSR-stream SpMV over chunks [c0, c1): products a_q * g(col_q) into shared memory (buffer c & 1),
+// then out(row, sum) with the row's products summed in order by one thread.  Vectors that the
+// team writes during the launch take plain coherent loads (inside g).
+template <class V, class F, int BB, int NPT, class Gather, class RowOut>
+__device__ __forceinline__ void chunk_spmv(const BProb &P, const V *A, int c0, int c1, F *prod, Gather g, RowOut out)
 {
-    const int lane = threadIdx.x % TPR;
-    constexpr int GPW = 32 / TPR;
-    const int w = threadIdx.x >> 5;
-    double dot = 0.0;
-    for (int i0 = r0 + w * GPW; i0 < r1; i0 += (BB / 32) * GPW) {
-        const int i = i0 + (threadIdx.x & 31) / TPR;
-        X s = X(0);
-        if (i < r1) {
-            const int lo = ip[i], hi = ip[i + 1];
-            for (int q = lo + lane; q < hi; q += 2 * TPR) {
-                const int c0 = ix[q];
-                const V a0 = A[q];
-                const bool two = q + TPR < hi;
-                const int c1 = two ? ix[q + TPR] : c0;
-                const V a1 = two ? A[q + TPR] : V(0);
-                s += (X)a0 * x[c0];
-                if (two) s += (X)a1 * x[c1];
-            }
+    constexpr int CAP = BB * NPT;
+    for (int c = c0; c < c1; ++c) {
+        F *buf = prod + (c & 1) * CAP;
+        const int rs = P.crow[c], re = P.crow[c + 1];
+        const int qs = P.cq[c], qe = P.cq[c + 1];
+        const int row0 = rs + (int)threadIdx.x;
+        int lo0 = 0, hi0 = 0;
+        if (row0 < re) { lo0 = P.indptr[row0]; hi0 = P.indptr[row0 + 1]; }
+        int col[NPT];
+        V a[NPT];
+#pragma unroll
+        for (int t = 0; t < NPT; ++t) {
+            const int qq = qs + t * BB + (int)threadIdx.x;
+            col[t] = qq < qe ? P.indices[qq] : -1;
+            a[t] = qq < qe ? A[qq] : V(0);
         }
 #pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
-        if (lane == 0 && i < r1) {
-            y[i] = s;
-            dot += (double)x[i] * (double)s;
+        for (int t = 0; t < NPT; ++t)
+            if (col[t] >= 0) buf[t * BB + threadIdx.x] = (F)a[t] * g(col[t]);
+        __syncthreads();
+        for (int row = row0; row < re; row += BB) {
+            int lo = lo0, hi = hi0;
+            if (row != row0) { lo = P.indptr[row]; hi = P.indptr[row + 1]; }
+            F s = F(0);
+            for (int qq = lo; qq < hi; ++qq) s += buf[qq - qs];
+            out(row, s);
         }
-    }
-    return dot;
-}
-
-template <class V, class X>
-__device__ double spmv_dispatch(int tpr, const int *ip, const int *ix, const V *A, const X *x, X *y, int r0, int r1)
-{
-    switch (tpr) {
-    case 2: return spmv_rows<V, X, 2>(ip, ix, A, x, y, r0, r1);
-    case 4: return spmv_rows<V, X, 4>(ip, ix, A, x, y, r0, r1);
-    case 8: return spmv_rows<V, X, 8>(ip, ix, A, x, y, r0, r1);
-    case 16: return spmv_rows<V, X, 16>(ip, ix, A, x, y, r0, r1);
-    default: return spmv_rows<V, X, 32>(ip, ix, A, x, y, r0, r1);
     }
 }
 
-// residual r64 = b - A64 x on [r0, r1): returns the shares of ||r||^2, and (mixed) of r32.(inv r32)
-// after writing r32 = (float) r (mixed) or r64 (FP64 mode, into P.r64)
-template <int TPR>
-__device__ __forceinline__ void residual_rows(const BProb &P, int r0, int r1, bool mixed, double &rr, double &rz)
+// the FP64 residual r = b - A64 x on chunks [c0, c1): stores r and z = inv r (FP32 copies in
+// mixed mode), adds the shares of ||r||^2 (FP64) and r.z
+template <int BB, int NPT, bool MIXED>
+__device__ __forceinline__ void residual_chunks(const BProb &P, int c0, int c1, double *prod, double &rr, double &rz)
 {
-    const int lane = threadIdx.x % TPR;
-    constexpr int GPW = 32 / TPR;
-    const int w = threadIdx.x >> 5;
-    for (int i0 = r0 + w * GPW; i0 < r1; i0 += (BB / 32) * GPW) {
-        const int i = i0 + (threadIdx.x & 31) / TPR;
-        double s = 0.0;
-        if (i < r1)
-            for (int q = P.indptr[i] + lane; q < P.indptr[i + 1]; q += TPR) s += P.A64[q] * P.x[P.indices[q]];
-#pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
-        if (lane == 0 && i < r1) {
+    const double *x = P.x;
+    chunk_spmv<double, double, BB, NPT>(
+        P, P.A64, c0, c1, prod, [&](int j) { return x[j]; },
+        [&](int i, double s) {
             const double ri = P.b[i] - s;
             rr += ri * ri;
-            if (mixed) {
-                const float rf = (float)ri;
+            if (MIXED) {
+                const float rf = (float)ri, zf = P.inv32[i] * rf;
                 P.r32[i] = rf;
-                rz += (double)(rf * rf * P.inv32[i]);
+                P.z32[i] = zf;
+                rz += (double)rf * (double)zf;
             } else {
+                const double zi = P.inv64[i] * ri;
                 P.r64[i] = ri;
-                rz += ri * ri * P.inv64[i];
+                P.z64[i] = zi;
+                rz += ri * zi;
             }
+        });
+}
+
+// r -= alpha Ap, acc += alpha p (x in FP64 mode, the correction d in mixed mode), z = inv r on
+// [r0, r1); two rows per thread per pass with all loads issued first
+template <class F, int BB>
+__device__ __forceinline__ void update_rows(F *r, F *z, const F *Ap, const F *inv, F *acc, const F *p, F alpha, int r0, int r1,
+                                            double &rr, double &rz)
+{
+    for (int i = r0 + (int)threadIdx.x; i < r1; i += 2 * BB) {
+        const int j = i + BB;
+        const bool two = j < r1;
+        F ri = r[i], api = Ap[i], ivi = inv[i], ai = acc[i], pi = p[i];
+        F rj = F(0), apj = F(0), ivj = F(0), aj = F(0), pj = F(0);
+        if (two) { rj = r[j]; apj = Ap[j]; ivj = inv[j]; aj = acc[j]; pj = p[j]; }
+        ri -= alpha * api;
+        const F zi = ivi * ri;
+        r[i] = ri;
+        z[i] = zi;
+        acc[i] = ai + alpha * pi;
+        rr += (double)ri * (double)ri;
+        rz += (double)ri * (double)zi;
+        if (two) {
+            rj -= alpha * apj;
+            const F zj = ivj * rj;
+            r[j] = rj;
+            z[j] = zj;
+            acc[j] = aj + alpha * pj;
+            rr += (double)rj * (double)rj;
+            rz += (double)rj * (double)zj;
         }
     }
 }
 
-__device__ void residual_dispatch(const BProb &P, int r0, int r1, bool mixed, double &rr, double &rz)
+// rank m of the member's team: advance the solve by at most q->iters iterations; false when the
+// batch has to stop
+template <bool MIXED, int BB, int NPT>
+__device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const int *abort_flag, double *prod64)
 {
-    switch (P.tpr) {
-    case 2: residual_rows<2>(P, r0, r1, mixed, rr, rz); break;
-    case 4: residual_rows<4>(P, r0, r1, mixed, rr, rz); break;
-    case 8: residual_rows<8>(P, r0, r1, mixed, rr, rz); break;
-    case 16: residual_rows<16>(P, r0, r1, mixed, rr, rz); break;
-    default: residual_rows<32>(P, r0, r1, mixed, rr, rz); break;
-    }
-}
-
-// one problem, as member m of its team; returns false when the batch has to stop
-template <bool MIXED>
-__device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const int *abort_flag)
-{
-    const int n = P.n, T = P.team;
-    const int r0 = (int)((long long)n * m / T), r1 = (int)((long long)n * (m + 1) / T);
+    using F = typename std::conditional<MIXED, float, double>::type;
+    F *prod = reinterpret_cast<F *>(prod64);
+    const int T = P.team;
+    const int c0 = (int)((long long)P.nch * m / T), c1 = (int)((long long)P.nch * (m + 1) / T);
+    const int r0 = P.crow[c0], r1 = P.crow[c1];
+    F *r = MIXED ? (F *)P.r32 : (F *)P.r64;
+    F *z = MIXED ? (F *)P.z32 : (F *)P.z64;
+    F *pa = MIXED ? (F *)P.pa32 : (F *)P.pa64;
+    F *pb = MIXED ? (F *)P.pb32 : (F *)P.pb64;
+    F *Ap = MIXED ? (F *)P.Ap32 : (F *)P.Ap64;
+    const F *inv = MIXED ? (const F *)P.inv32 : (const F *)P.inv64;
+    const F *A = MIXED ? (const F *)P.A32 : (const F *)P.A64;
+    F *acc = MIXED ? (F *)P.d32 : (F *)P.x;
     unsigned phase = 0;
-    // start: x = x0 (given), r = b - A x, nb, rz, p = inv r; d = 0 (mixed)
-    {
-        double v[3] = {0.0, 0.0, 0.0};                     // ||r||^2, r.z, ||b||^2
-        residual_dispatch(P, r0, r1, MIXED, v[0], v[1]);
-        __syncthreads();                                   // r is written by row-group leaders, read strided
-        for (int i = r0 + threadIdx.x; i < r1; i += BB) {
-            v[2] += P.b[i] * P.b[i];
-            if (MIXED) { P.p32[i] = P.inv32[i] * P.r32[i]; P.d32[i] = 0.0f; }
-            else P.p64[i] = P.inv64[i] * P.r64[i];
+    const bool lead = m == 0 && threadIdx.x == 0;
+    BState S = *P.st;
+
+    if (!(S.flags & BS_STARTED)) {
+        // start: (mixed) the FP32 copies of this rank's rows; r = b - A x0, z = inv r, pold = 0
+        if (MIXED) {
+            const int q0 = P.cq[c0], q1 = P.cq[c1];
+            for (int qq = q0 + (int)threadIdx.x; qq < q1; qq += BB) P.A32[qq] = (float)P.A64[qq];
+            for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) P.inv32[i] = (float)P.inv64[i];
+            __syncthreads();                              // inv32 is read by the row owners below
         }
-        if (!team_reduce<3>(P, m, 0, v, phase, q, abort_flag)) return false;
+        double v[3] = {0.0, 0.0, 0.0};                    // ||r||^2, r.z, ||b||^2
+        residual_chunks<BB, NPT, MIXED>(P, c0, c1, prod64, v[0], v[1]);
+        for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) {
+            const double bi = P.b[i];
+            v[2] += bi * bi;
+            pb[i] = F(0);
+            if (MIXED) P.d32[i] = 0.0f;
+        }
+        if (!team_reduce<3, BB>(P, m, 0, v, phase, q, abort_flag)) return false;
         const double nb = sqrt(v[2]), rn0 = sqrt(v[0]);
+        S.flags = BS_STARTED;
+        S.it = 0;
+        S.rus = 0;
+        S.beta = 0.0;
+        S.rz = v[1];
+        S.maxr = rn0;
+        S.nb = nb;
+        S.res = nb == 0.0 ? 0.0 : rn0 / nb;
         if (nb == 0.0) {
-            for (int i = r0 + threadIdx.x; i < r1; i += BB) P.x[i] = 0.0;
-            if (m == 0 && threadIdx.x == 0) { P.res_i[0] = 0; P.res_i[1] = 1; P.res_i[2] = 0; P.res_d[0] = 0.0; }
+            for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) P.x[i] = 0.0;
+            S.flags |= BS_DONE | BS_CONVERGED;
+        } else if (rn0 <= P.tol * nb) {
+            S.flags |= BS_DONE | BS_CONVERGED;
+        } else if (!(S.rz > 0.0)) {
+            S.flags |= BS_BREAKDOWN;
+        }
+        if (S.flags & BS_DONE) {
+            if (lead) *P.st = S;
             return true;
         }
-        if (rn0 <= P.tol * nb) {
-            if (m == 0 && threadIdx.x == 0) { P.res_i[0] = 0; P.res_i[1] = 1; P.res_i[2] = 0; P.res_d[0] = rn0 / nb; }
-            return true;
-        }
-        double rz = v[1], maxr = rn0, rz_prev = rz;
-        int it = 0, breakdown = 0, rus = 0;
-        bool done = false;
-        double res_final = rn0 / nb;
-        if (!(rz > 0.0)) { breakdown = 1; done = true; }
-        while (!done && it < P.max_iter) {
-            // Ap = A p, p.Ap
-            double pap[1];
-            pap[0] = MIXED ? spmv_dispatch<float, float>(P.tpr, P.indptr, P.indices, P.A32, P.p32, P.Ap32, r0, r1)
-                           : spmv_dispatch<double, double>(P.tpr, P.indptr, P.indices, P.A64, P.p64, P.Ap64, r0, r1);
-            if (!team_reduce<1>(P, m, 3, pap, phase, q, abort_flag)) return false;
-            if (!(pap[0] > 0.0)) { breakdown = 1; break; }
-            const double alpha = rz / pap[0];
-            // x (or d) += alpha p, r -= alpha Ap; ||r||^2, r.z
-            double u[2] = {0.0, 0.0};
-            for (int i = r0 + threadIdx.x; i < r1; i += BB) {
-                if (MIXED) {
-                    const float af = (float)alpha;
-                    const float ri = P.r32[i] - af * P.Ap32[i];
-                    P.r32[i] = ri;
-                    P.d32[i] += af * P.p32[i];
-                    u[0] += (double)(ri * ri);
-                    u[1] += (double)(ri * ri * P.inv32[i]);
-                } else {
-                    const double ri = P.r64[i] - alpha * P.Ap64[i];
-                    P.r64[i] = ri;
-                    P.x[i] += alpha * P.p64[i];
-                    u[0] += ri * ri;
-                    u[1] += ri * ri * P.inv64[i];
+    }
+    double rz = S.rz, beta = S.beta, maxr = S.maxr, res = S.res;
+    const double nb = S.nb;
+    int it = S.it, rus = S.rus;
+    bool brk = (S.flags & BS_BREAKDOWN) != 0, done = false;
+    const long long it_lim = (long long)it + q->iters;
+    const int it_end = it_lim < (long long)P.max_iter ? (int)it_lim : P.max_iter;
+    F *pold = (it & 1) ? pa : pb, *pnew = (it & 1) ? pb : pa;
+    while (!brk && !done && it < it_end) {
+        double pap[1] = {0.0};
+        const F fb = (F)beta;
+        chunk_spmv<F, F, BB, NPT>(
+            P, A, c0, c1, prod, [&](int j) { return pdir(z, pold, fb, j); },
+            [&](int i, F s) {
+                const F pi = pdir(z, pold, fb, i);
+                pnew[i] = pi;
+                Ap[i] = s;
+                pap[0] += (double)pi * (double)s;
+            });
+        if (!team_reduce<1, BB>(P, m, 3, pap, phase, q, abort_flag)) return false;
+        if (!(pap[0] > 0.0)) { brk = true; break; }
+        const double alpha = rz / pap[0];
+        double u[2] = {0.0, 0.0};                         // ||r||^2, r.z
+        update_rows<F, BB>(r, z, Ap, inv, acc, pnew, (F)alpha, r0, r1, u[0], u[1]);
+        if (!team_reduce<2, BB>(P, m, 4, u, phase, q, abort_flag)) return false;
+        ++it;
+        const double rn = sqrt(u[0]);
+        if (!MIXED) {
+            res = rn / nb;
+            if (rn <= P.tol * nb) { done = true; break; }
+            beta = u[1] / rz;
+            rz = u[1];
+            if (!(rz > 0.0)) { brk = true; break; }
+        } else {
+            const bool ru = rn <= 0.1 * maxr || rn <= P.tol * nb || it >= P.max_iter || !(u[1] > 0.0);
+            if (ru) {
+                // reliable update: x += d, d = 0; r = b - A64 x in FP64, r32 = (float) r
+                for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) {
+                    P.x[i] += (double)P.d32[i];
+                    P.d32[i] = 0.0f;
                 }
-            }
-            if (!team_reduce<2>(P, m, 4, u, phase, q, abort_flag)) return false;
-            ++it;
-            const double rn = sqrt(u[0]);
-            double beta;
-            if (!MIXED) {
-                res_final = rn / nb;
-                if (rn <= P.tol * nb) { done = true; break; }
+                if (!team_barrier(P, phase, q, abort_flag, true)) return false;
+                double w[2] = {0.0, 0.0};
+                residual_chunks<BB, NPT, true>(P, c0, c1, prod64, w[0], w[1]);
+                if (!team_reduce<2, BB>(P, m, 6, w, phase, q, abort_flag)) return false;
+                ++rus;
+                const double rt = sqrt(w[0]);
+                res = rt / nb;
+                maxr = rt;
+                if (rt <= P.tol * nb || it >= P.max_iter) { done = true; break; }
+                if (!(w[1] > 0.0)) { brk = true; break; }
+                beta = w[1] / rz;
+                rz = w[1];
+            } else {
                 beta = u[1] / rz;
                 rz = u[1];
-                if (!(rz > 0.0)) { breakdown = 1; break; }
-            } else {
-                const bool ru = rn <= 0.1 * maxr || rn <= P.tol * nb || it >= P.max_iter || !(u[1] > 0.0);
-                if (ru) {
-                    // reliable update: x += d, d = 0; r = b - A64 x (FP64), r32 = (float) r
-                    for (int i = r0 + threadIdx.x; i < r1; i += BB) { P.x[i] += (double)P.d32[i]; P.d32[i] = 0.0f; }
-                    if (!team_barrier(P, phase, q, abort_flag)) return false;
-                    double w2[2] = {0.0, 0.0};
-                    residual_dispatch(P, r0, r1, true, w2[0], w2[1]);
-                    if (!team_reduce<2>(P, m, 6, w2, phase, q, abort_flag)) return false;
-                    ++rus;
-                    const double rt = sqrt(w2[0]);
-                    res_final = rt / nb;
-                    maxr = rt;
-                    if (rt <= P.tol * nb || it >= P.max_iter) { done = true; break; }
-                    if (!(w2[1] > 0.0)) { breakdown = 1; break; }
-                    beta = w2[1] / rz;
-                    rz = w2[1];
-                } else {
-                    rz_prev = rz;
-                    beta = u[1] / rz;
-                    rz = u[1];
-                }
             }
-            (void)rz_prev;
-            // p = inv r + beta p
-            for (int i = r0 + threadIdx.x; i < r1; i += BB) {
-                if (MIXED) P.p32[i] = P.inv32[i] * P.r32[i] + (float)beta * P.p32[i];
-                else P.p64[i] = P.inv64[i] * P.r64[i] + beta * P.p64[i];
-            }
-            if (!team_barrier(P, phase, q, abort_flag)) return false;
         }
-        // the true residual for the FP64 path (cg.hpp:222-237): r = b - A x
+        F *t = pold;
+        pold = pnew;
+        pnew = t;
+    }
+    const bool finished = brk || done || it >= P.max_iter;
+    if (finished) {
         if (!MIXED) {
-            if (!team_barrier(P, phase, q, abort_flag)) return false;
-            double w3[2] = {0.0, 0.0};
-            residual_dispatch(P, r0, r1, false, w3[0], w3[1]);
-            if (!team_reduce<2>(P, m, 6, w3, phase, q, abort_flag)) return false;
-            res_final = sqrt(w3[0]) / nb;
-        } else if (breakdown) {
-            for (int i = r0 + threadIdx.x; i < r1; i += BB) { P.x[i] += (double)P.d32[i]; P.d32[i] = 0.0f; }
+            // the true residual (cg.hpp:222-237): every rank's x is final at the last reduction
+            double w[2] = {0.0, 0.0};
+            residual_chunks<BB, NPT, false>(P, c0, c1, prod64, w[0], w[1]);
+            if (!team_reduce<2, BB>(P, m, 6, w, phase, q, abort_flag)) return false;
+            res = sqrt(w[0]) / nb;
+        } else if (brk) {
+            for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) {
+                P.x[i] += (double)P.d32[i];
+                P.d32[i] = 0.0f;
+            }
         }
-        if (m == 0 && threadIdx.x == 0) {
+    }
+    if (lead) {
+        S.rz = rz;
+        S.beta = beta;
+        S.maxr = maxr;
+        S.res = res;
+        S.it = it;
+        S.rus = rus;
+        if (brk) S.flags |= BS_BREAKDOWN;
+        if (finished) {
             const double tol = P.tol;
-            int conv = !breakdown && res_final <= tol * (1.0 + 1e-6) + 1e-15;
-            if (!conv && !breakdown && res_final <= 10.0 * tol && it < P.max_iter) conv = 1;
-            P.res_i[0] = it; P.res_i[1] = conv; P.res_i[2] = breakdown; P.res_i[4] = rus;
-            P.res_d[0] = res_final;
+            int conv = !brk && res <= tol * (1.0 + 1e-6) + 1e-15;
+            if (!conv && !brk && res <= 10.0 * tol && it < P.max_iter) conv = 1;
+            S.flags |= BS_DONE | (conv ? BS_CONVERGED : 0);
         }
+        *P.st = S;
     }
     return true;
 }
 
-template <bool MIXED>
-__global__ void __launch_bounds__(BB) k_batch_pcg(const BProb *__restrict__ probs, const int *__restrict__ slot_prob,
-                                                  const int *__restrict__ slot_member, int nslots, BQueue *q,
-                                                  volatile const int *abort_flag)
+template <bool MIXED, int BB, int NPT>
+__global__ void __launch_bounds__(BB, 1024 / BB) k_batch_pcg(const BProb *__restrict__ probs, const int *__restrict__ slot_prob,
+                                                             const int *__restrict__ slot_member, BQueue *q,
+                                                             volatile const int *abort_flag)
 {
+    __shared__ double prod[2 * BB * NPT];
     __shared__ int s_slot, s_stop;
+    const int nslots = q->nslots;
     for (;;) {
         if (threadIdx.x == 0) {
             s_slot = (int)atomicAdd(&q->next, 1u);
@@ -357,46 +450,141 @@ __global__ void __launch_bounds__(BB) k_batch_pcg(const BProb *__restrict__ prob
         const int slot = s_slot, stop = s_stop;
         __syncthreads();
         if (slot >= nslots || stop) return;
-        const BProb P = probs[slot_prob[slot]];
-        if (!solve_member<MIXED>(P, slot_member[slot], q, abort_flag)) {
-            if (threadIdx.x == 0) P.res_i[3] = *(volatile int *)&q->flag ? *(volatile int *)&q->flag : FEMD_ETIMEOUT;
+        const BProb &P = probs[slot_prob[slot]];
+        if (!solve_member<MIXED, BB, NPT>(P, slot_member[slot], q, abort_flag, prod)) {
+            if (threadIdx.x == 0) {
+                const int f = *(volatile int *)&q->flag;
+                P.st->status = f ? f : FEMD_ETIMEOUT;
+            }
             return;
         }
     }
 }
 
-// f32 copies of a matrix's values and inverse diagonal
-__global__ void k_batch_f32(const double *__restrict__ a, float *__restrict__ b, long long n)
+// chunk tables of one matrix: chunk k starts at the first row whose first nonzero is at or after
+// k * cp (cp = chunk capacity - longest row), so no chunk holds more than the capacity
+__global__ void k_chunk_table(const int *__restrict__ indptr, int n, int nnz, int cp, int nch, int *crow, int *cq)
 {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        b[i] = (float)a[i];
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > nch) return;
+    if (k == nch) { crow[k] = n; cq[k] = nnz; return; }
+    const long long key = (long long)k * cp;
+    int lo = 0, hi = n;                                    // first i in [0, n] with indptr[i] >= key
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (indptr[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    crow[k] = lo;
+    cq[k] = indptr[lo];
+}
+
+__device__ __forceinline__ int warp_max(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void k_max_row(const int *__restrict__ indptr, int n, int *out)
+{
+    int m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, indptr[i + 1] - indptr[i]);
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+using BatchKernel = void (*)(const BProb *, const int *, const int *, BQueue *, volatile const int *);
+
+template <bool MIXED>
+static BatchKernel batch_kernel_m(int block, int npt)
+{
+#define FEMD_BK(B_, N_) if (block == B_ && npt == N_) return k_batch_pcg<MIXED, B_, N_>;
+    FEMD_BK(128, 2) FEMD_BK(128, 4) FEMD_BK(128, 8)
+    FEMD_BK(256, 2) FEMD_BK(256, 4) FEMD_BK(256, 8)
+    FEMD_BK(512, 2) FEMD_BK(512, 4)
+#undef FEMD_BK
+    return nullptr;
+}
+static BatchKernel batch_kernel(bool mixed, int block, int npt)
+{
+    return mixed ? batch_kernel_m<true>(block, npt) : batch_kernel_m<false>(block, npt);
 }
 
 }  // namespace femd
 
 using namespace femd;
 
+namespace {
+
+struct Member {
+    femd_matrix K = nullptr;
+    bool armed = false;
+    int n = 0, team = 1, nch = 0, maxlen = 0;
+    long long nnz = 0;
+    DevBuf<int> tables;                         // crow (nch+1), cq (nch+1)
+    float *f32 = nullptr;                       // A32, inv32, r, z, p, p', Ap, d
+    double *f64 = nullptr;                      // r, z, p, p', Ap
+    const double *b = nullptr;
+    double *x = nullptr;
+    double tol = 0.0;
+    int max_iter = 0;
+};
+
+}  // namespace
+
 struct femd_batch_s : femd::HandleBase {
     femd_ctx ctx = nullptr;
-    int nprob = 0;
-    std::vector<femd_matrix> mats;
-    std::vector<int> team, tpr;
-    std::vector<int> order;                    // problems, largest teams first
+    std::vector<std::unique_ptr<Member>> mem;   // index = member id (null: free)
+    // launch shape: threads per block, nonzeros per team rank, nonzeros per thread per chunk
+    int block = 256, nnz_per_block = 65536, npt = 4;
+    int grid = 0;
+    int cap = 0;                                // member capacity of the device arrays
+    size_t slot_cap = 0;                        // slot capacity of the device arrays
     DevBuf<BProb> d_probs;
-    DevBuf<int> d_slot_prob, d_slot_member, d_res_i;
-    DevBuf<double> d_res_d, d_part;
+    DevBuf<BState> d_state;
     DevBuf<unsigned> d_bar;
+    DevBuf<int> d_slots;                        // slot_prob then slot_member (2 x slot_cap)
+    DevBuf<double> d_part;
     DevBuf<BQueue> d_queue;
-    DevBuf<float> f32;                          // all problems' FP32 values, inv, r, p, Ap, d
-    DevBuf<double> f64;                         // all problems' FP64 r, p, Ap
-    std::vector<BProb> probs;
-    int nslots = 0, grid = 0, team_target = 0;
-    int ghost = -1;                             // test hook: this problem waits for a member that never comes
+    DevBuf<int> d_scratch;
+    size_t part_cap = 0;
+    // pinned staging of a launch: descriptors, slots and queue in, states out
+    void *pinned = nullptr;
+    BProb *h_desc = nullptr;
+    BState *h_state = nullptr;
+    int *h_slots = nullptr;
+    BQueue *h_q0 = nullptr, *h_qout = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int graph_state[2] = {0, 0};                // 0 none, 1 captured, -1 capture refused (direct launches)
+    int ghost = -1;                             // test hook: this member waits for a rank that never comes
     long long spin_limit = SPIN_LIMIT;
     int *abort_host = nullptr;                  // mapped pinned flag
     int *abort_dev = nullptr;
     femd_batch_s() : HandleBase(femd::KIND_BATCH) {}
-    ~femd_batch_s() override { if (abort_host) cudaFreeHost(abort_host); }
+    void drop_graphs()
+    {
+        for (int k = 0; k < 2; ++k) {
+            if (exec[k]) cudaGraphExecDestroy(exec[k]);
+            exec[k] = nullptr;
+            graph_state[k] = 0;
+        }
+    }
+    void free_vectors(Member &M)
+    {
+        if (M.f32) cudaFreeAsync(M.f32, ctx->stream);
+        if (M.f64) cudaFreeAsync(M.f64, ctx->stream);
+        M.f32 = nullptr;
+        M.f64 = nullptr;
+    }
+    ~femd_batch_s() override
+    {
+        drop_graphs();
+        for (auto &M : mem)
+            if (M) free_vectors(*M);
+        if (ctx) cudaStreamSynchronize(ctx->stream);
+        if (abort_host) cudaFreeHost(abort_host);
+        if (pinned) cudaFreeHost(pinned);
+    }
 };
 
 static femd_batch_s *as_batch(void *h)
@@ -405,107 +593,455 @@ static femd_batch_s *as_batch(void *h)
     return (b && b->kind == KIND_BATCH) ? b : nullptr;
 }
 
+static int chunk_cap(const femd_batch_s *B) { return B->block * B->npt; }
+
+// a member's team size and chunk tables for the current launch shape
+static int member_layout(femd_batch_s *B, Member &M)
+{
+    cudaStream_t s = B->ctx->stream;
+    const int C = chunk_cap(B);
+    FEMD_CHECK_ARG(M.maxlen <= C / 2, "batch: a row is longer than half the SpMV chunk (block x nonzeros per thread)");
+    const int cp = C - M.maxlen;
+    const int nch = (int)std::max<long long>(1, (M.nnz + cp - 1) / cp);
+    if (M.tables.n < 2 * (size_t)(nch + 1)) {
+        int st = M.tables.alloc(2 * (size_t)(nch + 1));
+        if (st) return st;
+    }
+    M.nch = nch;
+    k_chunk_table<<<grid_for((size_t)nch + 1, 256), 256, 0, counted(s)>>>(M.K->pattern->indptr.p, M.n, (int)M.nnz, cp, nch,
+                                                                          M.tables.p, M.tables.p + nch + 1);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    int T = (int)std::min<long long>((M.nnz + B->nnz_per_block - 1) / B->nnz_per_block, (long long)B->grid / 2);
+    M.team = std::max(1, std::min(T, std::min(nch, std::max(1, M.n / 64))));
+    return FEMD_OK;
+}
+
+static int grow_arrays(femd_batch_s *B, int cap)
+{
+    if (cap <= B->cap) return FEMD_OK;
+    cap = std::max(cap, 2 * B->cap);
+    int st;
+    if ((st = B->d_probs.alloc(cap)) || (st = B->d_bar.alloc(cap))) return st;
+    {
+        // members may be part-way through a resumable solve: keep their states
+        BState *ns = nullptr;
+        cudaError_t e = cudaMalloc(&ns, (size_t)cap * sizeof(BState));
+        if (e != cudaSuccess) { cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
+        cudaStream_t s = B->ctx->stream;
+        e = cudaMemsetAsync(ns, 0, (size_t)cap * sizeof(BState), s);
+        if (e == cudaSuccess && B->d_state.p)
+            e = cudaMemcpyAsync(ns, B->d_state.p, B->d_state.n * sizeof(BState), cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { cudaFree(ns); set_error(std::string("batch: ") + cudaGetErrorString(e)); return FEMD_ECUDA; }
+        B->d_state.release();
+        B->d_state.p = ns;
+        B->d_state.n = (size_t)cap;
+    }
+    if (B->pinned) cudaFreeHost(B->pinned);
+    B->pinned = nullptr;
+    B->cap = 0;
+    const size_t pin = (size_t)cap * (sizeof(BProb) + sizeof(BState)) + 2 * sizeof(BQueue) + 64;
+    FEMD_TRY_CUDA(cudaHostAlloc(&B->pinned, pin, cudaHostAllocDefault));
+    char *c = static_cast<char *>(B->pinned);
+    B->h_desc = reinterpret_cast<BProb *>(c); c += (size_t)cap * sizeof(BProb);
+    B->h_state = reinterpret_cast<BState *>(c); c += (size_t)cap * sizeof(BState);
+    B->h_q0 = reinterpret_cast<BQueue *>(c); c += sizeof(BQueue);
+    B->h_qout = reinterpret_cast<BQueue *>(c);
+    std::memset(B->h_desc, 0, (size_t)cap * sizeof(BProb));
+    B->cap = cap;
+    B->drop_graphs();
+    return FEMD_OK;
+}
+
+static int grow_slots(femd_batch_s *B, size_t need)
+{
+    if (need <= B->slot_cap) return FEMD_OK;
+    need = std::max(need, 2 * B->slot_cap);
+    int st;
+    if ((st = B->d_slots.alloc(2 * need)) || (st = B->d_part.alloc(8 * need + 8))) return st;
+    if (B->h_slots) cudaFreeHost(B->h_slots);
+    B->h_slots = nullptr;
+    FEMD_TRY_CUDA(cudaHostAlloc(&B->h_slots, 2 * need * sizeof(int), cudaHostAllocDefault));
+    B->slot_cap = need;
+    B->drop_graphs();
+    return FEMD_OK;
+}
+
+static int batch_shape(femd_batch_s *B)
+{
+    int bps = 0, bps64 = 0;
+    FEMD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_kernel(true, B->block, B->npt), B->block, 0));
+    FEMD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps64, batch_kernel(false, B->block, B->npt), B->block, 0));
+    bps = std::min(bps, bps64);
+    FEMD_CHECK_ARG(bps >= 1, "batch: the batch kernel does not fit on an SM");
+    B->grid = bps * B->ctx->sm_count;
+    size_t slots = 0;
+    for (auto &up : B->mem)
+        if (up) {
+            int st = member_layout(B, *up);
+            if (st) return st;
+            slots += (size_t)up->team;
+        }
+    FEMD_TRY_CUDA(cudaStreamSynchronize(B->ctx->stream));
+    B->drop_graphs();
+    return grow_slots(B, std::max<size_t>(slots, 1));
+}
+
+static int add_member(femd_batch_s *B, femd_matrix K, int *id_out)
+{
+    FEMD_CHECK_ARG(K && K->kind == KIND_MATRIX, "batch: not a matrix handle");
+    FEMD_CHECK_ARG(K->ctx == B->ctx, "batch: the matrix belongs to another context");
+    FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "batch: the matrices must be square");
+    FEMD_CHECK_ARG(K->pattern->nrows >= 1, "batch: empty matrix");
+    FEMD_CHECK_ARG(K->pattern->nnz < INT_MAX, "batch: more than 2^31 nonzeros");
+    int id = -1;
+    for (size_t i = 0; i < B->mem.size(); ++i)
+        if (!B->mem[i]) { id = (int)i; break; }
+    if (id < 0) { id = (int)B->mem.size(); B->mem.emplace_back(); }
+    int st;
+    if ((st = grow_arrays(B, (int)B->mem.size()))) return st;
+    B->mem[id].reset(new Member());
+    Member &M = *B->mem[id];
+    M.K = K;
+    M.n = K->pattern->nrows;
+    M.nnz = K->pattern->nnz;
+    cudaStream_t s = B->ctx->stream;
+    FEMD_TRY_CUDA(cudaMemsetAsync(B->d_scratch.p, 0, sizeof(int), s));
+    k_max_row<<<grid_for((size_t)M.n, 256, 1024), 256, 0, counted(s)>>>(K->pattern->indptr.p, M.n, B->d_scratch.p);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&M.maxlen, B->d_scratch.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    if ((st = member_layout(B, M))) { B->mem[id].reset(); return st; }
+    size_t slots = 0;
+    for (auto &X : B->mem)
+        if (X) slots += (size_t)X->team;
+    if ((st = grow_slots(B, slots))) { B->mem[id].reset(); return st; }
+    *id_out = id;
+    return FEMD_OK;
+}
+
+// the member's vectors of one precision (stream-ordered allocation on the first use)
+static int member_vectors(femd_batch_s *B, Member &M, bool mixed)
+{
+    cudaStream_t s = B->ctx->stream;
+    const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
+    if (mixed && !M.f32) {
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 7 * n + 32) * sizeof(float), s);
+        if (e != cudaSuccess) { M.f32 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
+    }
+    if (!mixed && !M.f64) {
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f64), (5 * n + 8) * sizeof(double), s);
+        if (e != cudaSuccess) { M.f64 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
+    }
+    return FEMD_OK;
+}
+
+static BProb describe(femd_batch_s *B, int id, bool mixed)
+{
+    Member &M = *B->mem[id];
+    BProb P{};
+    P.n = M.n;
+    P.team = M.team;
+    P.max_iter = M.max_iter;
+    P.nch = M.nch;
+    P.tol = M.tol;
+    P.indptr = M.K->pattern->indptr.p;
+    P.indices = M.K->pattern->indices.p;
+    P.crow = M.tables.p;
+    P.cq = M.tables.p + M.nch + 1;
+    P.A64 = M.K->data.p;
+    P.inv64 = M.K->inv.p;
+    const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
+    if (mixed) {
+        float *f = M.f32;
+        P.A32 = f; f += nnz;
+        f = M.f32 + ((nnz + 7) & ~(size_t)7);
+        P.inv32 = f; f += n;
+        P.r32 = f; f += n;
+        P.z32 = f; f += n;
+        P.pa32 = f; f += n;
+        P.pb32 = f; f += n;
+        P.Ap32 = f; f += n;
+        P.d32 = f;
+    } else {
+        double *d = M.f64;
+        P.r64 = d; d += n;
+        P.z64 = d; d += n;
+        P.pa64 = d; d += n;
+        P.pb64 = d; d += n;
+        P.Ap64 = d;
+    }
+    P.b = M.b;
+    P.x = M.x;
+    P.bar = B->d_bar.p + id;
+    P.st = B->d_state.p + id;
+    return P;
+}
+
+static cudaError_t launch_batch(femd_batch_s *B, bool mixed, cudaStream_t s)
+{
+    const BProb *probs = B->d_probs.p;
+    const int *sp = B->d_slots.p, *sm = B->d_slots.p + B->slot_cap;
+    BQueue *q = B->d_queue.p;
+    volatile const int *ab = B->abort_dev;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)B->grid);
+    cfg.blockDim = dim3((unsigned)B->block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, batch_kernel(mixed, B->block, B->npt), probs, sp, sm, q, ab);
+}
+
+// one launch's device work: descriptors, slots and queue in, the launch, states out
+static cudaError_t enqueue_step(femd_batch_s *B, bool mixed, cudaStream_t s)
+{
+    cudaError_t e;
+    const size_t cap = (size_t)B->cap;
+    if ((e = cudaMemcpyAsync(B->d_probs.p, B->h_desc, cap * sizeof(BProb), cudaMemcpyHostToDevice, s))) return e;
+    if ((e = cudaMemcpyAsync(B->d_slots.p, B->h_slots, 2 * B->slot_cap * sizeof(int), cudaMemcpyHostToDevice, s))) return e;
+    if ((e = cudaMemsetAsync(B->d_bar.p, 0, cap * sizeof(unsigned), s))) return e;
+    if ((e = cudaMemcpyAsync(B->d_queue.p, B->h_q0, sizeof(BQueue), cudaMemcpyHostToDevice, s))) return e;
+    if ((e = launch_batch(B, mixed, s))) return e;
+    if ((e = cudaMemcpyAsync(B->h_state, B->d_state.p, cap * sizeof(BState), cudaMemcpyDeviceToHost, s))) return e;
+    return cudaMemcpyAsync(B->h_qout, B->d_queue.p, sizeof(BQueue), cudaMemcpyDeviceToHost, s);
+}
+
+static void fill_result(const BState &S, femd_cg_result &r, double seconds)
+{
+    r.iterations = S.it;
+    r.converged = (S.flags & BS_CONVERGED) ? 1 : 0;
+    r.breakdown = (S.flags & BS_BREAKDOWN) ? 1 : 0;
+    r.status = S.status;
+    r.outer = S.rus;
+    r.residual = S.res;
+    r.seconds = seconds;
+}
+
+// one launch over the armed members: each advances by at most iters iterations.  Members that
+// finish are disarmed and listed (ids, results) when the lists are given.
+static int batch_step(femd_ctx ctx, femd_batch_s *B, int iters, bool mx, int *nfinished, int *fin_ids, femd_cg_result *fin_res,
+                      double *seconds)
+{
+    cudaStream_t s = ctx->stream;
+    int st;
+    std::vector<int> order;
+    for (int id = 0; id < (int)B->mem.size(); ++id) {
+        if (!B->mem[id] || !B->mem[id]->armed) continue;
+        Member &M = *B->mem[id];
+        if ((st = member_vectors(B, M, mx))) return st;
+        order.push_back(id);
+    }
+    if (nfinished) *nfinished = 0;
+    if (seconds) *seconds = 0.0;
+    if (order.empty()) return FEMD_OK;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        if (B->mem[a]->team != B->mem[b]->team) return B->mem[a]->team > B->mem[b]->team;
+        return B->mem[a]->nnz > B->mem[b]->nnz;
+    });
+    // descriptors, slots and team scratch
+    size_t ns = 0, opart = 0;
+    for (int id : order) ns += (size_t)B->mem[id]->team + (id == B->ghost ? 1 : 0);
+    if ((st = grow_slots(B, ns + 1))) return st;
+    int *sp = B->h_slots, *sm = B->h_slots + B->slot_cap;
+    ns = 0;
+    for (int id : order) {
+        BProb P = describe(B, id, mx);
+        P.part = B->d_part.p + opart;
+        opart += 8 * (size_t)(P.team + 1);
+        for (int m = 0; m < P.team; ++m) { sp[ns] = id; sm[ns] = m; ++ns; }
+        if (id == B->ghost) P.team += 1;                // test hook (femd_cuda_batch_debug)
+        B->h_desc[id] = P;
+    }
+    if (opart > B->d_part.n) {
+        if ((st = B->d_part.alloc(opart + 8))) return st;
+        // the part pointers were set from the old buffer: redo them
+        opart = 0;
+        for (int id : order) {
+            B->h_desc[id].part = B->d_part.p + opart;
+            opart += 8 * (size_t)(B->mem[id]->team + 1);
+        }
+        B->drop_graphs();
+    }
+    *B->h_q0 = BQueue{0u, 0, B->spin_limit, (int)ns, std::max(1, iters)};
+    *(volatile int *)B->abort_host = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    FEMD_TRY_CUDA(cudaEventCreate(&e0));
+    FEMD_TRY_CUDA(cudaEventCreate(&e1));
+    cudaError_t e = cudaSuccess;
+    const int k = mx ? 1 : 0;
+    if (B->graph_state[k] == 0) {
+        cudaGraph_t g = nullptr;
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const cudaError_t e2 = enqueue_step(B, mx, s);
+            e = cudaStreamEndCapture(s, &g);
+            if (e == cudaSuccess) e = e2;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&B->exec[k], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e == cudaSuccess) {
+            B->graph_state[k] = 1;
+        } else {
+            cudaGetLastError();
+            B->exec[k] = nullptr;
+            B->graph_state[k] = -1;                     // this runtime does not capture the launch: launch directly
+            e = cudaSuccess;
+        }
+    }
+    cudaEventRecord(e0, s);
+    if (B->graph_state[k] == 1) {
+        e = launch_graph(B->exec[k], 1, s);
+    } else {
+        e = enqueue_step(B, mx, s);
+        if (e == cudaSuccess) add_launches(1);
+    }
+    cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) { set_error(std::string("batch: ") + cudaGetErrorString(e)); return FEMD_ECUDA; }
+    if (seconds) *seconds = ms * 1e-3;
+    const int flag = B->h_qout->flag;
+    int nf = 0;
+    for (int id : order) {
+        const BState &S = B->h_state[id];
+        if (!(S.flags & BS_DONE) && !flag && !S.status) continue;
+        B->mem[id]->armed = false;
+        if (fin_ids) fin_ids[nf] = id;
+        if (fin_res) {
+            fill_result(S, fin_res[nf], ms * 1e-3);
+            if (flag) fin_res[nf].status = flag;
+        }
+        ++nf;
+    }
+    if (nfinished) *nfinished = nf;
+    if (flag == FEMD_ETIMEOUT) { set_error("batch: a team barrier wait ran out"); return FEMD_ETIMEOUT; }
+    if (flag == FEMD_EABORT) { set_error("batch: aborted by the host"); return FEMD_EABORT; }
+    return FEMD_OK;
+}
+
+static int arm_member(femd_batch_s *B, int id, const double *b, double *x, int max_iter, double tol)
+{
+    FEMD_CHECK_ARG(id >= 0 && id < (int)B->mem.size() && B->mem[id], "batch: no such member");
+    FEMD_CHECK_ARG(b && x, "batch: NULL vector");
+    FEMD_CHECK_ARG(tol >= 0.0, "batch: tol < 0");
+    Member &M = *B->mem[id];
+    M.b = b;
+    M.x = x;
+    M.tol = tol;
+    M.max_iter = max_iter > 0 ? max_iter : std::max(1000, 10 * M.n);
+    M.armed = true;
+    FEMD_TRY_CUDA(cudaMemsetAsync(B->d_state.p + id, 0, sizeof(BState), B->ctx->stream));
+    return FEMD_OK;
+}
+
 extern "C" {
 
 int femd_cuda_batch_create(femd_ctx ctx, int nprob, const femd_matrix *mats, int nnz_per_block, femd_batch *out)
 {
     clear_error();
-    FEMD_CHECK_ARG(ctx && out && nprob >= 1 && mats, "batch_create: bad arguments");
+    FEMD_CHECK_ARG(ctx && out && nprob >= 0 && (mats || nprob == 0), "batch_create: bad arguments");
     *out = nullptr;
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
     auto B = new femd_batch_s();
     std::unique_ptr<femd_batch_s> guard(B);
     B->ctx = ctx;
-    B->nprob = nprob;
-    B->mats.assign(mats, mats + nprob);
-    // resident blocks (cooperative launch)
-    int bps = 0;
-    FEMD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_pcg<true>, BB, 0));
-    int bps64 = 0;
-    FEMD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps64, k_batch_pcg<false>, BB, 0));
-    bps = std::min(bps, bps64);
-    FEMD_CHECK_ARG(bps >= 1, "batch_create: the batch kernel does not fit on an SM");
-    B->grid = bps * ctx->sm_count;
-    B->team_target = nnz_per_block > 0 ? nnz_per_block : 65536;
-    size_t nf32 = 0, nf64 = 0;
-    B->team.resize(nprob);
-    B->tpr.resize(nprob);
-    for (int p = 0; p < nprob; ++p) {
-        femd_matrix K = mats[p];
-        FEMD_CHECK_ARG(K && K->kind == KIND_MATRIX, "batch_create: not a matrix handle");
-        FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "batch_create: the matrices must be square");
-        const long long nnz = K->pattern->nnz;
-        const int n = K->pattern->nrows;
-        int T = (int)std::min<long long>((nnz + B->team_target - 1) / B->team_target, (long long)B->grid / 2);
-        T = std::max(1, std::min(T, std::max(1, n / 64)));
-        B->team[p] = T;
-        const int shape = K->spmv_tpr ? K->spmv_tpr : 0;
-        const double avg = n ? (double)nnz / n : 1.0;
-        B->tpr[p] = shape ? (shape & 0xff) : (avg <= 6 ? 4 : avg <= 14 ? 8 : avg <= 28 ? 16 : 32);
-        nf32 += (size_t)nnz + 6 * (size_t)n + 16;
-        nf64 += 3 * (size_t)n + 4;
-    }
-    B->order.resize(nprob);
-    std::iota(B->order.begin(), B->order.end(), 0);
-    std::stable_sort(B->order.begin(), B->order.end(), [&](int a, int b) {
-        if (B->team[a] != B->team[b]) return B->team[a] > B->team[b];
-        return B->mats[a]->pattern->nnz > B->mats[b]->pattern->nnz;
-    });
-    std::vector<int> sp, sm;
-    for (int p : B->order)
-        for (int m = 0; m < B->team[p]; ++m) { sp.push_back(p); sm.push_back(m); }
-    B->nslots = (int)sp.size();
-    const size_t totteam = sp.size();
+    B->nnz_per_block = nnz_per_block > 0 ? nnz_per_block : 65536;
     int st;
-    if ((st = B->f32.alloc(nf32)) || (st = B->f64.alloc(nf64)) || (st = B->d_probs.alloc(nprob)) ||
-        (st = B->d_slot_prob.alloc(totteam)) || (st = B->d_slot_member.alloc(totteam)) ||
-        (st = B->d_res_i.alloc(8 * (size_t)nprob)) || (st = B->d_res_d.alloc(2 * (size_t)nprob)) ||
-        (st = B->d_part.alloc(8 * totteam + 8)) || (st = B->d_bar.alloc(nprob)) || (st = B->d_queue.alloc(1)))
-        return st;
+    if ((st = B->d_queue.alloc(1)) || (st = B->d_scratch.alloc(4))) return st;
     FEMD_TRY_CUDA(cudaHostAlloc(&B->abort_host, sizeof(int), cudaHostAllocMapped));
     *B->abort_host = 0;
     FEMD_TRY_CUDA(cudaHostGetDevicePointer(&B->abort_dev, B->abort_host, 0));
-    // carve the per-problem vectors
-    B->probs.resize(nprob);
-    size_t o32 = 0, o64 = 0, opart = 0;
-    std::vector<size_t> part_off(nprob);
-    for (int p : B->order) { part_off[p] = opart; opart += 8 * (size_t)B->team[p]; }
+    if ((st = grow_arrays(B, std::max(nprob, 4)))) return st;
+    if ((st = batch_shape(B))) return st;
     for (int p = 0; p < nprob; ++p) {
-        femd_matrix K = mats[p];
-        const int n = K->pattern->nrows;
-        const long long nnz = K->pattern->nnz;
-        BProb &P = B->probs[p];
-        P = BProb{};
-        P.n = n;
-        P.tpr = B->tpr[p];
-        P.team = B->team[p];
-        P.indptr = K->pattern->indptr.p;
-        P.indices = K->pattern->indices.p;
-        P.A64 = K->data.p;
-        P.inv64 = K->inv.p;
-        float *f = B->f32.p + o32;
-        P.A32 = f; f += nnz;
-        P.inv32 = f; f += n;
-        P.r32 = f; f += n;
-        P.p32 = f; f += n;
-        P.Ap32 = f; f += n;
-        P.d32 = f; f += n;
-        o32 += (size_t)nnz + 6 * (size_t)n + 8;
-        o32 = (o32 + 7) & ~(size_t)7;
-        double *d = B->f64.p + o64;
-        P.r64 = d; d += n;
-        P.p64 = d; d += n;
-        P.Ap64 = d;
-        o64 += 3 * (size_t)n + 4;
-        P.part = B->d_part.p + part_off[p];
-        P.bar = B->d_bar.p + p;
-        P.res_i = B->d_res_i.p + 8 * (size_t)p;
-        P.res_d = B->d_res_d.p + 2 * (size_t)p;
+        int id = -1;
+        if ((st = add_member(B, mats[p], &id))) return st;
     }
-    FEMD_TRY_CUDA(cudaMemcpyAsync(B->d_slot_prob.p, sp.data(), sp.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    FEMD_TRY_CUDA(cudaMemcpyAsync(B->d_slot_member.p, sm.data(), sm.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    FEMD_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
     *out = reinterpret_cast<femd_batch>(guard.release());
+    return FEMD_OK;
+}
+
+int femd_cuda_batch_add(femd_batch handle, femd_matrix K, int *id_out)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(B && id_out, "batch_add: bad arguments");
+    FEMD_TRY_CUDA(cudaSetDevice(B->ctx->device));
+    return add_member(B, K, id_out);
+}
+
+int femd_cuda_batch_remove(femd_batch handle, int id)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(B && id >= 0 && id < (int)B->mem.size() && B->mem[id], "batch_remove: no such member");
+    B->free_vectors(*B->mem[id]);
+    B->mem[id].reset();
+    return FEMD_OK;
+}
+
+int femd_cuda_batch_arm(femd_batch handle, int id, const double *b_dev, double *x_dev, int max_iter, double tol)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(B, "batch_arm: not a batch handle");
+    return arm_member(B, id, b_dev, x_dev, max_iter, tol);
+}
+
+int femd_cuda_batch_step(femd_ctx ctx, femd_batch handle, int iters, int mixed, int *nfinished, int *finished_ids,
+                         femd_cg_result *finished)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(ctx && B && ctx == B->ctx, "batch_step: bad arguments");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    return batch_step(ctx, B, iters, mixed != 0, nfinished, finished_ids, finished, nullptr);
+}
+
+int femd_cuda_batch_configure(femd_batch handle, int block, int nnz_per_block, int nnz_per_thread)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(B, "batch_configure: not a batch handle");
+    FEMD_CHECK_ARG(block == 128 || block == 256 || block == 512, "batch_configure: block is 128, 256 or 512");
+    FEMD_CHECK_ARG(nnz_per_block >= 256, "batch_configure: nnz_per_block < 256");
+    FEMD_CHECK_ARG(nnz_per_thread == 2 || nnz_per_thread == 4 || nnz_per_thread == 8,
+                   "batch_configure: nnz_per_thread is 2, 4 or 8");
+    FEMD_CHECK_ARG(block * nnz_per_thread <= 2048, "batch_configure: block x nnz_per_thread > 2048 is not built");
+    for (const auto &M : B->mem)
+        FEMD_CHECK_ARG(!M || !M->armed, "batch_configure: a solve is in progress");
+    FEMD_TRY_CUDA(cudaSetDevice(B->ctx->device));
+    const int ob = B->block, on = B->nnz_per_block, ot = B->npt;
+    B->block = block;
+    B->nnz_per_block = nnz_per_block;
+    B->npt = nnz_per_thread;
+    int st = batch_shape(B);
+    if (st) {
+        B->block = ob;
+        B->nnz_per_block = on;
+        B->npt = ot;
+        batch_shape(B);
+    }
+    return st;
+}
+
+int femd_cuda_batch_params(femd_batch handle, int *block, int *nnz_per_block, int *nnz_per_thread, int *graph)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(B, "batch_params: not a batch handle");
+    if (block) *block = B->block;
+    if (nnz_per_block) *nnz_per_block = B->nnz_per_block;
+    if (nnz_per_thread) *nnz_per_thread = B->npt;
+    if (graph) *graph = std::max(B->graph_state[0], B->graph_state[1]);
     return FEMD_OK;
 }
 
@@ -514,72 +1050,84 @@ int femd_cuda_batch_solve(femd_ctx ctx, femd_batch handle, const double *const *
 {
     clear_error();
     femd_batch_s *B = as_batch(handle);
-    FEMD_CHECK_ARG(ctx && B && b_dev && x_dev && results, "batch_solve: NULL argument");
+    FEMD_CHECK_ARG(ctx && B && b_dev && x_dev && results && ctx == B->ctx, "batch_solve: bad arguments");
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
-    cudaStream_t s = ctx->stream;
-    // refresh the FP32 copies (the matrices may have been re-assembled)
-    for (int p = 0; p < B->nprob; ++p) {
-        femd_matrix K = B->mats[p];
-        BProb &P = B->probs[p];
-        FEMD_CHECK_ARG(b_dev[p] && x_dev[p], "batch_solve: NULL vector");
-        P.b = b_dev[p];
-        P.x = x_dev[p];
-        P.tol = tol;
-        P.max_iter = max_iter > 0 ? max_iter : std::max(1000, 10 * P.n);
-        if (mixed) {
-            const long long nnz = K->pattern->nnz;
-            k_batch_f32<<<grid_for((size_t)nnz + 1, 256, 1u << 16), 256, 0, counted(s)>>>(K->data.p, const_cast<float *>(P.A32), nnz);
-            k_batch_f32<<<grid_for((size_t)P.n + 1, 256, 1u << 16), 256, 0, counted(s)>>>(K->inv.p, const_cast<float *>(P.inv32), P.n);
+    std::vector<int> ids;
+    for (int id = 0; id < (int)B->mem.size(); ++id)
+        if (B->mem[id]) ids.push_back(id);
+    int st;
+    for (size_t p = 0; p < ids.size(); ++p)
+        if ((st = arm_member(B, ids[p], b_dev[p], x_dev[p], max_iter, tol))) return st;
+    std::vector<int> fin(ids.size());
+    std::vector<femd_cg_result> fr(ids.size());
+    int nf = 0;
+    double sec = 0.0;
+    st = batch_step(ctx, B, INT_MAX, mixed != 0, &nf, fin.data(), fr.data(), &sec);
+    for (size_t p = 0; p < ids.size(); ++p) {
+        fill_result(B->h_state[ids[p]], results[p], sec);
+        if (B->h_qout->flag) results[p].status = B->h_qout->flag;
+        B->mem[ids[p]]->armed = false;
+    }
+    return st;
+}
+
+int femd_cuda_batch_tune(femd_ctx ctx, femd_batch handle, const double *const *b_dev, double *const *x_dev, int max_iter,
+                         double tol, int mixed, int *best_out, double *seconds_out)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(ctx && B && b_dev && x_dev, "batch_tune: NULL argument");
+    std::vector<int> ids;
+    for (int id = 0; id < (int)B->mem.size(); ++id)
+        if (B->mem[id]) ids.push_back(id);
+    std::vector<femd_cg_result> res(ids.size() + 1);
+    auto run = [&](int blk, int npb, int npt, double *sec) -> int {
+        if (blk * npt > 2048) { *sec = 1e300; return FEMD_OK; }   // not built
+        int st = femd_cuda_batch_configure(handle, blk, npb, npt);
+        if (st) return st;
+        double best = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {
+            for (size_t p = 0; p < ids.size(); ++p)
+                FEMD_TRY_CUDA(cudaMemsetAsync(x_dev[p], 0, (size_t)B->mem[ids[p]]->n * sizeof(double), ctx->stream));
+            st = femd_cuda_batch_solve(ctx, handle, b_dev, x_dev, max_iter, tol, mixed, res.data());
+            if (st) return st;
+            best = std::min(best, res[0].seconds);
+        }
+        *sec = best;
+        return FEMD_OK;
+    };
+    // coordinate descent over nonzeros per rank, threads per block and nonzeros per thread
+    static const int NPB[] = {8192, 16384, 32768, 65536, 131072};
+    static const int BLK[] = {128, 256, 512};
+    static const int NPT[] = {2, 4, 8};
+    int cb = 256, cn = 65536, ct = 4;
+    double tbest = 1e300;
+    int st;
+    if ((st = run(cb, cn, ct, &tbest))) return st;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int v : NPB) {
+            if (v == cn) continue;
+            double t;
+            if ((st = run(cb, v, ct, &t))) return st;
+            if (t < tbest) { tbest = t; cn = v; }
+        }
+        if (pass == 1) break;
+        for (int v : BLK) {
+            if (v == cb) continue;
+            double t;
+            if ((st = run(v, cn, ct, &t))) return st;
+            if (t < tbest) { tbest = t; cb = v; }
+        }
+        for (int v : NPT) {
+            if (v == ct) continue;
+            double t;
+            if ((st = run(cb, cn, v, &t))) return st;
+            if (t < tbest) { tbest = t; ct = v; }
         }
     }
-    FEMD_TRY_CUDA(cudaGetLastError());
-    std::vector<BProb> desc = B->probs;
-    if (B->ghost >= 0 && B->ghost < B->nprob) desc[B->ghost].team += 1;   // test hook (femd_cuda_batch_debug)
-    FEMD_TRY_CUDA(cudaMemcpyAsync(B->d_probs.p, desc.data(), desc.size() * sizeof(BProb), cudaMemcpyHostToDevice, s));
-    FEMD_TRY_CUDA(cudaMemsetAsync(B->d_bar.p, 0, B->nprob * sizeof(unsigned), s));
-    BQueue q0{0u, 0, B->spin_limit};
-    FEMD_TRY_CUDA(cudaMemcpyAsync(B->d_queue.p, &q0, sizeof(BQueue), cudaMemcpyHostToDevice, s));
-    FEMD_TRY_CUDA(cudaMemsetAsync(B->d_res_i.p, 0, 8 * (size_t)B->nprob * sizeof(int), s));
-    *B->abort_host = 0;
-    const BProb *probs = B->d_probs.p;
-    const int *sp = B->d_slot_prob.p, *sm = B->d_slot_member.p;
-    int nslots = B->nslots;
-    BQueue *q = B->d_queue.p;
-    const int *ab = B->abort_dev;
-    void *args[] = {(void *)&probs, (void *)&sp, (void *)&sm, (void *)&nslots, (void *)&q, (void *)&ab};
-    cudaEvent_t e0, e1;
-    FEMD_TRY_CUDA(cudaEventCreate(&e0));
-    FEMD_TRY_CUDA(cudaEventCreate(&e1));
-    cudaEventRecord(e0, s);
-    cudaError_t e = mixed ? cudaLaunchCooperativeKernel((const void *)k_batch_pcg<true>, B->grid, BB, args, 0, s)
-                          : cudaLaunchCooperativeKernel((const void *)k_batch_pcg<false>, B->grid, BB, args, 0, s);
-    if (e == cudaSuccess) add_launches(1);
-    cudaEventRecord(e1, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (e != cudaSuccess) { set_error(std::string("batch_solve: ") + cudaGetErrorString(e)); return FEMD_ECUDA; }
-    std::vector<int> ri(8 * (size_t)B->nprob);
-    std::vector<double> rd(2 * (size_t)B->nprob);
-    BQueue qh;
-    FEMD_TRY_CUDA(cudaMemcpyAsync(ri.data(), B->d_res_i.p, ri.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
-    FEMD_TRY_CUDA(cudaMemcpyAsync(rd.data(), B->d_res_d.p, rd.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-    FEMD_TRY_CUDA(cudaMemcpyAsync(&qh, B->d_queue.p, sizeof(BQueue), cudaMemcpyDeviceToHost, s));
-    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
-    for (int p = 0; p < B->nprob; ++p) {
-        femd_cg_result &r = results[p];
-        r.iterations = ri[8 * p];
-        r.converged = ri[8 * p + 1];
-        r.breakdown = ri[8 * p + 2];
-        r.status = qh.flag ? qh.flag : ri[8 * p + 3];
-        r.outer = ri[8 * p + 4];
-        r.residual = rd[2 * p];
-        r.seconds = ms * 1e-3;
-    }
-    if (qh.flag == FEMD_ETIMEOUT) { set_error("batch_solve: a team barrier wait ran out"); return FEMD_ETIMEOUT; }
-    if (qh.flag == FEMD_EABORT) { set_error("batch_solve: aborted by the host"); return FEMD_EABORT; }
+    if ((st = femd_cuda_batch_configure(handle, cb, cn, ct))) return st;
+    if (best_out) { best_out[0] = cb; best_out[1] = cn; best_out[2] = ct; }
+    if (seconds_out) *seconds_out = tbest;
     return FEMD_OK;
 }
 
@@ -591,13 +1139,13 @@ int femd_cuda_batch_abort(femd_batch handle)
     return FEMD_OK;
 }
 
-int femd_cuda_batch_debug(femd_batch handle, int ghost_problem, long long spin_limit)
+int femd_cuda_batch_debug(femd_batch handle, int ghost_member, long long spin_limit)
 {
     clear_error();
     femd_batch_s *B = as_batch(handle);
     FEMD_CHECK_ARG(B, "batch_debug: not a batch handle");
-    FEMD_CHECK_ARG(ghost_problem < B->nprob, "batch_debug: problem index out of range");
-    B->ghost = ghost_problem;
+    FEMD_CHECK_ARG(ghost_member < (int)B->mem.size(), "batch_debug: member index out of range");
+    B->ghost = ghost_member;
     B->spin_limit = spin_limit > 0 ? spin_limit : SPIN_LIMIT;
     return FEMD_OK;
 }
@@ -607,10 +1155,16 @@ int femd_cuda_batch_info(femd_batch handle, int *nprob, int *grid, int *nslots, 
     clear_error();
     femd_batch_s *B = as_batch(handle);
     FEMD_CHECK_ARG(B, "batch_info: not a batch handle");
-    if (nprob) *nprob = B->nprob;
+    int np = 0, ns = 0;
+    for (const auto &M : B->mem)
+        if (M) {
+            if (team_out) team_out[np] = M->team;
+            ++np;
+            ns += M->team;
+        }
+    if (nprob) *nprob = np;
     if (grid) *grid = B->grid;
-    if (nslots) *nslots = B->nslots;
-    if (team_out) for (int p = 0; p < B->nprob; ++p) team_out[p] = B->team[p];
+    if (nslots) *nslots = ns;
     return FEMD_OK;
 }
 

@@ -248,28 +248,63 @@ FEMD_API int femd_cuda_cg_jacobi_noalloc(femd_ctx ctx, femd_matrix K, int use_ja
  * Batched solves: K7.  Many independent Jacobi-PCG solves in ONE persistent cooperative
  * launch.  No single reference counterpart: it runs the reference's cg_jacobi
  * (include/femd/krylov/cg.hpp:296-350, stopping rule and final true residual included) for
- * every system of the batch at once.  Each problem gets a team of thread blocks sized from its
- * nonzeros (nnz_per_block, 0 = 65536); the members meet at software barriers with bounded
- * waits (FEMD_ETIMEOUT when one runs out; every block then returns).  A problem's result does
- * not depend on the rest of the batch: its reductions are ordered by the problem alone.
- * mixed != 0: FP32 matrix copy, vectors and accumulation, with FP64 reliable updates
- * (r = b - A x on the FP64 matrix, x updated in FP64) until ||b - A x|| <= tol ||b||.
+ * every member system of the batch at once.  Each member gets a team of thread blocks sized
+ * from its nonzeros; the ranks of a team meet at software barriers with bounded waits
+ * (FEMD_ETIMEOUT when one runs out; every block then returns).  A member's result does not
+ * depend on the rest of the batch: its reductions are ordered by the member and the launch
+ * shape alone.  mixed != 0: FP32 matrix copy, vectors and SpMV accumulation, with FP64 reliable
+ * updates (r = b - A x on the FP64 matrix, x updated in FP64) until ||b - A x|| <= tol ||b||.
+ * Solves are resumable: femd_cuda_batch_step advances every armed member by a number of
+ * iterations, so members can join (add + arm) and leave between launches (continuous
+ * batching).  The matrices must outlive their membership.
  * ====================================================================================== */
 typedef struct femd_batch_s *femd_batch;
+/* A batch with members 0..nprob-1 = mats (nprob may be 0); nnz_per_block <= 0: 65536. */
 FEMD_API int femd_cuda_batch_create(femd_ctx ctx, int nprob, const femd_matrix *mats, int nnz_per_block, femd_batch *out);
-/* b_dev[p], x_dev[p]: device vectors of problem p (x: initial guess in, solution out).
- * max_iter <= 0: max(1000, 10 n) per problem.  results[p] per problem; res.seconds = the launch. */
+/* Solve every member to completion in one launch.  b_dev[p], x_dev[p]: device vectors of the
+ * p-th member in id order (x: initial guess in, solution out).  max_iter <= 0: max(1000, 10 n)
+ * per member.  results[p] per member; res.seconds = the launch. */
 FEMD_API int femd_cuda_batch_solve(femd_ctx ctx, femd_batch B, const double *const *b_dev, double *const *x_dev,
                                    int max_iter, double tol, int mixed, femd_cg_result *results);
-/* Ask a running batch solve to stop (safe from another host thread): FEMD_EABORT. */
+/* Add a member (a square matrix with its Jacobi inverse diagonal); *id_out its id (a free id is
+ * reused).  Remove frees its solver vectors; a removed member's solve is dropped. */
+FEMD_API int femd_cuda_batch_add(femd_batch B, femd_matrix K, int *id_out);
+FEMD_API int femd_cuda_batch_remove(femd_batch B, int id);
+/* Start a solve of member id on the next steps: b_dev, x_dev (initial guess in, solution out)
+ * stay in use until the member finishes.  max_iter <= 0: max(1000, 10 n). */
+FEMD_API int femd_cuda_batch_arm(femd_batch B, int id, const double *b_dev, double *x_dev, int max_iter, double tol);
+/* One launch: every armed member advances by at most iters iterations (all in FP32-inner mixed
+ * mode or all in FP64).  Members that finish are disarmed; *nfinished of them are listed in
+ * finished_ids / finished (room for every armed member; either list may be NULL). */
+FEMD_API int femd_cuda_batch_step(femd_ctx ctx, femd_batch B, int iters, int mixed, int *nfinished, int *finished_ids,
+                                  femd_cg_result *finished);
+/* Ask a running batch launch to stop (safe from another host thread): FEMD_EABORT. */
 FEMD_API int femd_cuda_batch_abort(femd_batch B);
-/* Problems, resident blocks, team slots and each problem's team size (team_out: nprob ints). */
+/* Members, resident blocks, team slots and each member's team size in id order (team_out:
+ * one int per member). */
 FEMD_API int femd_cuda_batch_info(femd_batch B, int *nprob, int *grid, int *nslots, int *team_out);
-/* Failure-detection hook for tests: the next solves make problem ghost_problem (-1: none) wait
- * at its barriers for one team member that never comes, and bound every wait by spin_limit
- * spins (<= 0: the default, a few seconds).  The solve then returns FEMD_ETIMEOUT and the
- * context stays usable.  No reference counterpart. */
-FEMD_API int femd_cuda_batch_debug(femd_batch B, int ghost_problem, long long spin_limit);
+/* The launch shape: threads per block (128, 256 or 512), nonzeros per team rank (>= 256: a
+ * member's team is ceil(nnz / nnz_per_block) blocks, at most half the grid and one per 64
+ * rows) and nonzeros per thread of an SpMV chunk (2, 4 or 8; 512 x 8 is not built): a chunk of
+ * whole rows holds at most block x nnz_per_thread nonzeros, i.e. it sets the rows each warp
+ * sums per chunk.  A member's iterates depend on these and on the member alone.  No reference
+ * counterpart.  Not while a solve is in progress. */
+FEMD_API int femd_cuda_batch_configure(femd_batch B, int block, int nnz_per_block, int nnz_per_thread);
+/* The current shape, and graph = 1 when launches run as a captured CUDA graph (-1: direct
+ * launches, 0: no launch yet). */
+FEMD_API int femd_cuda_batch_params(femd_batch B, int *block, int *nnz_per_block, int *nnz_per_thread, int *graph);
+/* Autotuner: coordinate descent over nnz_per_block {8192 .. 131072}, block {128, 256, 512} and
+ * nnz_per_thread {2, 4, 8}, each shape timed (CUDA events, best of two) on these systems with
+ * x_dev zeroed before every run (x_dev is scratch: it holds the last run's iterate), max_iter
+ * iterations (<= 0: to convergence).  Leaves the fastest shape configured; best_out = {block,
+ * nnz_per_block, nnz_per_thread}, *seconds_out its time.  No reference counterpart. */
+FEMD_API int femd_cuda_batch_tune(femd_ctx ctx, femd_batch B, const double *const *b_dev, double *const *x_dev, int max_iter,
+                                  double tol, int mixed, int *best_out, double *seconds_out);
+/* Failure-detection hook for tests: the next launches make member ghost_member (-1: none) wait
+ * at its barriers for one team rank that never comes, and bound every wait by spin_limit spins
+ * (<= 0: the default, a few seconds).  The launch then returns FEMD_ETIMEOUT and the context
+ * stays usable.  No reference counterpart. */
+FEMD_API int femd_cuda_batch_debug(femd_batch B, int ghost_member, long long spin_limit);
 
 /* ======================================================================================
  * Host-side setup of the synthetic problems (the reference's own setup code runs on the

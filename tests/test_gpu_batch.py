@@ -126,3 +126,58 @@ def test_host_abort(fb):
     assert not th.is_alive()
     assert B.last_status == 7                             # FEMD_EABORT
     assert out["res"][0]["status"] == 7
+
+
+def test_launch_shapes_and_autotuner(fb, problems):
+    mats = [K for _, K, _ in problems]
+    bs = [b for _, _, b in problems]
+    B = fb.Batch(mats)
+    for block, npb, npt in ((128, 1024, 2), (512, 4096, 4), (256, 8192, 8)):
+        B.configure(block, npb, npt)
+        xs, res = B.solve(bs, tol=1e-10, mixed=True)
+        assert B.last_status == 0 and B.params()["block"] == block
+        assert B.params()["graph"] in (1, -1)
+        for (s, K, b), x, r in zip(problems, xs, res):
+            assert r["converged"]
+            xd = direct(K, b)
+            assert np.linalg.norm(x.cpu().numpy() - xd) / np.linalg.norm(xd) <= 1e-8
+    p, sec = B.tune(bs, max_iter=20, mixed=True)
+    assert p["block"] in (128, 256, 512) and p["nnz_per_thread"] in (2, 4, 8) and sec > 0
+    assert p["nnz_per_block"] in (8192, 16384, 32768, 65536, 131072)
+    xs, res = B.solve(bs, tol=1e-10, mixed=True)
+    assert all(r["converged"] for r in res)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_resumable_steps_give_the_same_bits(fb, problems, mixed):
+    """Stepping a few iterations per launch, with members joining part-way through, gives the
+    bits of one launch per member."""
+    import torch
+    mats = [K for _, K, _ in problems]
+    bs = [b for _, _, b in problems]
+    xs_ref, res_ref = fb.Batch(mats).solve(bs, tol=1e-10, mixed=mixed)
+    B = fb.Batch()
+    ids, xs = [], []
+    done = {}
+    for p in range(len(mats)):
+        i = B.add(mats[p])
+        ids.append(i)
+        xs.append(torch.zeros(mats[p].nrows, dtype=torch.float64, device="cuda"))
+    for p in range(6):
+        B.arm(ids[p], bs[p], xs[p], tol=1e-10)
+    steps = 0
+    while len(done) < len(mats):
+        for i, r in B.step(7, mixed=mixed):
+            done[i] = r
+        steps += 1
+        if steps == 3:
+            for p in range(6, len(mats)):
+                B.arm(ids[p], bs[p], xs[p], tol=1e-10)
+        assert steps < 100000
+    for p, i in enumerate(ids):
+        assert np.array_equal(xs[p].cpu().numpy(), xs_ref[p].cpu().numpy()), p
+        assert done[i]["iterations"] == res_ref[p]["iterations"]
+        assert done[i]["converged"]
+    B.remove(ids[3])
+    j = B.add(mats[3])
+    assert j == ids[3]
