@@ -9,6 +9,7 @@ launch shape alone: the same bits alone or in any mix.
 from __future__ import annotations
 
 import ctypes as C
+import sys
 
 import numpy as np
 
@@ -43,7 +44,7 @@ class Batch:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and not sys.is_finalizing():
                 lib.femd_cuda_release(self.h)
                 self.h = None
         except Exception:

@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import sys
 import threading
 
 import numpy as np
@@ -85,7 +86,8 @@ class Context:
 
     def __del__(self):
         try:
-            self.close()
+            if not sys.is_finalizing():     # at exit the process frees everything
+                self.close()
         except Exception:
             pass
 
@@ -112,7 +114,7 @@ class _Handle:
 
     def __del__(self):
         try:
-            if self.h:
+            if self.h and not sys.is_finalizing():
                 lib.femd_cuda_release(self.h)
                 self.h = None
         except Exception:

@@ -18,9 +18,10 @@
 // fixed batch; short launches with members joining and leaving between them are the continuous
 // batching of the request loop.
 //
-// SpMV: CSR-stream over precomputed chunks of whole rows (at most BB x NPT nonzeros): the block
-// loads the chunk's column indices and values coalesced, gathers, stores the products in shared
-// memory (two buffers, one barrier per chunk), and one thread per row sums its products in order.
+// SpMV: CSR-stream over precomputed chunks of whole rows (at most BB x NPT nonzeros): bulk
+// asynchronous copies (TMA) bring chunk c+1's column indices and values into shared memory while
+// chunk c is computed; the block gathers, stores the products in shared memory (two buffers, one
+// barrier per chunk), and one thread per row sums its products in order.
 //
 // One iteration is two team reductions.  The search direction is never written before the SpMV
 // that needs it: the SpMV forms p_j = z_j + beta p_j (one fused multiply-add, the same one the
@@ -54,7 +55,7 @@ struct BState {
 };
 
 struct BProb {
-    int n, team, max_iter, nch;
+    int n, team, max_iter, nch, nnz;
     double tol;
     const int *indptr, *indices;
     const int *crow, *cq;  // chunk c = rows [crow[c], crow[c+1]) = nonzeros [cq[c], cq[c+1])
@@ -185,50 +186,165 @@ __device__ bool team_reduce(const BProb &P, int m, int base, double (&v)[NV], un
     return true;
 }
 
-// CSR-stream SpMV over chunks [c0, c1): products a_q * g(col_q) into shared memory (buffer c & 1),
-// then out(row, sum) with the row's products summed in order by one thread.  Vectors that the
-// team writes during the launch take plain coherent loads (inside g).
-template <class V, class F, int BB, int NPT, class Gather, class RowOut>
-__device__ __forceinline__ void chunk_spmv(const BProb &P, const V *A, int c0, int c1, F *prod, Gather g, RowOut out)
+// ---- chunk staging: bulk asynchronous copies (TMA, into this block's own shared memory) ------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *m, unsigned count)
 {
-    constexpr int CAP = BB * NPT;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *m, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *m, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(m)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait for a phase of a staging barrier (a copy that never lands ends the batch)
+__device__ __forceinline__ bool mbar_wait(uint64_t *m, unsigned parity)
+{
+    for (int k = 0; k < (1 << 22); ++k)
+        if (mbar_try_wait(m, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *m)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(m))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// a block's SpMV shared memory: two staging buffers of column indices and values (filled by bulk
+// copies, 16-byte aligned), two product buffers, and the staging barriers
+template <int CAP>
+struct ChunkSmem {
+    static constexpr int IXN = CAP + 4;
+    int ix[2][IXN];
+    double val[2][IXN];        // FP64 values, or FP32 values in the first half
+    double prod[2][CAP];       // FP64 products, or FP32 products in the first half
+    uint64_t mbar[2];
+    int fail;
+};
+
+// the part of chunk c that bulk copies bring in: nonzeros [qa, qb) with qa = qs rounded down to
+// 4 (16 bytes of indices) and qb = qe rounded up but not past nnz rounded down; the rest of the
+// chunk (at most 3 nonzeros at the matrix's end) is read directly
+__device__ __forceinline__ int staged_end(int qa, int qe, int nnz4)
+{
+    int qb = (qe + 3) & ~3;
+    if (qb > nnz4) qb = nnz4;
+    return qb < qa ? qa : qb;
+}
+
+template <class V, int CAP>
+__device__ __forceinline__ void stage_issue(const BProb &P, const V *A, int c, ChunkSmem<CAP> &S)
+{
+    const int s = c & 1;
+    const int qs = P.cq[c], qe = P.cq[c + 1];
+    const int qa = qs & ~3, qb = staged_end(qa, qe, P.nnz & ~3);
+    const unsigned n = (unsigned)(qb - qa);
+    fence_proxy_async_smem();                                 // the buffer's last readers were generic
+    mbar_arrive_tx(&S.mbar[s], n * (unsigned)(sizeof(int) + sizeof(V)));
+    if (n) {
+        bulk_g2s(S.ix[s], P.indices + qa, n * (unsigned)sizeof(int), &S.mbar[s]);
+        bulk_g2s(S.val[s], A + qa, n * (unsigned)sizeof(V), &S.mbar[s]);
+    }
+}
+
+// CSR-stream SpMV over chunks [c0, c1): chunk c+1's indices and values are copied into shared
+// memory while chunk c is computed; products a_q * g(col_q) go to shared memory (buffer c & 1)
+// and out(row, sum) gets each row's products summed in order by one thread.  Vectors that the
+// team writes during the launch take plain coherent loads (inside g).  false: a staging copy did
+// not land (the batch is stopped; the other outstanding copy has been waited for).
+template <class V, class F, int BB, int NPT, class Gather, class RowOut>
+__device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, int c1, ChunkSmem<BB * NPT> &S, unsigned &par,
+                                           BQueue *q, Gather g, RowOut out)
+{
+    if (c0 >= c1) return true;
+    const int nnz4 = P.nnz & ~3;
+    if (threadIdx.x == 0) stage_issue<V>(P, A, c0, S);
     for (int c = c0; c < c1; ++c) {
-        F *buf = prod + (c & 1) * CAP;
+        const int s = c & 1;
+        if (c + 1 < c1 && threadIdx.x == 0) stage_issue<V>(P, A, c + 1, S);
         const int rs = P.crow[c], re = P.crow[c + 1];
         const int qs = P.cq[c], qe = P.cq[c + 1];
+        const int qa = qs & ~3, qb = staged_end(qa, qe, nnz4);
         const int row0 = rs + (int)threadIdx.x;
         int lo0 = 0, hi0 = 0;
         if (row0 < re) { lo0 = P.indptr[row0]; hi0 = P.indptr[row0 + 1]; }
-        int col[NPT];
-        V a[NPT];
+        const bool ok = mbar_wait(&S.mbar[s], (par >> s) & 1u);
+        par ^= 1u << s;
+        if (ok) {
+            const int *ixs = S.ix[s];
+            const V *vs = reinterpret_cast<const V *>(S.val[s]);
+            F *buf = reinterpret_cast<F *>(S.prod[s]);
+            int col[NPT];
+            V a[NPT];
 #pragma unroll
-        for (int t = 0; t < NPT; ++t) {
-            const int qq = qs + t * BB + (int)threadIdx.x;
-            col[t] = qq < qe ? P.indices[qq] : -1;
-            a[t] = qq < qe ? A[qq] : V(0);
+            for (int t = 0; t < NPT; ++t) {
+                const int qq = qs + t * BB + (int)threadIdx.x;
+                col[t] = -1;
+                a[t] = V(0);
+                if (qq < qb) { col[t] = ixs[qq - qa]; a[t] = vs[qq - qa]; }
+                else if (qq < qe) { col[t] = P.indices[qq]; a[t] = A[qq]; }
+            }
+            F gv[NPT];
+#pragma unroll
+            for (int t = 0; t < NPT; ++t) gv[t] = col[t] >= 0 ? g(col[t]) : F(0);
+#pragma unroll
+            for (int t = 0; t < NPT; ++t)
+                if (col[t] >= 0) buf[t * BB + threadIdx.x] = (F)a[t] * gv[t];
+        } else {
+            S.fail = 1;
         }
-#pragma unroll
-        for (int t = 0; t < NPT; ++t)
-            if (col[t] >= 0) buf[t * BB + threadIdx.x] = (F)a[t] * g(col[t]);
         __syncthreads();
+        if (S.fail) {
+            // stop the batch; wait (bounded) for the copy of chunk c + 1 before the block leaves
+            if (threadIdx.x == 0) {
+                atomicCAS(&q->flag, 0, FEMD_ETIMEOUT);
+                if (c + 1 < c1) mbar_wait(&S.mbar[s ^ 1], (par >> (s ^ 1)) & 1u);
+            }
+            return false;
+        }
+        const F *buf = reinterpret_cast<const F *>(S.prod[s]);
         for (int row = row0; row < re; row += BB) {
             int lo = lo0, hi = hi0;
             if (row != row0) { lo = P.indptr[row]; hi = P.indptr[row + 1]; }
-            F s = F(0);
-            for (int qq = lo; qq < hi; ++qq) s += buf[qq - qs];
-            out(row, s);
+            F sum = F(0);
+            for (int qq = lo; qq < hi; ++qq) sum += buf[qq - qs];
+            out(row, sum);
         }
     }
+    return true;
 }
 
 // the FP64 residual r = b - A64 x on chunks [c0, c1): stores r and z = inv r (FP32 copies in
 // mixed mode), adds the shares of ||r||^2 (FP64) and r.z
 template <int BB, int NPT, bool MIXED>
-__device__ __forceinline__ void residual_chunks(const BProb &P, int c0, int c1, double *prod, double &rr, double &rz)
+__device__ __forceinline__ bool residual_chunks(const BProb &P, int c0, int c1, ChunkSmem<BB * NPT> &S, unsigned &par, BQueue *q,
+                                                double &rr, double &rz)
 {
     const double *x = P.x;
-    chunk_spmv<double, double, BB, NPT>(
-        P, P.A64, c0, c1, prod, [&](int j) { return x[j]; },
+    return chunk_spmv<double, double, BB, NPT>(
+        P, P.A64, c0, c1, S, par, q, [&](int j) { return x[j]; },
         [&](int i, double s) {
             const double ri = P.b[i] - s;
             rr += ri * ri;
@@ -280,10 +396,10 @@ __device__ __forceinline__ void update_rows(F *r, F *z, const F *Ap, const F *in
 // rank m of the member's team: advance the solve by at most q->iters iterations; false when the
 // batch has to stop
 template <bool MIXED, int BB, int NPT>
-__device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const int *abort_flag, double *prod64)
+__device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const int *abort_flag, ChunkSmem<BB * NPT> &SM,
+                             unsigned &par)
 {
     using F = typename std::conditional<MIXED, float, double>::type;
-    F *prod = reinterpret_cast<F *>(prod64);
     const int T = P.team;
     const int c0 = (int)((long long)P.nch * m / T), c1 = (int)((long long)P.nch * (m + 1) / T);
     const int r0 = P.crow[c0], r1 = P.crow[c1];
@@ -305,10 +421,11 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
             const int q0 = P.cq[c0], q1 = P.cq[c1];
             for (int qq = q0 + (int)threadIdx.x; qq < q1; qq += BB) P.A32[qq] = (float)P.A64[qq];
             for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) P.inv32[i] = (float)P.inv64[i];
+            fence_proxy_async_global();                   // A32 is read by bulk copies later
             __syncthreads();                              // inv32 is read by the row owners below
         }
         double v[3] = {0.0, 0.0, 0.0};                    // ||r||^2, r.z, ||b||^2
-        residual_chunks<BB, NPT, MIXED>(P, c0, c1, prod64, v[0], v[1]);
+        if (!residual_chunks<BB, NPT, MIXED>(P, c0, c1, SM, par, q, v[0], v[1])) return false;
         for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) {
             const double bi = P.b[i];
             v[2] += bi * bi;
@@ -348,14 +465,15 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
     while (!brk && !done && it < it_end) {
         double pap[1] = {0.0};
         const F fb = (F)beta;
-        chunk_spmv<F, F, BB, NPT>(
-            P, A, c0, c1, prod, [&](int j) { return pdir(z, pold, fb, j); },
+        const bool ok = chunk_spmv<F, F, BB, NPT>(
+            P, A, c0, c1, SM, par, q, [&](int j) { return pdir(z, pold, fb, j); },
             [&](int i, F s) {
                 const F pi = pdir(z, pold, fb, i);
                 pnew[i] = pi;
                 Ap[i] = s;
                 pap[0] += (double)pi * (double)s;
             });
+        if (!ok) return false;
         if (!team_reduce<1, BB>(P, m, 3, pap, phase, q, abort_flag)) return false;
         if (!(pap[0] > 0.0)) { brk = true; break; }
         const double alpha = rz / pap[0];
@@ -380,7 +498,7 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
                 }
                 if (!team_barrier(P, phase, q, abort_flag, true)) return false;
                 double w[2] = {0.0, 0.0};
-                residual_chunks<BB, NPT, true>(P, c0, c1, prod64, w[0], w[1]);
+                if (!residual_chunks<BB, NPT, true>(P, c0, c1, SM, par, q, w[0], w[1])) return false;
                 if (!team_reduce<2, BB>(P, m, 6, w, phase, q, abort_flag)) return false;
                 ++rus;
                 const double rt = sqrt(w[0]);
@@ -404,7 +522,7 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
         if (!MIXED) {
             // the true residual (cg.hpp:222-237): every rank's x is final at the last reduction
             double w[2] = {0.0, 0.0};
-            residual_chunks<BB, NPT, false>(P, c0, c1, prod64, w[0], w[1]);
+            if (!residual_chunks<BB, NPT, false>(P, c0, c1, SM, par, q, w[0], w[1])) return false;
             if (!team_reduce<2, BB>(P, m, 6, w, phase, q, abort_flag)) return false;
             res = sqrt(w[0]) / nb;
         } else if (brk) {
@@ -438,9 +556,17 @@ __global__ void __launch_bounds__(BB, 1024 / BB) k_batch_pcg(const BProb *__rest
                                                              const int *__restrict__ slot_member, BQueue *q,
                                                              volatile const int *abort_flag)
 {
-    __shared__ double prod[2 * BB * NPT];
+    __shared__ __align__(16) ChunkSmem<BB * NPT> SM;
     __shared__ int s_slot, s_stop;
     const int nslots = q->nslots;
+    if (threadIdx.x == 0) {
+        mbar_init(&SM.mbar[0], 1);
+        mbar_init(&SM.mbar[1], 1);
+        SM.fail = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned par = 0;                                     // next phase parity of each staging barrier
     for (;;) {
         if (threadIdx.x == 0) {
             s_slot = (int)atomicAdd(&q->next, 1u);
@@ -451,7 +577,7 @@ __global__ void __launch_bounds__(BB, 1024 / BB) k_batch_pcg(const BProb *__rest
         __syncthreads();
         if (slot >= nslots || stop) return;
         const BProb &P = probs[slot_prob[slot]];
-        if (!solve_member<MIXED, BB, NPT>(P, slot_member[slot], q, abort_flag, prod)) {
+        if (!solve_member<MIXED, BB, NPT>(P, slot_member[slot], q, abort_flag, SM, par)) {
             if (threadIdx.x == 0) {
                 const int f = *(volatile int *)&q->flag;
                 P.st->status = f ? f : FEMD_ETIMEOUT;
@@ -500,8 +626,8 @@ static BatchKernel batch_kernel_m(int block, int npt)
 {
 #define FEMD_BK(B_, N_) if (block == B_ && npt == N_) return k_batch_pcg<MIXED, B_, N_>;
     FEMD_BK(128, 2) FEMD_BK(128, 4) FEMD_BK(128, 8)
-    FEMD_BK(256, 2) FEMD_BK(256, 4) FEMD_BK(256, 8)
-    FEMD_BK(512, 2) FEMD_BK(512, 4)
+    FEMD_BK(256, 2) FEMD_BK(256, 4)
+    FEMD_BK(512, 2)
 #undef FEMD_BK
     return nullptr;
 }
@@ -584,6 +710,8 @@ struct femd_batch_s : femd::HandleBase {
         if (ctx) cudaStreamSynchronize(ctx->stream);
         if (abort_host) cudaFreeHost(abort_host);
         if (pinned) cudaFreeHost(pinned);
+        if (h_slots) cudaFreeHost(h_slots);
+        femd::ctx_release(ctx);
     }
 };
 
@@ -728,6 +856,13 @@ static int member_vectors(femd_batch_s *B, Member &M, bool mixed)
     if (mixed && !M.f32) {
         cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 7 * n + 32) * sizeof(float), s);
         if (e != cudaSuccess) { M.f32 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
+        if (reinterpret_cast<uintptr_t>(M.f32) & 15) {
+            // the FP32 values are read by 16-byte bulk copies
+            cudaFreeAsync(M.f32, s);
+            M.f32 = nullptr;
+            set_error("batch: FP32 arena not 16-byte aligned");
+            return FEMD_ECUDA;
+        }
     }
     if (!mixed && !M.f64) {
         cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f64), (5 * n + 8) * sizeof(double), s);
@@ -744,6 +879,7 @@ static BProb describe(femd_batch_s *B, int id, bool mixed)
     P.team = M.team;
     P.max_iter = M.max_iter;
     P.nch = M.nch;
+    P.nnz = (int)M.nnz;
     P.tol = M.tol;
     P.indptr = M.K->pattern->indptr.p;
     P.indices = M.K->pattern->indices.p;
@@ -953,6 +1089,7 @@ int femd_cuda_batch_create(femd_ctx ctx, int nprob, const femd_matrix *mats, int
     auto B = new femd_batch_s();
     std::unique_ptr<femd_batch_s> guard(B);
     B->ctx = ctx;
+    ctx_retain(ctx);
     B->nnz_per_block = nnz_per_block > 0 ? nnz_per_block : 65536;
     int st;
     if ((st = B->d_queue.alloc(1)) || (st = B->d_scratch.alloc(4))) return st;
@@ -1015,7 +1152,7 @@ int femd_cuda_batch_configure(femd_batch handle, int block, int nnz_per_block, i
     FEMD_CHECK_ARG(nnz_per_block >= 256, "batch_configure: nnz_per_block < 256");
     FEMD_CHECK_ARG(nnz_per_thread == 2 || nnz_per_thread == 4 || nnz_per_thread == 8,
                    "batch_configure: nnz_per_thread is 2, 4 or 8");
-    FEMD_CHECK_ARG(block * nnz_per_thread <= 2048, "batch_configure: block x nnz_per_thread > 2048 is not built");
+    FEMD_CHECK_ARG(block * nnz_per_thread <= 1024, "batch_configure: block x nnz_per_thread > 1024 is not built");
     for (const auto &M : B->mem)
         FEMD_CHECK_ARG(!M || !M->armed, "batch_configure: a solve is in progress");
     FEMD_TRY_CUDA(cudaSetDevice(B->ctx->device));
@@ -1082,7 +1219,7 @@ int femd_cuda_batch_tune(femd_ctx ctx, femd_batch handle, const double *const *b
         if (B->mem[id]) ids.push_back(id);
     std::vector<femd_cg_result> res(ids.size() + 1);
     auto run = [&](int blk, int npb, int npt, double *sec) -> int {
-        if (blk * npt > 2048) { *sec = 1e300; return FEMD_OK; }   // not built
+        if (blk * npt > 1024) { *sec = 1e300; return FEMD_OK; }   // not built
         int st = femd_cuda_batch_configure(handle, blk, npb, npt);
         if (st) return st;
         double best = 1e300;

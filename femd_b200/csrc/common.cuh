@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <stdint.h>
 
 #include <string>
@@ -77,6 +78,9 @@ struct Workspace;
 }  // namespace femd
 
 struct femd_ctx_s {
+    // handles that keep the context (patterns, matrices, batches) hold a reference each;
+    // femd_cuda_ctx_destroy drops the creator's, and the last one frees the stream
+    std::atomic<int> refs{1};
     int device = 0;
     cudaStream_t stream = nullptr;
     int sm_count = 0;
@@ -84,6 +88,11 @@ struct femd_ctx_s {
     int *status_dev = nullptr;
     int *status_host = nullptr;   // pinned
 };
+
+namespace femd {
+void ctx_retain(femd_ctx ctx);
+void ctx_release(femd_ctx ctx);
+}  // namespace femd
 
 struct femd_pattern_s : femd::HandleBase {
     femd_ctx ctx = nullptr;
@@ -106,6 +115,7 @@ struct femd_pattern_s : femd::HandleBase {
     // its size (built on the first FAST assembly when every row is shorter than 255)
     femd::DevBuf<unsigned char> pair_off;
     femd_pattern_s() : HandleBase(femd::KIND_PATTERN) {}
+    ~femd_pattern_s() override { femd::ctx_release(ctx); }
 };
 
 struct femd_matrix_s : femd::HandleBase {
@@ -120,7 +130,11 @@ struct femd_matrix_s : femd::HandleBase {
     void *solver_ws = nullptr;
     void (*solver_ws_free)(void *) = nullptr;
     femd_matrix_s() : HandleBase(femd::KIND_MATRIX) {}
-    ~femd_matrix_s() override { if (solver_ws_free) solver_ws_free(solver_ws); }
+    ~femd_matrix_s() override
+    {
+        if (solver_ws_free) solver_ws_free(solver_ws);
+        femd::ctx_release(ctx);
+    }
 };
 
 namespace femd {

@@ -125,6 +125,24 @@ int reset_status(femd_ctx ctx)
 
 using namespace femd;
 
+namespace femd {
+void ctx_retain(femd_ctx ctx)
+{
+    if (ctx) ctx->refs.fetch_add(1);
+}
+
+void ctx_release(femd_ctx ctx)
+{
+    if (!ctx || ctx->refs.fetch_sub(1) != 1) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->status_dev);
+    cudaFreeHost(ctx->status_host);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+}  // namespace femd
+
 extern "C" {
 
 const char *femd_cuda_last_error(void) { return g_last_error.c_str(); }
@@ -168,13 +186,7 @@ int femd_cuda_ctx_create(int device, femd_ctx *out)
 
 int femd_cuda_ctx_destroy(femd_ctx ctx)
 {
-    if (!ctx) return FEMD_OK;
-    cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(ctx->status_dev);
-    cudaFreeHost(ctx->status_host);
-    cudaStreamDestroy(ctx->stream);
-    delete ctx;
+    femd::ctx_release(ctx);
     return FEMD_OK;
 }
 

@@ -836,6 +836,7 @@ int femd_cuda_matrix_create(femd_ctx ctx, femd_pattern p, femd_matrix *out)
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
     femd_matrix K = new femd_matrix_s();
     K->ctx = ctx;
+    ctx_retain(ctx);
     K->pattern = p;
     int st = K->data.alloc((size_t)p->nnz + 1);
     if (st == FEMD_OK) st = K->inv.alloc((size_t)p->nrows + 1);

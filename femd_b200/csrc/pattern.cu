@@ -213,6 +213,7 @@ int femd_cuda_pattern_from_cells(femd_ctx ctx, int nrows, int ncells, int nloc, 
     cudaStream_t s = ctx->stream;
     femd_pattern p = new femd_pattern_s();
     p->ctx = ctx;
+    ctx_retain(ctx);
     p->nrows = p->ncols = nrows;
     p->ncells = ncells;
     p->nloc = nloc;
@@ -307,6 +308,7 @@ int femd_cuda_pattern_from_csr_host(femd_ctx ctx, int nrows, int ncols, const in
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
     femd_pattern p = new femd_pattern_s();
     p->ctx = ctx;
+    ctx_retain(ctx);
     p->nrows = nrows;
     p->ncols = ncols;
     p->nnz = nnz;

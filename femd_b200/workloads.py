@@ -53,3 +53,22 @@ def build_poisson(spec, cache: SpaceCache):
     fb.assemble_matrix_2d(Q, Q, [1, 2], [1, 2], [spec["c"], spec["c"]], K)
     b = np.random.default_rng(spec["seed"]).standard_normal(s["V"].dim)
     return K, torch.as_tensor(b).cuda()
+
+
+def l2_error(V, coeffs, exact, degree=None):
+    """sqrt(integral over the mesh of (u_h - exact)^2), u_h = sum_i coeffs_i N_i on the space V
+    (constrained nodes 0), by the quadrature rule of the given degree (default 2k + 2) on every
+    triangle -- the value of form((w - exact)**2 * dx).assemble() in the reference's examples.
+    Host numpy; exact(x, y) takes and returns arrays."""
+    coeffs = np.asarray(coeffs.cpu().numpy() if hasattr(coeffs, "cpu") else coeffs, dtype=np.float64)
+    Q = V.cache(degree or 2 * V.degree + 2)
+    pts, tris = V.mesh.points, V.mesh.tris
+    p0, p1, p2 = pts[tris[:, 0]], pts[tris[:, 1]], pts[tris[:, 2]]
+    e1, e2 = p1 - p0, p2 - p0
+    det = np.abs(e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0])
+    xq = p0[:, None, :] + Q.xi[None, :, None] * e1[:, None, :] + Q.eta[None, :, None] * e2[:, None, :]
+    cd = V.cell_dofs
+    cv = np.where(cd >= 0, coeffs[np.maximum(cd, 0)], 0.0)
+    uh = cv @ Q.ref[:, 0, :].T
+    err = uh - exact(xq[..., 0], xq[..., 1])
+    return float(np.sqrt(np.sum(det[:, None] * Q.w[None, :] * err * err)))

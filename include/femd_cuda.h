@@ -285,7 +285,7 @@ FEMD_API int femd_cuda_batch_abort(femd_batch B);
 FEMD_API int femd_cuda_batch_info(femd_batch B, int *nprob, int *grid, int *nslots, int *team_out);
 /* The launch shape: threads per block (128, 256 or 512), nonzeros per team rank (>= 256: a
  * member's team is ceil(nnz / nnz_per_block) blocks, at most half the grid and one per 64
- * rows) and nonzeros per thread of an SpMV chunk (2, 4 or 8; 512 x 8 is not built): a chunk of
+ * rows) and nonzeros per thread of an SpMV chunk (2, 4 or 8, with block x nnz_per_thread <= 1024): a chunk of
  * whole rows holds at most block x nnz_per_thread nonzeros, i.e. it sets the rows each warp
  * sums per chunk.  A member's iterates depend on these and on the member alone.  No reference
  * counterpart.  Not while a solve is in progress. */

@@ -132,7 +132,7 @@ def test_launch_shapes_and_autotuner(fb, problems):
     mats = [K for _, K, _ in problems]
     bs = [b for _, _, b in problems]
     B = fb.Batch(mats)
-    for block, npb, npt in ((128, 1024, 2), (512, 4096, 4), (256, 8192, 8)):
+    for block, npb, npt in ((128, 1024, 2), (512, 4096, 2), (256, 8192, 4), (128, 2048, 8)):
         B.configure(block, npb, npt)
         xs, res = B.solve(bs, tol=1e-10, mixed=True)
         assert B.last_status == 0 and B.params()["block"] == block
