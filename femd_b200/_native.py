@@ -82,6 +82,7 @@ SIGNATURES = {
     "femd_cuda_batch_abort": (_I, [_P]),
     "femd_cuda_batch_info": (_I, [_P, _PI, _PI, _PI, _PI]),
     "femd_cuda_batch_debug": (_I, [_P, _I, C.c_longlong]),
+    "femd_cuda_batch_profile": (_I, [_P, C.POINTER(C.c_longlong)]),
     "femd_cuda_batch_configure": (_I, [_P, _I, _I, _I]),
     "femd_cuda_batch_params": (_I, [_P, _PI, _PI, _PI, _PI]),
     "femd_cuda_batch_tune": (_I, [_P, _P, _P, _P, _I, _D, _I, _PI, C.POINTER(C.c_double)]),

@@ -158,5 +158,12 @@ class Batch:
     def abort(self):
         lib.femd_cuda_batch_abort(self.h)
 
+    def profile(self):
+        """Cycle counters of the last launch summed over blocks: kernel, team-barrier waits,
+        SpMV chunk-barrier waits (femd_cuda_batch_profile)."""
+        out = (C.c_longlong * 3)()
+        check(lib.femd_cuda_batch_profile(self.h, out))
+        return dict(block=out[0], team_wait=out[1], chunk_sync=out[2])
+
     def debug(self, ghost_problem=-1, spin_limit=0):
         check(lib.femd_cuda_batch_debug(self.h, int(ghost_problem), int(spin_limit)))

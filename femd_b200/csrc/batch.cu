@@ -76,6 +76,9 @@ struct BQueue {
     long long spin_limit;  // the bound of every barrier wait (spins)
     int nslots;
     int iters;             // iterations per member in this launch
+    // cycle counters of the launch (thread 0 of every block): in the kernel, waiting at team
+    // barriers, and waiting at the SpMV chunk barriers
+    unsigned long long block_cycles, team_wait_cycles, chunk_sync_cycles;
 };
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
@@ -108,6 +111,7 @@ __device__ bool team_barrier(const BProb &P, unsigned &phase, BQueue *q, volatil
             const unsigned target = (phase + 1) * (unsigned)P.team;
             const long long lim = q->spin_limit;
             long long spins = 0;
+            const long long t0 = clock64();
             while (ld_acquire(P.bar) < target) {
                 if (((++spins) & 255) == 0) {
                     if (*(volatile int *)&q->flag) { ok = 0; break; }
@@ -115,6 +119,7 @@ __device__ bool team_barrier(const BProb &P, unsigned &phase, BQueue *q, volatil
                 }
                 __nanosleep(32);
             }
+            atomicAdd(&q->team_wait_cycles, (unsigned long long)(clock64() - t0));
             __threadfence();
         }
         if (check) {
@@ -274,9 +279,9 @@ __device__ __forceinline__ void stage_issue(const BProb &P, const V *A, int c, C
 // and out(row, sum) gets each row's products summed in order by one thread.  Vectors that the
 // team writes during the launch take plain coherent loads (inside g).  false: a staging copy did
 // not land (the batch is stopped; the other outstanding copy has been waited for).
-template <class V, class F, int BB, int NPT, class Gather, class RowOut>
+template <class V, class F, int BB, int NPT, class Gather, class Pre, class RowOut>
 __device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, int c1, ChunkSmem<BB * NPT> &S, unsigned &par,
-                                           BQueue *q, Gather g, RowOut out)
+                                           BQueue *q, Gather g, Pre pre, RowOut out)
 {
     if (c0 >= c1) return true;
     const int nnz4 = P.nnz & ~3;
@@ -289,7 +294,12 @@ __device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, i
         const int qa = qs & ~3, qb = staged_end(qa, qe, nnz4);
         const int row0 = rs + (int)threadIdx.x;
         int lo0 = 0, hi0 = 0;
-        if (row0 < re) { lo0 = P.indptr[row0]; hi0 = P.indptr[row0 + 1]; }
+        decltype(pre(0)) pv{};
+        if (row0 < re) {
+            lo0 = P.indptr[row0];
+            hi0 = P.indptr[row0 + 1];
+            pv = pre(row0);                                   // the row's own values, loaded early
+        }
         const bool ok = mbar_wait(&S.mbar[s], (par >> s) & 1u);
         par ^= 1u << s;
         if (ok) {
@@ -315,7 +325,9 @@ __device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, i
         } else {
             S.fail = 1;
         }
+        const long long ts = clock64();
         __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(&q->chunk_sync_cycles, (unsigned long long)(clock64() - ts));
         if (S.fail) {
             // stop the batch; wait (bounded) for the copy of chunk c + 1 before the block leaves
             if (threadIdx.x == 0) {
@@ -327,10 +339,14 @@ __device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, i
         const F *buf = reinterpret_cast<const F *>(S.prod[s]);
         for (int row = row0; row < re; row += BB) {
             int lo = lo0, hi = hi0;
-            if (row != row0) { lo = P.indptr[row]; hi = P.indptr[row + 1]; }
+            if (row != row0) {
+                lo = P.indptr[row];
+                hi = P.indptr[row + 1];
+                pv = pre(row);
+            }
             F sum = F(0);
             for (int qq = lo; qq < hi; ++qq) sum += buf[qq - qs];
-            out(row, sum);
+            out(row, sum, pv);
         }
     }
     return true;
@@ -344,9 +360,9 @@ __device__ __forceinline__ bool residual_chunks(const BProb &P, int c0, int c1, 
 {
     const double *x = P.x;
     return chunk_spmv<double, double, BB, NPT>(
-        P, P.A64, c0, c1, S, par, q, [&](int j) { return x[j]; },
-        [&](int i, double s) {
-            const double ri = P.b[i] - s;
+        P, P.A64, c0, c1, S, par, q, [&](int j) { return x[j]; }, [&](int i) { return P.b[i]; },
+        [&](int i, double s, double bi) {
+            const double ri = bi - s;
             rr += ri * ri;
             if (MIXED) {
                 const float rf = (float)ri, zf = P.inv32[i] * rf;
@@ -467,8 +483,8 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
         const F fb = (F)beta;
         const bool ok = chunk_spmv<F, F, BB, NPT>(
             P, A, c0, c1, SM, par, q, [&](int j) { return pdir(z, pold, fb, j); },
-            [&](int i, F s) {
-                const F pi = pdir(z, pold, fb, i);
+            [&](int i) { return pdir(z, pold, fb, i); },
+            [&](int i, F s, F pi) {
                 pnew[i] = pi;
                 Ap[i] = s;
                 pap[0] += (double)pi * (double)s;
@@ -566,6 +582,7 @@ __global__ void __launch_bounds__(BB, 1024 / BB) k_batch_pcg(const BProb *__rest
         fence_mbar_init();
     }
     __syncthreads();
+    const long long t_start = clock64();
     unsigned par = 0;                                     // next phase parity of each staging barrier
     for (;;) {
         if (threadIdx.x == 0) {
@@ -575,7 +592,10 @@ __global__ void __launch_bounds__(BB, 1024 / BB) k_batch_pcg(const BProb *__rest
         __syncthreads();
         const int slot = s_slot, stop = s_stop;
         __syncthreads();
-        if (slot >= nslots || stop) return;
+        if (slot >= nslots || stop) {
+            if (threadIdx.x == 0) atomicAdd(&q->block_cycles, (unsigned long long)(clock64() - t_start));
+            return;
+        }
         const BProb &P = probs[slot_prob[slot]];
         if (!solve_member<MIXED, BB, NPT>(P, slot_member[slot], q, abort_flag, SM, par)) {
             if (threadIdx.x == 0) {
@@ -1003,7 +1023,7 @@ static int batch_step(femd_ctx ctx, femd_batch_s *B, int iters, bool mx, int *nf
         }
         B->drop_graphs();
     }
-    *B->h_q0 = BQueue{0u, 0, B->spin_limit, (int)ns, std::max(1, iters)};
+    *B->h_q0 = BQueue{0u, 0, B->spin_limit, (int)ns, std::max(1, iters), 0ull, 0ull, 0ull};
     *(volatile int *)B->abort_host = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     FEMD_TRY_CUDA(cudaEventCreate(&e0));
@@ -1273,6 +1293,17 @@ int femd_cuda_batch_abort(femd_batch handle)
     femd_batch_s *B = as_batch(handle);
     if (!B || !B->abort_host) return FEMD_EINVAL;
     *(volatile int *)B->abort_host = 1;
+    return FEMD_OK;
+}
+
+int femd_cuda_batch_profile(femd_batch handle, long long *cycles_out)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(B && cycles_out && B->h_qout, "batch_profile: bad arguments");
+    cycles_out[0] = (long long)B->h_qout->block_cycles;
+    cycles_out[1] = (long long)B->h_qout->team_wait_cycles;
+    cycles_out[2] = (long long)B->h_qout->chunk_sync_cycles;
     return FEMD_OK;
 }
 
