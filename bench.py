@@ -1,24 +1,33 @@
 """Benchmark of the FEMd 2D P_k assembly + Jacobi-PCG path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-cpu]
+                    [--workload c4s|c2]
 
-Workload (the plain method at scale on one GPU): -Lap u + u = f on rectangle_mesh 1024 x 1024
-(2,097,152 triangles), P2 Lagrange (4,190,209 unknowns, 48,136,245 nonzeros), zero Dirichlet,
-f = 2 pi^2 sin(pi x) sin(pi y) + sin(pi x) sin(pi y); FP64 assembly of A and b into CSR on the
-cached pattern, then FP64 Jacobi-PCG to relative residual 1e-10.  One step = one solve
-(assemble A and b, Jacobi, CG).  The metric is solves/s.  Inputs (the CSR matrix, 0.58 GB) are
-larger than L2 (126 MB), so no L2 flush is needed between steps.
+Default workload (c4s), the metric's "served + mixed vs plain GPU": the stream of 256 independent
+Poisson problems -c Lap u = f on rectangle_mesh(0,0,1,1,N,N), N uniform in {16..256}, P_k with k
+uniform in {1,2,3}, c log-uniform in [0.1, 10], load-vector dof values N(0,1), all from seed 0
+(30.5M unknowns, 448M nonzeros in all), served by femd_b200.serve.Server: every problem is a
+request (all arriving at once), assembled in FP64 on its cached pattern and solved by the
+batched persistent Jacobi-PCG -- FP32 inner iteration on an FP32 matrix copy with FP64 reliable
+updates -- to relative residual 1e-10.  One step = serving the whole stream.  The metric is
+solves/s; p50 / p99 request latency, the plain FP64 GPU path on the same stream (one assembly +
+cg_solve per request, first come first served) and the largest relative difference between the
+served and the plain FP64 solutions are reported beside it.  The working set (4+ GB) is larger
+than L2, so no flush is needed between steps.
 
-value      device-resident: mesh, pattern and scatter map already in HBM
-e2e        through the public API from host buffers: each step copies the mesh coordinates
-           from pinned host memory to the device, assembles, solves and copies x back
-roofline   the dominant kernel, the CSR SpMV of the CG loop (k_spmv), timed with CUDA events
-           on the library's stream: algorithmic bytes 12 nnz + 4 (n+1) + 8 n + 8 n per launch
+value      device-resident: meshes, spaces and patterns built, load vectors in HBM
+e2e        through the public API from host buffers: each step copies every load vector from
+           pinned host memory to the device and every solution back to pinned host memory
+roofline   the dominant kernel, the batched PCG launch (k_batch_pcg), timed with CUDA events on
+           the library's stream; algorithmic bytes from each member's iterations and reliable
+           updates (batch_bytes below)
 cpu_baseline / --impl reference: the reference's own C++ (oracle/_ref/femd_ref_omp, OpenMP,
-           every host thread) on the same problem: assembly + Jacobi-PCG, a bounded sample of
-           CG iterations per step extrapolated to the full iteration count
-Multi-GPU (torchrun): replicas only -- every rank solves its own copy, no collective on the
-data path; value = all ranks' solves / the slowest rank's time.
+           every host thread) on a stratified sample of 8 of the 256 problems (the midpoints of
+           8 strata of equal count by size): assembly + Jacobi-PCG; solves/s on the sample
+Workload c2 (the plain method at scale): -Lap u + u = f on rectangle_mesh 1024x1024, P2,
+           FP64 assembly + FP64 Jacobi-PCG to 1e-10, one solve per step.
+Multi-GPU (torchrun): replicas only -- every rank serves its own copy of the stream, no
+collective on the data path; value = all ranks' solves / the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -34,7 +43,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "solves/s (FP64 assembly + Jacobi-PCG to 1e-10), rectangle 1024x1024 P2"
+METRIC_C4 = ("solves/s of the served config-4 stream (256 Poisson problems, FP64 assembly + FP32-inner/FP64-refined "
+             "batched Jacobi-PCG to 1e-10), with p99 latency and the plain FP64 GPU path beside it")
 UNIT = "solves/s"
+NPROB, SEED, NSAMPLE, CG_SAMPLE = 256, 0, 8, 40
 N_MESH, DEGREE, TOL = 1024, 2, 1e-10
 PI = 3.141592653589793
 
@@ -192,7 +204,7 @@ def event_time(torch, stream, fn, reps):
     return e0.elapsed_time(e1) / 1e3, out
 
 
-def ours(args, rank, world, dist):
+def ours_c2(args, rank, world, dist):
     import torch
     import femd_b200 as fb
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -321,7 +333,7 @@ def cpu_baseline(gpu_its):
 
 
 # ---- reference arm ---------------------------------------------------------------------------
-def reference(args, rank, world):
+def reference_c2(args, rank, world):
     if rank != 0:
         return None
     sample = 40
@@ -349,20 +361,272 @@ def reference(args, rank, world):
             "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+
+# ---- the served config-4 stream ----------------------------------------------------------------
+def c4_spec():
+    from femd_b200 import workloads as W
+    return W.poisson_batch_spec(seed=SEED, nprob=NPROB)
+
+
+def c4_sample(spec, m=NSAMPLE):
+    """A stratified sample: the problems sorted by size (n x iterations ~ (kN)^3), cut into m
+    strata of equal count, the middle problem of each."""
+    work = [(s["k"] * s["N"]) ** 3 for s in spec]
+    order = sorted(range(len(spec)), key=lambda i: (work[i], i))
+    return [order[(2 * j + 1) * len(order) // (2 * m)] for j in range(m)]
+
+
+def c4_rhs(spec):
+    """The load vectors (float64 numpy), from each problem's seed."""
+    import numpy as np
+    from femd_b200 import serve
+    out = []
+    for s in spec:
+        n = serve.SpaceLibrary.dim(s["N"], s["k"])
+        out.append(np.random.default_rng(s["seed"]).standard_normal(n))
+    return out
+
+
+def batch_bytes(reqs, lib, mixed=True):
+    """Algorithmic HBM bytes of one batched launch: per member and iteration the SpMV's matrix
+    (8 B / nonzero in FP32: value + column index; 12 in FP64) and vectors (gathers of z and the
+    previous direction, stores of the direction and A p; the update's loads of r, A p, inv, x or
+    d, p and stores of r, z, x or d: 12 accesses of 4 or 8 B per row), plus per reliable update and
+    at the start an FP64 residual (12 B / nonzero, b, x, inv, r, z: 40 B / row) and, in mixed mode,
+    the FP32 copy of the matrix (12 B / nonzero)."""
+    tot = 0
+    for r in reqs:
+        sp = lib.get(r.N, r.k)
+        n, nnz = sp["n"], sp["nnz"]
+        if mixed:
+            tot += r.iterations * (8 * nnz + 48 * n) + (r.outer + 1) * (12 * nnz + 40 * n) + 12 * nnz
+        else:
+            tot += r.iterations * (12 * nnz + 96 * n) + 2 * (12 * nnz + 40 * n)
+    return tot
+
+
+def ours_c4(args, rank, world, dist):
+    import numpy as np
+    import torch
+    import femd_b200 as fb
+    from femd_b200 import serve
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    hbm, peak_kind = peaks()
+    t_setup = time.time()
+    spec = c4_spec()
+    lib = serve.SpaceLibrary()
+    for sp in spec:
+        lib.get(sp["N"], sp["k"])
+    rhs = c4_rhs(spec)
+    b_dev = [torch.as_tensor(b).cuda() for b in rhs]
+    b_host = [torch.as_tensor(b).pin_memory() for b in rhs]
+    x_host = [torch.empty(b.size, dtype=torch.float64).pin_memory() for b in rhs]
+    srv = serve.Server(lib, [], mixed=True, iters=1 << 30, keep_solutions=False)
+    setup_s = time.time() - t_setup
+    ctx = fb.context()
+    s = ctx.stream
+
+    def reqs(host=False, keep=False):
+        return [serve.Request(i, 0.0, "poisson", N=sp["N"], k=sp["k"], c=sp["c"], seed=sp["seed"],
+                              b=(b_host[i] if host else b_dev[i]), out=(x_host[i] if host else None))
+                for i, sp in enumerate(spec)]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        srv.run(reqs(), realtime=False)
+    # ---- device-resident timed region
+    barrier()
+    clk = Clocks(local)
+    l0 = fb.lib.femd_cuda_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    stats, launch_s, last = [], [], None
+    for _ in range(args.steps):
+        last = reqs()
+        stats.append(srv.run(last, realtime=False))
+        launch_s.append(srv.last_launch_s)
+    e1.record(s)
+    e1.synchronize()
+    barrier()
+    clocks = clk.stop()
+    launches = (fb.lib.femd_cuda_kernel_launches() - l0) // args.steps
+    t = e0.elapsed_time(e1) / 1e3
+    t_all = _max_over_ranks(torch, dist, t)
+    value = world * args.steps * NPROB / t_all
+    st = stats[-1]
+    # ---- end to end: load vectors from pinned host memory, solutions back to pinned host memory
+    srv.run(reqs(host=True), realtime=False)
+    barrier()
+    e0.record(s)
+    for _ in range(args.steps):
+        srv.run(reqs(host=True), realtime=False)
+    e1.record(s)
+    e1.synchronize()
+    te = _max_over_ranks(torch, dist, e0.elapsed_time(e1) / 1e3)
+    e2e_value = world * args.steps * NPROB / te
+    # ---- the plain FP64 GPU path on the same stream (one pass), and the served-vs-plain error
+    served = reqs()
+    srv_keep = serve.Server(lib, [], mixed=True, iters=1 << 30, keep_solutions=True)
+    srv_keep.run(served, realtime=False)
+    xs_served = {r.rid: r.x for r in served}
+    plain = reqs()
+    pst = serve.run_plain(lib, [], plain, tol=1e-10, realtime=False, keep_solutions=True)
+    err = 0.0
+    for r in plain:
+        a = xs_served[r.rid]
+        err = max(err, float(torch.linalg.norm(a - r.x) / torch.linalg.norm(r.x)))
+        r.x = None
+    xs_served.clear()
+    # ---- roofline of the batched launch of the last timed step
+    alg = batch_bytes(last, lib, mixed=True)
+    t_launch = launch_s[-1]
+    achieved = alg / t_launch / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "k_batch_pcg_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = int(json.load(open(tp))["dram_over_algorithmic"] * alg)
+        except Exception:
+            traffic = None
+    nnz = sum(lib.get(sp["N"], sp["k"])["nnz"] for sp in spec)
+    n = sum(lib.get(sp["N"], sp["k"])["n"] for sp in spec)
+    line = {
+        "metric": METRIC_C4, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_all / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (FP32 inner PCG, FP64 assembly/residual/update)",
+        "data": "synthetic (seeded: meshes, coefficients, N(0,1) load vectors)",
+        "config": {"workload": "config-4 stream: 256 Poisson problems, rectangle N x N (N in 16..256), P1-P3, "
+                               "c log-uniform [0.1,10], served (all arrive at t=0; continuous batching, one "
+                               "persistent launch), FP32-inner / FP64-refined Jacobi-PCG to 1e-10",
+                   "problems": NPROB, "n_total": n, "nnz_total": nnz, "arrivals": "burst at t=0",
+                   "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
+                   "mean_iterations": round(st["mean_iterations"], 1), "all_converged": st["all_converged"],
+                   "max_rel_diff_vs_plain_fp64": err,
+                   "plain_fp64_gpu": {"solves_per_s": round(pst["solves_per_s"], 3), "p50_ms": round(pst["p50_ms"], 2),
+                                      "p99_ms": round(pst["p99_ms"], 2), "mean_iterations": round(pst["mean_iterations"], 1),
+                                      "path": "per request: FP64 assembly + cg_solve (CUDA-graph CG), FIFO"},
+                   "batch_shape": srv.batch.params(), "l2": "working set > 4 GB, larger than L2; no flush",
+                   "parallelism": f"replicas x{world}", "setup_s": round(setup_s, 2)},
+        "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(sum(b.nbytes for b in rhs)),
+                "d2h_bytes_per_step": int(sum(b.nbytes for b in rhs))},
+        "roofline": {"kernel": "k_batch_pcg (batched persistent Jacobi-PCG, mixed)", "bound": "hbm",
+                     "achieved": round(achieved, 1), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": traffic, "algorithmic_bytes": alg,
+                     "launch_ms": round(t_launch * 1e3, 3)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        its = {r.rid: r.iterations for r in plain}
+        line["cpu_baseline"] = cpu_baseline_c4(spec, rhs, its)
+    return line
+
+
+def run_reference_c4(spec, rhs, idx, reps, sample, full_first):
+    """The reference's C++ on the sampled problems (poisson_vec: c grad.grad, the load vector read
+    from a file); per problem a list of (t_asm, t_cg, its) per rep."""
+    import numpy as np
+    exe = _ref_binary()
+    if exe is None:
+        return None, {"error": "oracle/_ref is not built (make -C oracle ref where the reference tree is)"}
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = str(os.cpu_count())
+    out, meta = {}, {}
+    with tempfile.TemporaryDirectory() as d:
+        for i in idx:
+            sp = spec[i]
+            bp = os.path.join(d, f"b{i}.bin")
+            np.asarray(rhs[i], dtype=np.float64).tofile(bp)
+            a = [exe, "poisson_vec", str(sp["N"]), str(sp["k"]), "-", "--c", repr(sp["c"]), "--b", bp, "--nodump",
+                 "--nocg", "--time", str(reps), "--cg-sample", str(sample)]
+            if full_first:
+                a.append("--full-first")
+            txt = subprocess.run(a, capture_output=True, text=True, env=env, check=True).stdout
+            steps = []
+            for line in txt.splitlines():
+                p = line.split()
+                if p and p[0] == "step":
+                    steps.append((float(p[1]), float(p[2]), int(p[3])))
+                elif len(p) == 2:
+                    meta[p[0]] = p[1]
+            out[i] = steps
+    meta["exe"] = os.path.basename(exe)
+    return out, meta
+
+
+def cpu_baseline_c4(spec, rhs, gpu_its):
+    idx = c4_sample(spec)
+    steps, meta = run_reference_c4(spec, rhs, idx, 2, CG_SAMPLE, False)
+    if steps is None:
+        return {"value": None, "unit": UNIT, "error": meta.get("error")}
+    t = 0.0
+    for i in idx:
+        t_asm = min(a for a, _, _ in steps[i])
+        t_it = min(c / k for _, c, k in steps[i])
+        t += t_asm + t_it * gpu_its[i]
+    return {"value": round(len(idx) / t, 5), "unit": UNIT, "cores": int(meta.get("threads", 1)), "kind": "reference",
+            "sample": f"reference C++ ({meta['exe']}, {cpu_model()}) on {len(idx)} of the 256 problems (stratified by "
+                      f"size: {[(spec[i]['N'], spec[i]['k']) for i in idx]}): best of 2 steps of assembly + {CG_SAMPLE} "
+                      f"Jacobi-PCG iterations, extrapolated to each problem's FP64 iteration count on the GPU; "
+                      f"solves/s = {len(idx)} / the summed solve times"}
+
+
+def reference_c4(args, rank, world):
+    if rank != 0:
+        return None
+    spec = c4_spec()
+    rhs = c4_rhs(spec)
+    idx = c4_sample(spec)
+    steps, meta = run_reference_c4(spec, rhs, idx, args.warmup + args.steps, CG_SAMPLE, True)
+    if steps is None:
+        return {"impl": "reference", "unavailable": meta.get("error")}
+    per = []
+    for rep in range(args.warmup, args.warmup + args.steps):
+        t = 0.0
+        for i in idx:
+            its_full = steps[i][0][2]
+            sa, sc, si = steps[i][rep]
+            t += sa + (sc / si) * its_full
+        per.append(t)
+    t = sum(per)
+    value = len(per) * len(idx) / t
+    cores = int(meta.get("threads", 1))
+    sample_txt = (f"reference C++ ({meta['exe']}, OpenMP, {cores} threads, {cpu_model()}) on {len(idx)} of the 256 "
+                  f"problems (stratified by size: {[(spec[i]['N'], spec[i]['k']) for i in idx]}): per step and problem "
+                  f"assembly + {CG_SAMPLE} Jacobi-PCG iterations extrapolated to the count of its own full solve (first "
+                  f"warm-up step); solves/s = problems / summed solve times")
+    return {"impl": "reference", "metric": METRIC_C4, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
+            "steps": len(per), "warmup": args.warmup, "ms_per_step": round(t / len(per) * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded: meshes, coefficients, N(0,1) load vectors)",
+            "config": {"workload": "config-4 stream: 256 Poisson problems (stratified sample of 8 on the host), FP64 "
+                                   "assembly + Jacobi-PCG to 1e-10", "parallelism": "OpenMP (host)"},
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": sample_txt},
+            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="c4s", choices=["c4s", "c2"],
+                    help="c4s: the served config-4 stream (default); c2: one P2 solve on 1024x1024")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
-        line = reference(args, rank, world)
+        line = (reference_c4 if args.workload == "c4s" else reference_c2)(args, rank, world)
         if line is not None:
             print(json.dumps(line), flush=True)
         return
@@ -375,7 +639,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         D.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = D
-    line = ours(args, rank, world, dist)
+    line = (ours_c4 if args.workload == "c4s" else ours_c2)(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -41,6 +41,11 @@ class SpaceLibrary:
     def __init__(self):
         self.spaces = {}
 
+    @staticmethod
+    def dim(N, k):
+        """Unknowns of P_k with every exterior node Dirichlet: the interior nodes of the lattice."""
+        return (k * N - 1) ** 2
+
     def get(self, N, k):
         s = self.spaces.get((N, k))
         if s is None:
@@ -109,7 +114,10 @@ class Request:
     converged: bool = False
     residual: float = math.nan
     status: int = 0
+    outer: int = 0                # reliable updates (mixed precision)
     x: object = None              # the solution (kept when the server is asked to)
+    b: object = None              # poisson: the load vector (device, or pinned host: copied in), else seeded
+    out: object = None            # a host tensor that receives the solution
 
     @property
     def latency(self):
@@ -191,6 +199,7 @@ class Server:
             S.member = self.batch.add(S.A)
         self.launches = 0
         self.active = {}
+        self.last_launch_s = 0.0
 
     def _admit(self, r, budget):
         """Set the request up and arm it; the bytes it takes, or None when it has to wait."""
@@ -209,7 +218,7 @@ class Server:
             self.active[S.member] = (r, S, None, b, x, need)
         else:
             K = stiffness(self.lib, r.N, r.k, r.c)
-            b = poisson_rhs(K.nrows, r.seed)
+            b = _rhs(r, K.nrows)
             x = torch.zeros(K.nrows, dtype=torch.float64, device=b.device)
             mid = self.batch.add(K)
             self.batch.arm(mid, b, x, tol=self.tol)
@@ -259,9 +268,12 @@ class Server:
                     r, S, K, b, x, _ = self.active.pop(mid)
                     r.t_done = t_done
                     r.iterations, r.converged = res["iterations"], res["converged"]
-                    r.residual, r.status = res["residual"], res["status"]
+                    r.residual, r.status, r.outer = res["residual"], res["status"], res["reliable_updates"]
+                    self.last_launch_s = res["seconds"]
                     if self.keep:
                         r.x = x
+                    if r.out is not None:
+                        r.out.copy_(x, non_blocking=True)
                     if S is not None:
                         S.u = x
                         S.busy = False
@@ -275,6 +287,7 @@ class Server:
                     time.sleep(wait - 1e-3)
             if time.perf_counter() - t0 > max_seconds:
                 break
+        torch.cuda.synchronize()                    # results copied out to host buffers
         return summarize(trace, time.perf_counter() - t0)
 
 
@@ -303,7 +316,7 @@ def run_plain(lib, sessions, trace, *, tol=1e-10, realtime=True, keep_solutions=
             S.u = x
         else:
             K = stiffness(lib, r.N, r.k, r.c)
-            b = poisson_rhs(K.nrows, r.seed)
+            b = _rhs(r, K.nrows)
             x, conv, its, res, brk = fb.cg_solve(K, fb.JacobiPreconditioner(K), b, None, max(1000, 10 * K.nrows), tol,
                                                  mixed=mixed)
         torch.cuda.synchronize()
@@ -311,4 +324,17 @@ def run_plain(lib, sessions, trace, *, tol=1e-10, realtime=True, keep_solutions=
         r.iterations, r.converged, r.residual = its, conv, res
         if keep_solutions:
             r.x = x
+        if r.out is not None:
+            r.out.copy_(x, non_blocking=True)
+            torch.cuda.synchronize()
     return summarize(trace, time.perf_counter() - t0)
+
+
+def _rhs(r, n):
+    """The request's load vector on the device: its own (copied in from pinned host memory when
+    it is there) or the seeded N(0, 1) one."""
+    if r.b is None:
+        return poisson_rhs(n, r.seed)
+    if r.b.numel() != n:
+        raise ValueError("serve: load vector length differs from the problem")
+    return r.b if r.b.is_cuda else r.b.to("cuda", non_blocking=True)
