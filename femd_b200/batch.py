@@ -161,9 +161,10 @@ class Batch:
     def profile(self):
         """Cycle counters of the last launch summed over blocks: kernel, team-barrier waits,
         SpMV chunk-barrier waits (femd_cuda_batch_profile)."""
-        out = (C.c_longlong * 3)()
+        out = (C.c_longlong * 7)()
         check(lib.femd_cuda_batch_profile(self.h, out))
-        return dict(block=out[0], team_wait=out[1], chunk_sync=out[2])
+        return dict(block=out[0], team_wait=out[1], chunk_sync=out[2], fail_where=out[3], fail_at=out[4],
+                    fail_team=out[5], fail_seen=out[6])
 
     def debug(self, ghost_problem=-1, spin_limit=0):
         check(lib.femd_cuda_batch_debug(self.h, int(ghost_problem), int(spin_limit)))

@@ -28,7 +28,8 @@
 // row's owner stores) from the previous direction, held in a second buffer.
 //
 // Modes: FP64 Jacobi-PCG (cg.hpp:296-350 semantics, final true residual included) or mixed
-// precision: FP32 matrix copy (made by each rank from the FP64 values when the solve starts),
+// precision: FP32 matrix copy (made by k_batch_f32 before the member's first launch -- the bulk
+// copies only read what earlier launches wrote),
 // FP32 vectors and SpMV accumulation; FP64 residual b - A x on the FP64 matrix and FP64 solution
 // update at reliable updates.
 #include <algorithm>
@@ -66,6 +67,8 @@ struct BProb {
     float *r32, *z32, *pa32, *pb32, *Ap32, *d32;
     double *r64, *z64, *pa64, *pb64, *Ap64;
     double *part;          // 8 kinds x team
+    double *cpart;         // per-chunk sums of the SpMV passes: 6 kinds x nch (start 0-2, direction 3, residual 4-5)
+    unsigned long long *claim;   // chunk claims of the SpMV passes
     unsigned *bar;
     BState *st;
 };
@@ -79,6 +82,9 @@ struct BQueue {
     // cycle counters of the launch (thread 0 of every block): in the kernel, waiting at team
     // barriers, and waiting at the SpMV chunk barriers
     unsigned long long block_cycles, team_wait_cycles, chunk_sync_cycles;
+    // the first wait that gave up: 1 a team barrier, 2 a staging barrier; the barrier phase (team)
+    // or the chunk (staging) it was at, and the member's id in the launch (its slot's member)
+    int fail_where, fail_at, fail_team, fail_rank;
 };
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
@@ -115,7 +121,16 @@ __device__ bool team_barrier(const BProb &P, unsigned &phase, BQueue *q, volatil
             while (ld_acquire(P.bar) < target) {
                 if (((++spins) & 255) == 0) {
                     if (*(volatile int *)&q->flag) { ok = 0; break; }
-                    if (spins > lim) { atomicCAS(&q->flag, 0, FEMD_ETIMEOUT); ok = 0; break; }
+                    if (spins > lim) {
+                        if (atomicCAS(&q->flag, 0, FEMD_ETIMEOUT) == 0) {
+                            q->fail_where = 1;
+                            q->fail_at = (int)phase;
+                            q->fail_team = P.team;
+                            q->fail_rank = (int)ld_acquire(P.bar);
+                        }
+                        ok = 0;
+                        break;
+                    }
                 }
                 __nanosleep(32);
             }
@@ -247,6 +262,9 @@ struct ChunkSmem {
     double prod[2][CAP];       // FP64 products, or FP32 products in the first half
     uint64_t mbar[2];
     int fail;
+    int cid[2];                // the chunk staged in each buffer (-1: none)
+    double wsum[2][16][3];     // a chunk's warp partial sums, per buffer
+    double ctot[16][3];        // warp partials of the chunk-ordered team sums
 };
 
 // the part of chunk c that bulk copies bring in: nonzeros [qa, qb) with qa = qs rounded down to
@@ -260,9 +278,8 @@ __device__ __forceinline__ int staged_end(int qa, int qe, int nnz4)
 }
 
 template <class V, int CAP>
-__device__ __forceinline__ void stage_issue(const BProb &P, const V *A, int c, ChunkSmem<CAP> &S)
+__device__ __forceinline__ void stage_issue(const BProb &P, const V *A, int c, int s, ChunkSmem<CAP> &S)
 {
-    const int s = c & 1;
     const int qs = P.cq[c], qe = P.cq[c + 1];
     const int qa = qs & ~3, qb = staged_end(qa, qe, P.nnz & ~3);
     const unsigned n = (unsigned)(qb - qa);
@@ -274,21 +291,55 @@ __device__ __forceinline__ void stage_issue(const BProb &P, const V *A, int c, C
     }
 }
 
-// CSR-stream SpMV over chunks [c0, c1): chunk c+1's indices and values are copied into shared
-// memory while chunk c is computed; products a_q * g(col_q) go to shared memory (buffer c & 1)
-// and out(row, sum) gets each row's products summed in order by one thread.  Vectors that the
-// team writes during the launch take plain coherent loads (inside g).  false: a staging copy did
-// not land (the batch is stopped; the other outstanding copy has been waited for).
-template <class V, class F, int BB, int NPT, class Gather, class Pre, class RowOut>
-__device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, int c1, ChunkSmem<BB * NPT> &S, unsigned &par,
-                                           BQueue *q, Gather g, Pre pre, RowOut out)
+// CSR-stream SpMV over the member's chunks, claimed dynamically by the ranks of its team from
+// the member's counter (claims base .. base + nch - 1 are the chunks of this pass; every rank
+// makes exactly one claim past them, so the next pass starts at base + nch + team).  Chunk
+// claims run two ahead: bulk copies bring a claimed chunk's column indices and values into
+// shared memory while the one before it is computed.  Products a_q * g(col_q) go to shared
+// memory and out(row, sum, pre(row), acc) gets each row's products summed in order by one
+// thread and adds the row's share of NK sums to acc; the block sums acc per chunk in warp
+// order and writes it to cpart[k * nch + chunk].  So a sum over the chunks in chunk order (team
+// sum below) depends on the member and the launch shape alone, whichever rank took which chunk.
+// Vectors that the team writes during the launch take plain coherent loads (inside g).
+// false: a staging copy did not land (the batch is stopped; the outstanding copy was waited for).
+template <class V, class F, int BB, int NPT, int NK, class Gather, class Pre, class RowOut>
+__device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, unsigned long long base, double *cpart, int kbase,
+                                           ChunkSmem<BB * NPT> &S, unsigned &par, BQueue *q, Gather g, Pre pre, RowOut out)
 {
-    if (c0 >= c1) return true;
+    const int nch = P.nch;
     const int nnz4 = P.nnz & ~3;
-    if (threadIdx.x == 0) stage_issue<V>(P, A, c0, S);
-    for (int c = c0; c < c1; ++c) {
-        const int s = c & 1;
-        if (c + 1 < c1 && threadIdx.x == 0) stage_issue<V>(P, A, c + 1, S);
+    auto claim = [&]() -> int {
+        const unsigned long long v = atomicAdd(P.claim, 1ull) - base;
+        return v < (unsigned long long)nch ? (int)v : -1;
+    };
+    auto flush = [&](int c, int buf) {                    // thread 0: a chunk's sums, warps in order
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < BB / 32; ++w) t += S.wsum[buf][w][k];
+            cpart[(size_t)(kbase + k) * nch + c] = t;
+        }
+    };
+    __syncthreads();                                      // earlier readers of cid and the buffers are done
+    if (threadIdx.x == 0) {
+        fence_proxy_async_global();                       // values written by the team before: bulk-copy readable
+        const int a0 = claim();
+        S.cid[0] = a0;
+        S.cid[1] = -1;
+        if (a0 >= 0) {
+            stage_issue<V>(P, A, a0, 0, S);
+            const int a1 = claim();
+            S.cid[1] = a1;
+            if (a1 >= 0) stage_issue<V>(P, A, a1, 1, S);
+        }
+    }
+    __syncthreads();
+    int j = 0, cprev = -1;
+    for (;; ++j) {
+        const int b = j & 1;
+        const int c = S.cid[b];
+        if (c < 0) break;
         const int rs = P.crow[c], re = P.crow[c + 1];
         const int qs = P.cq[c], qe = P.cq[c + 1];
         const int qa = qs & ~3, qb = staged_end(qa, qe, nnz4);
@@ -298,14 +349,14 @@ __device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, i
         if (row0 < re) {
             lo0 = P.indptr[row0];
             hi0 = P.indptr[row0 + 1];
-            pv = pre(row0);                                   // the row's own values, loaded early
+            pv = pre(row0);                               // the row's own values, loaded early
         }
-        const bool ok = mbar_wait(&S.mbar[s], (par >> s) & 1u);
-        par ^= 1u << s;
+        const bool ok = mbar_wait(&S.mbar[b], (par >> b) & 1u);
+        par ^= 1u << b;
         if (ok) {
-            const int *ixs = S.ix[s];
-            const V *vs = reinterpret_cast<const V *>(S.val[s]);
-            F *buf = reinterpret_cast<F *>(S.prod[s]);
+            const int *ixs = S.ix[b];
+            const V *vs = reinterpret_cast<const V *>(S.val[b]);
+            F *buf = reinterpret_cast<F *>(S.prod[b]);
             int col[NPT];
             V a[NPT];
 #pragma unroll
@@ -329,14 +380,33 @@ __device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, i
         __syncthreads();
         if (threadIdx.x == 0) atomicAdd(&q->chunk_sync_cycles, (unsigned long long)(clock64() - ts));
         if (S.fail) {
-            // stop the batch; wait (bounded) for the copy of chunk c + 1 before the block leaves
+            // stop the batch; wait (bounded) for the copy still in flight before the block leaves
             if (threadIdx.x == 0) {
-                atomicCAS(&q->flag, 0, FEMD_ETIMEOUT);
-                if (c + 1 < c1) mbar_wait(&S.mbar[s ^ 1], (par >> (s ^ 1)) & 1u);
+                if (atomicCAS(&q->flag, 0, FEMD_ETIMEOUT) == 0) {
+                    q->fail_where = 2;
+                    q->fail_at = c;
+                    q->fail_team = P.team;
+                    q->fail_rank = (int)par;
+                }
+                if (S.cid[b ^ 1] >= 0) mbar_wait(&S.mbar[b ^ 1], (par >> (b ^ 1)) & 1u);
             }
             return false;
         }
-        const F *buf = reinterpret_cast<const F *>(S.prod[s]);
+        if (threadIdx.x == 0) {
+            if (cprev >= 0) flush(cprev, b ^ 1);          // its warps' sums were written before the barrier
+            // buffer b is free (every thread read it before the barrier): the chunk after next goes
+            // there, unless the claim for the next one was already past the end
+            int nx = -1;
+            if (S.cid[b ^ 1] >= 0) {
+                nx = claim();
+                if (nx >= 0) stage_issue<V>(P, A, nx, b, S);
+            }
+            S.cid[b] = nx;
+        }
+        double acc[NK];
+#pragma unroll
+        for (int k = 0; k < NK; ++k) acc[k] = 0.0;
+        const F *buf = reinterpret_cast<const F *>(S.prod[b]);
         for (int row = row0; row < re; row += BB) {
             int lo = lo0, hi = hi0;
             if (row != row0) {
@@ -346,34 +416,91 @@ __device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, int c0, i
             }
             F sum = F(0);
             for (int qq = lo; qq < hi; ++qq) sum += buf[qq - qs];
-            out(row, sum, pv);
+            out(row, sum, pv, acc);
         }
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+            const double t = warp_sum(acc[k]);
+            if ((threadIdx.x & 31) == 0) S.wsum[b][threadIdx.x >> 5][k] = t;
+        }
+        cprev = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && cprev >= 0) flush(cprev, (j - 1) & 1);
+    return true;
+}
+
+// Regions of the per-chunk sums, one per kind of pass.  A rank that has read a pass's sums goes on
+// to the next pass at once, while slower ranks may still be reading: consecutive passes write
+// different regions, and a region is written again only after a team barrier that every rank
+// reaches after its reads.
+static constexpr int KB_START = 0, KB_DIR = 3, KB_RES = 4, KB_KINDS = 6;
+
+// the team's totals of NK chunk sums of region kbase: meet, then every rank sums cpart over the
+// chunks in chunk order (thread-strided, then warps in order) -- the same bits on every rank
+template <int NK, int BB, int CAP>
+__device__ bool team_sum_chunks(const BProb &P, const double *cpart, int kbase, double (&v)[NK], ChunkSmem<CAP> &S,
+                                unsigned &phase, BQueue *q, volatile const int *abort_flag)
+{
+    if (!team_barrier(P, phase, q, abort_flag, true)) return false;
+    const int nch = P.nch;
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        double t = 0.0;
+        for (int i = threadIdx.x; i < nch; i += BB) t += __ldcg(cpart + (size_t)(kbase + k) * nch + i);
+        t = warp_sum(t);
+        if ((threadIdx.x & 31) == 0) S.ctot[threadIdx.x >> 5][k] = t;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < BB / 32; ++w) t += S.ctot[w][k];
+        v[k] = t;
     }
     return true;
 }
 
-// the FP64 residual r = b - A64 x on chunks [c0, c1): stores r and z = inv r (FP32 copies in
-// mixed mode), adds the shares of ||r||^2 (FP64) and r.z
-template <int BB, int NPT, bool MIXED>
-__device__ __forceinline__ bool residual_chunks(const BProb &P, int c0, int c1, ChunkSmem<BB * NPT> &S, unsigned &par, BQueue *q,
-                                                double &rr, double &rz)
+template <class F>
+struct ResPre {
+    double b;
+    F inv;
+};
+
+// the FP64 residual r = b - A64 x over the member's chunks: stores r and z = inv r (FP32 copies
+// in mixed mode; the inverse diagonal rounded from the FP64 one, the same value as the FP32
+// copy); chunk sums of ||r||^2 (FP64), r.z and, when START, ||b||^2, and then also zeroes the
+// previous direction (and the mixed correction d) of every row
+template <int BB, int NPT, bool MIXED, bool START>
+__device__ __forceinline__ bool residual_chunks(const BProb &P, unsigned long long base, ChunkSmem<BB * NPT> &S, unsigned &par,
+                                                BQueue *q)
 {
+    using F = typename std::conditional<MIXED, float, double>::type;
+    constexpr int NK = START ? 3 : 2;
     const double *x = P.x;
-    return chunk_spmv<double, double, BB, NPT>(
-        P, P.A64, c0, c1, S, par, q, [&](int j) { return x[j]; }, [&](int i) { return P.b[i]; },
-        [&](int i, double s, double bi) {
-            const double ri = bi - s;
-            rr += ri * ri;
+    F *pb = MIXED ? (F *)P.pb32 : (F *)P.pb64;
+    return chunk_spmv<double, double, BB, NPT, NK>(
+        P, P.A64, base, P.cpart, START ? KB_START : KB_RES, S, par, q, [&](int j) { return x[j]; },
+        [&](int i) { return ResPre<F>{P.b[i], (F)P.inv64[i]}; },
+        [&](int i, double s, const ResPre<F> &pv, double (&acc)[NK]) {
+            const double ri = pv.b - s;
+            acc[0] += ri * ri;
             if (MIXED) {
-                const float rf = (float)ri, zf = P.inv32[i] * rf;
+                const float rf = (float)ri, zf = (float)pv.inv * rf;
                 P.r32[i] = rf;
                 P.z32[i] = zf;
-                rz += (double)rf * (double)zf;
+                acc[1] += (double)rf * (double)zf;
             } else {
-                const double zi = P.inv64[i] * ri;
+                const double zi = (double)pv.inv * ri;
                 P.r64[i] = ri;
                 P.z64[i] = zi;
-                rz += ri * zi;
+                acc[1] += ri * zi;
+            }
+            if (START) {
+                acc[NK - 1] += pv.b * pv.b;
+                pb[i] = F(0);
+                if (MIXED) P.d32[i] = 0.0f;
             }
         });
 }
@@ -410,7 +537,9 @@ __device__ __forceinline__ void update_rows(F *r, F *z, const F *Ap, const F *in
 }
 
 // rank m of the member's team: advance the solve by at most q->iters iterations; false when the
-// batch has to stop
+// batch has to stop.  The SpMV passes take chunks dynamically (chunk_spmv); the elementwise update
+// and the FP32 copy at the start work on the rank's own rows (the rows of chunks
+// [nch m / T, nch (m+1) / T)) and reduce per rank in rank order.
 template <bool MIXED, int BB, int NPT>
 __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const int *abort_flag, ChunkSmem<BB * NPT> &SM,
                              unsigned &par)
@@ -428,27 +557,18 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
     const F *A = MIXED ? (const F *)P.A32 : (const F *)P.A64;
     F *acc = MIXED ? (F *)P.d32 : (F *)P.x;
     unsigned phase = 0;
+    unsigned long long base = 0;                          // claim base of the next SpMV pass
+    const unsigned long long pass = (unsigned long long)P.nch + (unsigned long long)T;
     const bool lead = m == 0 && threadIdx.x == 0;
     BState S = *P.st;
 
     if (!(S.flags & BS_STARTED)) {
-        // start: (mixed) the FP32 copies of this rank's rows; r = b - A x0, z = inv r, pold = 0
-        if (MIXED) {
-            const int q0 = P.cq[c0], q1 = P.cq[c1];
-            for (int qq = q0 + (int)threadIdx.x; qq < q1; qq += BB) P.A32[qq] = (float)P.A64[qq];
-            for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) P.inv32[i] = (float)P.inv64[i];
-            fence_proxy_async_global();                   // A32 is read by bulk copies later
-            __syncthreads();                              // inv32 is read by the row owners below
-        }
-        double v[3] = {0.0, 0.0, 0.0};                    // ||r||^2, r.z, ||b||^2
-        if (!residual_chunks<BB, NPT, MIXED>(P, c0, c1, SM, par, q, v[0], v[1])) return false;
-        for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) {
-            const double bi = P.b[i];
-            v[2] += bi * bi;
-            pb[i] = F(0);
-            if (MIXED) P.d32[i] = 0.0f;
-        }
-        if (!team_reduce<3, BB>(P, m, 0, v, phase, q, abort_flag)) return false;
+        // start: r = b - A x0, z = inv r, pold = 0 (the FP32 copies of A and inv were made by
+        // k_batch_f32 before the launch: bulk copies read only what earlier launches wrote)
+        if (!residual_chunks<BB, NPT, MIXED, true>(P, base, SM, par, q)) return false;
+        base += pass;
+        double v[3];                                      // ||r||^2, r.z, ||b||^2
+        if (!team_sum_chunks<3, BB>(P, P.cpart, KB_START, v, SM, phase, q, abort_flag)) return false;
         const double nb = sqrt(v[2]), rn0 = sqrt(v[0]);
         S.flags = BS_STARTED;
         S.it = 0;
@@ -479,18 +599,19 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
     const int it_end = it_lim < (long long)P.max_iter ? (int)it_lim : P.max_iter;
     F *pold = (it & 1) ? pa : pb, *pnew = (it & 1) ? pb : pa;
     while (!brk && !done && it < it_end) {
-        double pap[1] = {0.0};
         const F fb = (F)beta;
-        const bool ok = chunk_spmv<F, F, BB, NPT>(
-            P, A, c0, c1, SM, par, q, [&](int j) { return pdir(z, pold, fb, j); },
+        const bool ok = chunk_spmv<F, F, BB, NPT, 1>(
+            P, A, base, P.cpart, KB_DIR, SM, par, q, [&](int j) { return pdir(z, pold, fb, j); },
             [&](int i) { return pdir(z, pold, fb, i); },
-            [&](int i, F s, F pi) {
+            [&](int i, F s, F pi, double (&a)[1]) {
                 pnew[i] = pi;
                 Ap[i] = s;
-                pap[0] += (double)pi * (double)s;
+                a[0] += (double)pi * (double)s;
             });
         if (!ok) return false;
-        if (!team_reduce<1, BB>(P, m, 3, pap, phase, q, abort_flag)) return false;
+        base += pass;
+        double pap[1];
+        if (!team_sum_chunks<1, BB>(P, P.cpart, KB_DIR, pap, SM, phase, q, abort_flag)) return false;
         if (!(pap[0] > 0.0)) { brk = true; break; }
         const double alpha = rz / pap[0];
         double u[2] = {0.0, 0.0};                         // ||r||^2, r.z
@@ -513,9 +634,10 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
                     P.d32[i] = 0.0f;
                 }
                 if (!team_barrier(P, phase, q, abort_flag, true)) return false;
-                double w[2] = {0.0, 0.0};
-                if (!residual_chunks<BB, NPT, true>(P, c0, c1, SM, par, q, w[0], w[1])) return false;
-                if (!team_reduce<2, BB>(P, m, 6, w, phase, q, abort_flag)) return false;
+                if (!residual_chunks<BB, NPT, true, false>(P, base, SM, par, q)) return false;
+                base += pass;
+                double w[2];
+                if (!team_sum_chunks<2, BB>(P, P.cpart, KB_RES, w, SM, phase, q, abort_flag)) return false;
                 ++rus;
                 const double rt = sqrt(w[0]);
                 res = rt / nb;
@@ -537,9 +659,10 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
     if (finished) {
         if (!MIXED) {
             // the true residual (cg.hpp:222-237): every rank's x is final at the last reduction
-            double w[2] = {0.0, 0.0};
-            if (!residual_chunks<BB, NPT, false>(P, c0, c1, SM, par, q, w[0], w[1])) return false;
-            if (!team_reduce<2, BB>(P, m, 6, w, phase, q, abort_flag)) return false;
+            if (!residual_chunks<BB, NPT, false, false>(P, base, SM, par, q)) return false;
+            base += pass;
+            double w[2];
+            if (!team_sum_chunks<2, BB>(P, P.cpart, KB_RES, w, SM, phase, q, abort_flag)) return false;
             res = sqrt(w[0]) / nb;
         } else if (brk) {
             for (int i = r0 + (int)threadIdx.x; i < r1; i += BB) {
@@ -607,6 +730,15 @@ __global__ void __launch_bounds__(BB, 1024 / BB) k_batch_pcg(const BProb *__rest
     }
 }
 
+// the FP32 copies of a member's values and inverse diagonal (mixed mode), before its first launch
+__global__ void k_batch_f32(const double *__restrict__ a, float *__restrict__ a32, long long nnz, const double *__restrict__ inv,
+                            float *__restrict__ inv32, int n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += stride) a32[i] = (float)a[i];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv32[i] = (float)inv[i];
+}
+
 // chunk tables of one matrix: chunk k starts at the first row whose first nonzero is at or after
 // k * cp (cp = chunk capacity - longest row), so no chunk holds more than the capacity
 __global__ void k_chunk_table(const int *__restrict__ indptr, int n, int nnz, int cp, int nch, int *crow, int *cq)
@@ -668,12 +800,14 @@ struct Member {
     int n = 0, team = 1, nch = 0, maxlen = 0;
     long long nnz = 0;
     DevBuf<int> tables;                         // crow (nch+1), cq (nch+1)
+    DevBuf<double> cpart;                       // per-chunk sums of the SpMV passes (6 x nch)
     float *f32 = nullptr;                       // A32, inv32, r, z, p, p', Ap, d
     double *f64 = nullptr;                      // r, z, p, p', Ap
     const double *b = nullptr;
     double *x = nullptr;
     double tol = 0.0;
     int max_iter = 0;
+    bool need_f32 = false;                      // armed: the FP32 copies are made before its first mixed launch
 };
 
 }  // namespace
@@ -689,6 +823,7 @@ struct femd_batch_s : femd::HandleBase {
     DevBuf<BProb> d_probs;
     DevBuf<BState> d_state;
     DevBuf<unsigned> d_bar;
+    DevBuf<unsigned long long> d_claim;
     DevBuf<int> d_slots;                        // slot_prob then slot_member (2 x slot_cap)
     DevBuf<double> d_part;
     DevBuf<BQueue> d_queue;
@@ -755,6 +890,10 @@ static int member_layout(femd_batch_s *B, Member &M)
         int st = M.tables.alloc(2 * (size_t)(nch + 1));
         if (st) return st;
     }
+    if (M.cpart.n < KB_KINDS * (size_t)nch) {
+        int st = M.cpart.alloc(KB_KINDS * (size_t)nch);
+        if (st) return st;
+    }
     M.nch = nch;
     k_chunk_table<<<grid_for((size_t)nch + 1, 256), 256, 0, counted(s)>>>(M.K->pattern->indptr.p, M.n, (int)M.nnz, cp, nch,
                                                                           M.tables.p, M.tables.p + nch + 1);
@@ -769,7 +908,7 @@ static int grow_arrays(femd_batch_s *B, int cap)
     if (cap <= B->cap) return FEMD_OK;
     cap = std::max(cap, 2 * B->cap);
     int st;
-    if ((st = B->d_probs.alloc(cap)) || (st = B->d_bar.alloc(cap))) return st;
+    if ((st = B->d_probs.alloc(cap)) || (st = B->d_bar.alloc(cap)) || (st = B->d_claim.alloc(cap))) return st;
     {
         // members may be part-way through a resumable solve: keep their states
         BState *ns = nullptr;
@@ -930,6 +1069,8 @@ static BProb describe(femd_batch_s *B, int id, bool mixed)
     P.b = M.b;
     P.x = M.x;
     P.bar = B->d_bar.p + id;
+    P.claim = B->d_claim.p + id;
+    P.cpart = M.cpart.p;
     P.st = B->d_state.p + id;
     return P;
 }
@@ -961,6 +1102,7 @@ static cudaError_t enqueue_step(femd_batch_s *B, bool mixed, cudaStream_t s)
     if ((e = cudaMemcpyAsync(B->d_probs.p, B->h_desc, cap * sizeof(BProb), cudaMemcpyHostToDevice, s))) return e;
     if ((e = cudaMemcpyAsync(B->d_slots.p, B->h_slots, 2 * B->slot_cap * sizeof(int), cudaMemcpyHostToDevice, s))) return e;
     if ((e = cudaMemsetAsync(B->d_bar.p, 0, cap * sizeof(unsigned), s))) return e;
+    if ((e = cudaMemsetAsync(B->d_claim.p, 0, cap * sizeof(unsigned long long), s))) return e;
     if ((e = cudaMemcpyAsync(B->d_queue.p, B->h_q0, sizeof(BQueue), cudaMemcpyHostToDevice, s))) return e;
     if ((e = launch_batch(B, mixed, s))) return e;
     if ((e = cudaMemcpyAsync(B->h_state, B->d_state.p, cap * sizeof(BState), cudaMemcpyDeviceToHost, s))) return e;
@@ -995,6 +1137,17 @@ static int batch_step(femd_ctx ctx, femd_batch_s *B, int iters, bool mx, int *nf
     if (nfinished) *nfinished = 0;
     if (seconds) *seconds = 0.0;
     if (order.empty()) return FEMD_OK;
+    if (mx) {
+        for (int id : order) {
+            Member &M = *B->mem[id];
+            if (!M.need_f32) continue;
+            const BProb P = describe(B, id, true);
+            k_batch_f32<<<grid_for((size_t)M.nnz, 256, 4 * (unsigned)B->ctx->sm_count), 256, 0, counted(s)>>>(
+                M.K->data.p, P.A32, M.nnz, M.K->inv.p, P.inv32, M.n);
+            FEMD_TRY_CUDA(cudaGetLastError());
+            M.need_f32 = false;
+        }
+    }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
         if (B->mem[a]->team != B->mem[b]->team) return B->mem[a]->team > B->mem[b]->team;
         return B->mem[a]->nnz > B->mem[b]->nnz;
@@ -1023,7 +1176,7 @@ static int batch_step(femd_ctx ctx, femd_batch_s *B, int iters, bool mx, int *nf
         }
         B->drop_graphs();
     }
-    *B->h_q0 = BQueue{0u, 0, B->spin_limit, (int)ns, std::max(1, iters), 0ull, 0ull, 0ull};
+    *B->h_q0 = BQueue{0u, 0, B->spin_limit, (int)ns, std::max(1, iters), 0ull, 0ull, 0ull, 0, 0, 0, 0};
     *(volatile int *)B->abort_host = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     FEMD_TRY_CUDA(cudaEventCreate(&e0));
@@ -1094,6 +1247,7 @@ static int arm_member(femd_batch_s *B, int id, const double *b, double *x, int m
     M.tol = tol;
     M.max_iter = max_iter > 0 ? max_iter : std::max(1000, 10 * M.n);
     M.armed = true;
+    M.need_f32 = true;
     FEMD_TRY_CUDA(cudaMemsetAsync(B->d_state.p + id, 0, sizeof(BState), B->ctx->stream));
     return FEMD_OK;
 }
@@ -1304,6 +1458,10 @@ int femd_cuda_batch_profile(femd_batch handle, long long *cycles_out)
     cycles_out[0] = (long long)B->h_qout->block_cycles;
     cycles_out[1] = (long long)B->h_qout->team_wait_cycles;
     cycles_out[2] = (long long)B->h_qout->chunk_sync_cycles;
+    cycles_out[3] = B->h_qout->fail_where;
+    cycles_out[4] = B->h_qout->fail_at;
+    cycles_out[5] = B->h_qout->fail_team;
+    cycles_out[6] = B->h_qout->fail_rank;
     return FEMD_OK;
 }
 

@@ -3,9 +3,13 @@
     python -m femd_b200.profile_kernels spmv --n 640 --k 2 --reps 3
     python -m femd_b200.profile_kernels assemble --n 640 --k 2 --reps 3
     python -m femd_b200.profile_kernels cg --n 640 --k 2
+    python -m femd_b200.profile_kernels batch --nmin 150 --nmax 256 --nprob 24 --iters 100 --mixed
 
 Workload: -Lap u + u = f on rectangle_mesh(0, 0, 1, 1, n, n), P_k, zero Dirichlet (the form of
 the config-2 benchmark at another size).  Prints the sizes and a CUDA-event time per launch.
+batch: the problems of the config-4 stream (seed 0) with N in [nmin, nmax] and k >= kmin, the
+first nprob of them, solved together by the batched PCG capped at iters iterations; prints the
+launch time and its algorithmic bytes (femd_b200.workloads.batch_bytes).
 """
 from __future__ import annotations
 
@@ -17,11 +21,19 @@ PI = math.pi
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("kernel", choices=["spmv", "assemble", "rhs", "cg", "cg_mixed", "pattern"])
+    ap.add_argument("kernel", choices=["spmv", "assemble", "rhs", "cg", "cg_mixed", "pattern", "batch"])
     ap.add_argument("--n", type=int, default=640)
     ap.add_argument("--k", type=int, default=2)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--nprob", type=int, default=24)
+    ap.add_argument("--nmin", type=int, default=150)
+    ap.add_argument("--nmax", type=int, default=256)
+    ap.add_argument("--kmin", type=int, default=2)
+    ap.add_argument("--iters", type=int, default=100)
+    ap.add_argument("--mixed", action="store_true")
     a = ap.parse_args()
+    if a.kernel == "batch":
+        return batch(a)
     import torch
 
     import femd_b200 as fb
@@ -62,6 +74,27 @@ def main():
     e1.record(s)
     e1.synchronize()
     print(f"{a.kernel}: n {V.dim} nnz {P.nnz} ncells {m.ncells}: {e0.elapsed_time(e1) / a.reps * 1e3:.1f} us per call")
+
+
+def batch(a):
+    import femd_b200 as fb
+    from femd_b200 import workloads as W
+    spec = [s for s in W.poisson_batch_spec(seed=0, nprob=256) if a.nmin <= s["N"] <= a.nmax and s["k"] >= a.kmin]
+    spec = spec[:a.nprob]
+    cache = W.SpaceCache()
+    probs = [W.build_poisson(s, cache) for s in spec]
+    B = fb.Batch([K for K, _ in probs])
+    bs = [b for _, b in probs]
+    for _ in range(a.reps):
+        xs, res = B.solve(bs, tol=1e-10, max_iter=a.iters, mixed=a.mixed)
+    sizes = [(K.nrows, K.nnz) for K, _ in probs]
+    alg = W.batch_bytes(sizes, res, a.mixed)
+    t = res[0]["seconds"]
+    pr = B.profile()
+    print(f"batch ({'mixed' if a.mixed else 'fp64'}): {len(probs)} problems, n {sum(n for n, _ in sizes)} "
+          f"nnz {sum(z for _, z in sizes)}, {B.info()['slots']} team slots on a grid of {B.info()['grid']}: "
+          f"{t * 1e3:.3f} ms per launch, algorithmic {alg} B = {alg / t / 1e9:.1f} GB/s; team-barrier wait "
+          f"{pr['team_wait'] / pr['block']:.3f}, chunk-barrier wait {pr['chunk_sync'] / pr['block']:.3f} of block cycles")
 
 
 if __name__ == "__main__":

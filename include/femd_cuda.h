@@ -305,9 +305,12 @@ FEMD_API int femd_cuda_batch_tune(femd_ctx ctx, femd_batch B, const double *cons
  * (<= 0: the default, a few seconds).  The launch then returns FEMD_ETIMEOUT and the context
  * stays usable.  No reference counterpart. */
 FEMD_API int femd_cuda_batch_debug(femd_batch B, int ghost_member, long long spin_limit);
-/* Cycle counters of the last launch, summed over the blocks (thread 0 of each): [0] cycles in the
- * kernel, [1] cycles waiting at team barriers, [2] cycles waiting at the SpMV chunk barriers.
- * Their ratios show how much of a launch is synchronisation.  No reference counterpart. */
+/* Counters of the last launch (cycles_out: 7 entries).  Cycles summed over the blocks (thread 0 of
+ * each): [0] in the kernel, [1] waiting at team barriers, [2] waiting at the SpMV chunk barriers
+ * -- their ratios show how much of a launch is synchronisation.  When a bounded wait gave up
+ * (FEMD_ETIMEOUT): [3] which (1 a team barrier, 2 a staging copy), [4] the barrier phase or the
+ * chunk, [5] the team size, [6] the barrier count seen (team) or the staging parity bits.  No
+ * reference counterpart. */
 FEMD_API int femd_cuda_batch_profile(femd_batch B, long long *cycles_out);
 
 /* ======================================================================================
