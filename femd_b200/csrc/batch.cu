@@ -47,12 +47,15 @@ namespace femd {
 
 static constexpr long long SPIN_LIMIT = 1ll << 25;   // default bound of a barrier wait (spins of ~0.5 us)
 
-enum : int { BS_STARTED = 1, BS_DONE = 2, BS_BREAKDOWN = 4, BS_CONVERGED = 8 };
+enum : int { BS_STARTED = 1, BS_DONE = 2, BS_BREAKDOWN = 4, BS_CONVERGED = 8, BS_FALLBACK = 16 };
 
 // a member's solver scalars, kept in device memory between launches
 struct BState {
     double rz, beta, maxr, nb, res;
+    double prt;            // mixed: the true residual of the last reliable update
     int it, rus, flags, status;
+    int stall;             // mixed: reliable updates in a row that reduced it by less than 2x
+    int pad;
 };
 
 struct BProb {
@@ -576,6 +579,8 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
         S.beta = 0.0;
         S.rz = v[1];
         S.maxr = rn0;
+        S.prt = rn0;
+        S.stall = 0;
         S.nb = nb;
         S.res = nb == 0.0 ? 0.0 : rn0 / nb;
         if (nb == 0.0) {
@@ -591,10 +596,10 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
             return true;
         }
     }
-    double rz = S.rz, beta = S.beta, maxr = S.maxr, res = S.res;
+    double rz = S.rz, beta = S.beta, maxr = S.maxr, res = S.res, prt = S.prt;
     const double nb = S.nb;
-    int it = S.it, rus = S.rus;
-    bool brk = (S.flags & BS_BREAKDOWN) != 0, done = false;
+    int it = S.it, rus = S.rus, stall = S.stall;
+    bool brk = (S.flags & BS_BREAKDOWN) != 0, done = false, fallback = false;
     const long long it_lim = (long long)it + q->iters;
     const int it_end = it_lim < (long long)P.max_iter ? (int)it_lim : P.max_iter;
     F *pold = (it & 1) ? pa : pb, *pnew = (it & 1) ? pb : pa;
@@ -643,8 +648,14 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
                 res = rt / nb;
                 maxr = rt;
                 if (rt <= P.tol * nb || it >= P.max_iter) { done = true; break; }
+                // stagnation of the FP32 recurrence (the FP32 matrix too coarse for the slowest
+                // modes): the host goes on in FP64 from this iterate
+                stall = rt > 0.5 * prt ? stall + 1 : 0;
+                prt = rt;
+                if (stall >= 2 || !(rt < 1e300)) { fallback = true; break; }
                 if (!(w[1] > 0.0)) { brk = true; break; }
-                beta = w[1] / rz;
+                // drifted recurrence (true residual over twice its own): restart the direction
+                beta = rt > 2.0 * rn ? 0.0 : w[1] / rz;
                 rz = w[1];
             } else {
                 beta = u[1] / rz;
@@ -655,7 +666,7 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
         pold = pnew;
         pnew = t;
     }
-    const bool finished = brk || done || it >= P.max_iter;
+    const bool finished = brk || done || fallback || it >= P.max_iter;
     if (finished) {
         if (!MIXED) {
             // the true residual (cg.hpp:222-237): every rank's x is final at the last reduction
@@ -678,8 +689,12 @@ __device__ bool solve_member(const BProb &P, int m, BQueue *q, volatile const in
         S.res = res;
         S.it = it;
         S.rus = rus;
+        S.prt = prt;
+        S.stall = stall;
         if (brk) S.flags |= BS_BREAKDOWN;
-        if (finished) {
+        if (fallback) {
+            S.flags |= BS_DONE | BS_FALLBACK;
+        } else if (finished) {
             const double tol = P.tol;
             int conv = !brk && res <= tol * (1.0 + 1e-6) + 1e-15;
             if (!conv && !brk && res <= 10.0 * tol && it < P.max_iter) conv = 1;
@@ -808,6 +823,8 @@ struct Member {
     double tol = 0.0;
     int max_iter = 0;
     bool need_f32 = false;                      // armed: the FP32 copies are made before its first mixed launch
+    bool force_fp64 = false;                    // its FP32 recurrence stagnated: FP64 for the rest of the solve
+    int prior_its = 0, prior_rus = 0;           // iterations and reliable updates before the switch
 };
 
 }  // namespace
@@ -1122,21 +1139,15 @@ static void fill_result(const BState &S, femd_cg_result &r, double seconds)
 
 // one launch over the armed members: each advances by at most iters iterations.  Members that
 // finish are disarmed and listed (ids, results) when the lists are given.
-static int batch_step(femd_ctx ctx, femd_batch_s *B, int iters, bool mx, int *nfinished, int *fin_ids, femd_cg_result *fin_res,
-                      double *seconds)
+// one launch over the members `order` (armed), all in one precision: each advances by at most
+// iters iterations; the states are in h_state afterwards, the launch time in *ms
+static int launch_set(femd_ctx ctx, femd_batch_s *B, std::vector<int> order, int iters, bool mx, float *ms)
 {
     cudaStream_t s = ctx->stream;
     int st;
-    std::vector<int> order;
-    for (int id = 0; id < (int)B->mem.size(); ++id) {
-        if (!B->mem[id] || !B->mem[id]->armed) continue;
-        Member &M = *B->mem[id];
-        if ((st = member_vectors(B, M, mx))) return st;
-        order.push_back(id);
-    }
-    if (nfinished) *nfinished = 0;
-    if (seconds) *seconds = 0.0;
-    if (order.empty()) return FEMD_OK;
+    *ms = 0.f;
+    for (int id : order)
+        if ((st = member_vectors(B, *B->mem[id], mx))) return st;
     if (mx) {
         for (int id : order) {
             Member &M = *B->mem[id];
@@ -1211,26 +1222,80 @@ static int batch_step(femd_ctx ctx, femd_batch_s *B, int iters, bool mx, int *nf
     }
     cudaEventRecord(e1, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    float ms = 0.f;
-    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (e != cudaSuccess) { set_error(std::string("batch: ") + cudaGetErrorString(e)); return FEMD_ECUDA; }
-    if (seconds) *seconds = ms * 1e-3;
-    const int flag = B->h_qout->flag;
-    int nf = 0;
-    for (int id : order) {
-        const BState &S = B->h_state[id];
-        if (!(S.flags & BS_DONE) && !flag && !S.status) continue;
-        B->mem[id]->armed = false;
-        if (fin_ids) fin_ids[nf] = id;
-        if (fin_res) {
-            fill_result(S, fin_res[nf], ms * 1e-3);
-            if (flag) fin_res[nf].status = flag;
+    return FEMD_OK;
+}
+
+// a member's result: its iterations and reliable updates include those of a mixed-precision
+// phase that fell back to FP64
+static void fill_member(const femd_batch_s *B, int id, femd_cg_result &r, double seconds)
+{
+    const BState &S = B->h_state[id];
+    const Member &M = *B->mem[id];
+    fill_result(S, r, seconds);
+    r.iterations += M.prior_its;
+    r.outer += M.prior_rus;
+}
+
+// one step: every armed member advances by at most iters iterations.  In a mixed step the members
+// whose FP32 recurrence stagnated before (or stagnates in this launch) go on in an FP64 launch in
+// the same call, from their current iterate.  Members that finish are disarmed and listed.
+static int batch_step(femd_ctx ctx, femd_batch_s *B, int iters, bool mx, int *nfinished, int *fin_ids, femd_cg_result *fin_res,
+                      double *seconds)
+{
+    std::vector<int> set32, set64;
+    for (int id = 0; id < (int)B->mem.size(); ++id) {
+        if (!B->mem[id] || !B->mem[id]->armed) continue;
+        (mx && !B->mem[id]->force_fp64 ? set32 : set64).push_back(id);
+    }
+    if (nfinished) *nfinished = 0;
+    if (seconds) *seconds = 0.0;
+    int nf = 0, st = FEMD_OK;
+    double sec = 0.0;
+    int flag = 0;
+    auto collect = [&](const std::vector<int> &set, bool mode) {
+        for (int id : set) {
+            const BState &S = B->h_state[id];
+            Member &M = *B->mem[id];
+            if (!(S.flags & BS_DONE) && !flag && !S.status) continue;
+            if (mode && (S.flags & BS_FALLBACK) && !flag && !S.status) {
+                // the FP32 recurrence stagnated: go on in FP64 from the iterate x
+                M.force_fp64 = true;
+                M.prior_its += S.it;
+                M.prior_rus += S.rus;
+                M.max_iter = std::max(1, M.max_iter - S.it);
+                cudaMemsetAsync(B->d_state.p + id, 0, sizeof(BState), ctx->stream);
+                set64.push_back(id);
+                continue;
+            }
+            M.armed = false;
+            if (fin_ids) fin_ids[nf] = id;
+            if (fin_res) {
+                fill_member(B, id, fin_res[nf], sec);
+                if (flag) fin_res[nf].status = flag;
+            }
+            ++nf;
         }
-        ++nf;
+    };
+    if (!set32.empty()) {
+        float ms = 0.f;
+        if ((st = launch_set(ctx, B, set32, iters, true, &ms))) return st;
+        sec += ms * 1e-3;
+        flag = B->h_qout->flag;
+        collect(set32, true);
+    }
+    if (!set64.empty() && !flag) {
+        float ms = 0.f;
+        if ((st = launch_set(ctx, B, set64, iters, false, &ms))) return st;
+        sec += ms * 1e-3;
+        flag = B->h_qout->flag;
+        collect(set64, false);
     }
     if (nfinished) *nfinished = nf;
+    if (seconds) *seconds = sec;
     if (flag == FEMD_ETIMEOUT) { set_error("batch: a team barrier wait ran out"); return FEMD_ETIMEOUT; }
     if (flag == FEMD_EABORT) { set_error("batch: aborted by the host"); return FEMD_EABORT; }
     return FEMD_OK;
@@ -1248,6 +1313,9 @@ static int arm_member(femd_batch_s *B, int id, const double *b, double *x, int m
     M.max_iter = max_iter > 0 ? max_iter : std::max(1000, 10 * M.n);
     M.armed = true;
     M.need_f32 = true;
+    M.force_fp64 = false;
+    M.prior_its = 0;
+    M.prior_rus = 0;
     FEMD_TRY_CUDA(cudaMemsetAsync(B->d_state.p + id, 0, sizeof(BState), B->ctx->stream));
     return FEMD_OK;
 }
@@ -1375,7 +1443,7 @@ int femd_cuda_batch_solve(femd_ctx ctx, femd_batch handle, const double *const *
     double sec = 0.0;
     st = batch_step(ctx, B, INT_MAX, mixed != 0, &nf, fin.data(), fr.data(), &sec);
     for (size_t p = 0; p < ids.size(); ++p) {
-        fill_result(B->h_state[ids[p]], results[p], sec);
+        fill_member(B, ids[p], results[p], sec);
         if (B->h_qout->flag) results[p].status = B->h_qout->flag;
         B->mem[ids[p]]->armed = false;
     }

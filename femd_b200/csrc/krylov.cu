@@ -28,12 +28,16 @@ static constexpr int RED_BLOCK = 256;
 
 template <class T>
 struct CGState {
-    T rz, pAp, alpha, beta, rr;
+    double rz, pAp, alpha, beta, rr;       // scalars and dot products in FP64 for both precisions
     double nb, tol_nb, rn, res64;          // FP64 scalars (norms of b and of the true residual)
     double maxr;                           // mixed precision: largest ||r|| since the last reliable update
-    T rz_prev;                             // mixed precision: r.z before the last recurrence step
+    double rz_prev;                        // mixed precision: r.z before the last recurrence step
     int it, done, breakdown, max_iter;
     int want_ru, ru_count;
+    // mixed precision: the true residual of the last reliable update, the updates in a row that
+    // reduced it by less than 2x, and the switch to FP64 after two of them (or a non-finite one)
+    double prt;
+    int stall, fallback;
     unsigned ticket;
 };
 
@@ -95,15 +99,15 @@ __device__ __forceinline__ void reduce_partials(const T *part, int np, int ld, T
 template <class V, class T, int TPR, int U, bool DOT>
 __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indptr, const int *__restrict__ indices,
                                                     const V *__restrict__ vals, const T *__restrict__ x,
-                                                    T *__restrict__ y, int n, T *__restrict__ part,
+                                                    T *__restrict__ y, int n, double *__restrict__ part,
                                                     CGState<T> *__restrict__ st)
 {
-    __shared__ T sh[32];
-    if (DOT && st->done) return;
+    __shared__ double sh[32];
+    if (DOT && (st->done || st->want_ru)) return;
     const int lane = threadIdx.x % TPR;
     constexpr int GPW = 32 / TPR;   // rows per warp per step
     const int gwarp = (blockIdx.x * RED_BLOCK + threadIdx.x) >> 5, nwarp = (gridDim.x * RED_BLOCK) >> 5;
-    T dot = T(0);
+    double dot = 0.0;                                     // x.y accumulated in FP64 (FP32 vectors too)
     // the loop bound is uniform across the warp, so the full-warp shuffles below are safe
     for (int i0 = gwarp * GPW; i0 < n; i0 += nwarp * GPW) {
         const int i = i0 + (threadIdx.x & 31) / TPR;
@@ -133,21 +137,21 @@ __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indp
         for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
         if (lane == 0 && i < n) {
             y[i] = s;
-            if (DOT) dot += x[i] * s;
+            if (DOT) dot += (double)x[i] * (double)s;
         }
     }
     if (!DOT) return;
-    T v[1] = {dot};
-    block_reduce<T, 1>(v, sh);
+    double v[1] = {dot};
+    block_reduce<double, 1>(v, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = v[0];
     if (!last_block(&st->ticket)) return;
-    T tot[1];
-    reduce_partials<T, 1>(part, gridDim.x, 0, tot, sh);
+    double tot[1];
+    reduce_partials<double, 1>(part, gridDim.x, 0, tot, sh);
     if (threadIdx.x == 0) {
         st->ticket = 0;
-        const T pAp = tot[0];
+        const double pAp = tot[0];
         st->pAp = pAp;
-        if (!(pAp > T(0))) { st->breakdown = 1; st->done = 1; }
+        if (!(pAp > 0.0)) { st->breakdown = 1; st->done = 1; }
         else st->alpha = st->rz / pAp;
     }
 }
@@ -157,30 +161,30 @@ __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indp
 template <class T, bool JAC>
 __global__ void __launch_bounds__(RED_BLOCK) k_cg_update(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p,
                                                          const T *__restrict__ Ap, const T *__restrict__ inv, int n,
-                                                         T *__restrict__ part, CGState<T> *__restrict__ st,
+                                                         double *__restrict__ part, CGState<T> *__restrict__ st,
                                                          int mixed)
 {
-    __shared__ T sh[64];
-    if (st->done) return;
-    const T a = st->alpha;
-    T rr = T(0), rz = T(0);
+    __shared__ double sh[64];
+    if (st->done || st->want_ru) return;                  // want_ru: paused for a reliable update (mixed)
+    const T a = (T)st->alpha;
+    double rr = 0.0, rz = 0.0;                            // FP64 accumulation (FP32 vectors too)
     for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
         const T ri = r[i] - a * Ap[i];
         r[i] = ri;
         x[i] = x[i] + a * p[i];
-        const T t = ri * ri;
+        const double t = (double)ri * (double)ri;
         rr += t;
-        if (JAC) rz += t * inv[i];
+        if (JAC) rz += t * (double)inv[i];
     }
-    T v[2] = {rr, rz};
-    block_reduce<T, 2>(v, sh);
+    double v[2] = {rr, rz};
+    block_reduce<double, 2>(v, sh);
     if (threadIdx.x == 0) { part[blockIdx.x] = v[0]; part[gridDim.x + blockIdx.x] = v[1]; }
     if (!last_block(&st->ticket)) return;
-    T tot[2];
-    reduce_partials<T, 2>(part, gridDim.x, gridDim.x, tot, sh);
+    double tot[2];
+    reduce_partials<double, 2>(part, gridDim.x, gridDim.x, tot, sh);
     if (threadIdx.x == 0) {
         st->ticket = 0;
-        const T rrn = tot[0], rzn = JAC ? tot[1] : tot[0];
+        const double rrn = tot[0], rzn = JAC ? tot[1] : tot[0];
         st->rr = rrn;
         st->it += 1;
         const double rn = sqrt((double)rrn);
@@ -190,7 +194,7 @@ __global__ void __launch_bounds__(RED_BLOCK) k_cg_update(T *__restrict__ x, T *_
             if (st->it >= st->max_iter) { st->done = 1; return; }      // loop condition
             st->beta = rzn / st->rz;                                   // cg.hpp:335-336
             st->rz = rzn;
-            if (!(rzn > T(0))) { st->breakdown = 1; st->done = 1; }    // cg.hpp:324 at the next loop top
+            if (!(rzn > 0.0)) { st->breakdown = 1; st->done = 1; }     // cg.hpp:324 at the next loop top
         } else {
             // mixed precision: ask for a reliable update when the recurrence residual has
             // dropped by a decade since the last one, or looks converged
@@ -198,7 +202,7 @@ __global__ void __launch_bounds__(RED_BLOCK) k_cg_update(T *__restrict__ x, T *_
             st->rz_prev = st->rz;
             st->beta = rzn / st->rz;
             st->rz = rzn;
-            if (!(rzn > T(0))) st->want_ru = 1;
+            if (!(rzn > 0.0)) st->want_ru = 1;
         }
     }
 }
@@ -209,8 +213,8 @@ __global__ void __launch_bounds__(RED_BLOCK) k_cg_direction(T *__restrict__ p, c
                                                             const T *__restrict__ inv, int n,
                                                             const CGState<T> *__restrict__ st)
 {
-    if (st->done) return;
-    const T b = st->beta;
+    if (st->done || st->want_ru) return;
+    const T b = (T)st->beta;
     for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK)
         p[i] = (JAC ? inv[i] * r[i] : r[i]) + b * p[i];
 }
@@ -321,46 +325,52 @@ __global__ void __launch_bounds__(RED_BLOCK) k_mixed_spmv64(const int *__restric
 // residual and the restart of the recurrence from it.
 __global__ void __launch_bounds__(RED_BLOCK) k_mixed_residual(const double *__restrict__ b, const double *__restrict__ Ax,
                                                               float *__restrict__ r32, const float *__restrict__ inv32, int n,
-                                                              double *__restrict__ part64, float *__restrict__ part32,
+                                                              double *__restrict__ part64, double *__restrict__ part32,
                                                               CGState<float> *__restrict__ st)
 {
     __shared__ double sh64[32];
-    __shared__ float sh32[32];
+    __shared__ double sh32[32];
     if (st->done || !st->want_ru) return;
-    double rr = 0.0;
-    float rz = 0.0f;
+    double rr = 0.0, rz = 0.0;
     for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
         const double ri = b[i] - Ax[i];
         const float rf = (float)ri;
         r32[i] = rf;
         rr += ri * ri;
-        rz += rf * rf * inv32[i];
+        rz += (double)rf * (double)rf * (double)inv32[i];
     }
     double v[1] = {rr};
     block_reduce<double, 1>(v, sh64);
-    float w[1] = {rz};
+    double w[1] = {rz};
     __syncthreads();
-    block_reduce<float, 1>(w, sh32);
+    block_reduce<double, 1>(w, sh32);
     if (threadIdx.x == 0) { part64[blockIdx.x] = v[0]; part32[blockIdx.x] = w[0]; }
     if (!last_block(&st->ticket)) return;
     double t64[1];
-    float t32[1];
+    double t32[1];
     reduce_partials<double, 1>(part64, gridDim.x, 0, t64, sh64);
     __syncthreads();
-    reduce_partials<float, 1>(part32, gridDim.x, 0, t32, sh32);
+    reduce_partials<double, 1>(part32, gridDim.x, 0, t32, sh32);
     if (threadIdx.x == 0) {
         st->ticket = 0;
         st->want_ru = 0;
         st->ru_count += 1;
         const double rn = sqrt(t64[0]);
+        const double rn_rec = st->rn;                     // the FP32 recurrence's own residual norm
         st->res64 = rn;
         st->rn = rn;
         st->maxr = rn;
         if (rn <= st->tol_nb || st->it >= st->max_iter) { st->done = 1; return; }
-        // continue the recurrence from the true residual: beta from the refreshed r.z
-        const float rzn = t32[0];
-        if (!(rzn > 0.0f)) { st->breakdown = 1; st->done = 1; return; }
-        st->beta = rzn / st->rz_prev;
+        // stagnation of the FP32 recurrence (the FP32 matrix too coarse for the slowest modes):
+        // the solve goes on in FP64 from this iterate
+        st->stall = (rn > 0.5 * st->prt) ? st->stall + 1 : 0;
+        st->prt = rn;
+        if (st->stall >= 2 || !(rn < 1e300)) { st->fallback = 1; st->done = 1; return; }
+        // continue the recurrence from the true residual: beta from the refreshed r.z; when the
+        // recurrence has drifted (true residual over twice its own) restart the direction
+        const double rzn = t32[0];
+        if (!(rzn > 0.0)) { st->breakdown = 1; st->done = 1; return; }
+        st->beta = rn > 2.0 * rn_rec ? 0.0 : rzn / st->rz_prev;
         st->rz = rzn;
     }
 }
@@ -456,7 +466,7 @@ static inline int shape_u(int shape) { return (shape >> 8) ? (shape >> 8) : 1; }
 
 template <class V, class T, bool DOT, int U>
 static void launch_spmv_u(int tpr, unsigned grid, cudaStream_t s, const int *ip, const int *ix, const V *v, const T *x, T *y,
-                          int n, T *part, CGState<T> *st)
+                          int n, double *part, CGState<T> *st)
 {
     switch (tpr) {
     case 2: k_spmv<V, T, 2, U, DOT><<<grid, RED_BLOCK, 0, counted(s)>>>(ip, ix, v, x, y, n, part, st); break;
@@ -469,7 +479,7 @@ static void launch_spmv_u(int tpr, unsigned grid, cudaStream_t s, const int *ip,
 
 template <class V, class T, bool DOT>
 static void launch_spmv(int shape, unsigned grid, cudaStream_t s, const int *ip, const int *ix, const V *v, const T *x, T *y,
-                        int n, T *part, CGState<T> *st)
+                        int n, double *part, CGState<T> *st)
 {
     const int tpr = shape_tpr(shape);
     switch (shape_u(shape)) {
@@ -506,7 +516,8 @@ struct SolverWS {
     // mixed precision
     bool mixed_ready = false;
     DevBuf<double> Ax64, r64, part64;
-    DevBuf<float> r32, p32, Ap32, d32, part32;
+    DevBuf<float> r32, p32, Ap32, d32;
+    DevBuf<double> part32;                       // the FP32 recurrence's block partials (FP64 sums)
     DevBuf<CGState<float>> st32;
     CGState<float> *st32_host = nullptr;
     cudaGraphExec_t xm = nullptr;
@@ -696,10 +707,11 @@ static int prepare_mixed(femd_ctx ctx, femd_matrix K, SolverWS &W)
     FEMD_TRY(W.part32.alloc(npart));
     FEMD_TRY(W.st32.alloc(1));
     FEMD_TRY_CUDA(cudaMallocHost(&W.st32_host, sizeof(CGState<float>)));
-    W.chm = n > (1 << 18) ? 8 : 16;
+    // a chunk is CHM iterations of the FP32 recurrence only (SpMV with p.Ap, update, direction);
+    // when the update asks for a reliable update the rest of the chunk is skipped (want_ru) and
+    // the host runs the FP64 tail (mixed_ru) before the next chunk
+    W.chm = 32;
     const unsigned gs = W.gs, gr = W.gr;
-    double *x = W.wx.p;
-    const double *b = W.wb.p;
     cudaGraph_t graph = nullptr;
     FEMD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < W.chm; ++k) {
@@ -707,16 +719,6 @@ static int prepare_mixed(femd_ctx ctx, femd_matrix K, SolverWS &W)
                                         W.part32.p, W.st32.p);
         k_cg_update<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.d32.p, W.r32.p, W.p32.p, W.Ap32.p, K->inv32.p, n, W.part32.p,
                                                                    W.st32.p, 1);
-        // a reliable update (when requested) before the direction update uses r
-        k_mixed_flush<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, W.d32.p, n, W.st32.p);
-        switch (shape_tpr(W.shape)) {
-        case 2: k_mixed_spmv64<2><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
-        case 4: k_mixed_spmv64<4><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
-        case 8: k_mixed_spmv64<8><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
-        case 16: k_mixed_spmv64<16><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
-        default: k_mixed_spmv64<32><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
-        }
-        k_mixed_residual<<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ax64.p, W.r32.p, K->inv32.p, n, W.part64.p, W.part32.p, W.st32.p);
         k_cg_direction<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.p32.p, W.r32.p, K->inv32.p, n, W.st32.p);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -727,6 +729,29 @@ static int prepare_mixed(femd_ctx ctx, femd_matrix K, SolverWS &W)
     if (ce != cudaSuccess) { W.xm = nullptr; set_error(std::string("pcg_mixed: ") + cudaGetErrorString(ce)); return FEMD_ECUDA; }
     W.mixed_ready = true;
     return FEMD_OK;
+}
+
+// The reliable update, when the FP32 recurrence asked for it: x += d, d = 0; r = b - A64 x in
+// FP64, r32 = (float) r, the convergence test on it and the restart of the recurrence; then the
+// direction update the paused chunk skipped.
+static void mixed_ru(femd_ctx ctx, femd_matrix K, SolverWS &W)
+{
+    femd_pattern P = K->pattern;
+    cudaStream_t s = ctx->stream;
+    const int n = W.n;
+    const unsigned gs = W.gs, gr = W.gr;
+    double *x = W.wx.p;
+    const double *b = W.wb.p;
+    k_mixed_flush<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(x, W.d32.p, n, W.st32.p);
+    switch (shape_tpr(W.shape)) {
+    case 2: k_mixed_spmv64<2><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+    case 4: k_mixed_spmv64<4><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+    case 8: k_mixed_spmv64<8><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+    case 16: k_mixed_spmv64<16><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+    default: k_mixed_spmv64<32><<<gs, RED_BLOCK, 0, counted(s)>>>(P->indptr.p, P->indices.p, K->data.p, x, W.Ax64.p, n, W.st32.p); break;
+    }
+    k_mixed_residual<<<gr, RED_BLOCK, 0, counted(s)>>>(b, W.Ax64.p, W.r32.p, K->inv32.p, n, W.part64.p, W.part32.p, W.st32.p);
+    k_cg_direction<float, true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.p32.p, W.r32.p, K->inv32.p, n, W.st32.p);
 }
 
 // Mixed precision solve: inner FP32 Jacobi-PCG with reliable FP64 updates, on the workspace.
@@ -771,22 +796,32 @@ static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b_in, double *x_
     // FP32 state seeded from the FP64 start
     CGState<float> &s32 = *W.st32_host;
     s32 = CGState<float>{};
-    s32.rz = (float)s64.rz;
+    s32.rz = s64.rz;
     s32.nb = s64.nb;
     s32.tol_nb = s64.tol_nb;
     s32.rn = s64.rn;
     s32.maxr = s64.rn;
+    s32.prt = s64.rn;
     s32.max_iter = max_iter;
     FEMD_TRY_CUDA(cudaMemcpyAsync(W.st32.p, W.st32_host, sizeof(CGState<float>), cudaMemcpyHostToDevice, s));
-    const long long max_chunks = (long long)max_iter / W.chm + 2;
+    // every chunk either advances the recurrence or (paused) does nothing; a reliable update
+    // is run between chunks when the state asks for one (about once per decade of residual)
+    const long long max_polls = 2 * ((long long)max_iter / W.chm + 2) + 64;
     int status = FEMD_OK;
     cudaError_t ce = cudaSuccess;
-    for (long long c = 0; c < max_chunks; ++c) {
+    for (long long c = 0; c < max_polls; ++c) {
         ce = launch_graph(W.xm, W.nodesm, s);
         if (ce == cudaSuccess) ce = cudaMemcpyAsync(W.st32_host, W.st32.p, sizeof(CGState<float>), cudaMemcpyDeviceToHost, s);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
         if (ce != cudaSuccess) { set_error(std::string("pcg_mixed: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; break; }
         if (W.st32_host->done) break;
+        if (W.st32_host->want_ru) {
+            mixed_ru(ctx, K, W);
+            ce = cudaMemcpyAsync(W.st32_host, W.st32.p, sizeof(CGState<float>), cudaMemcpyDeviceToHost, s);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+            if (ce != cudaSuccess) { set_error(std::string("pcg_mixed: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; break; }
+            if (W.st32_host->done) break;
+        }
     }
     // final true residual in FP64 (cg.hpp:222-237)
     if (status == FEMD_OK) {
@@ -812,6 +847,17 @@ static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b_in, double *x_
         float ms = 0.f;
         cudaEventElapsedTime(&ms, W.e0, W.e1);
         res->seconds = ms * 1e-3;
+        if (sh.fallback && sh.it < max_iter) {
+            // the FP32 recurrence stagnated: FP64 Jacobi-PCG from the current iterate (x_out),
+            // with the rest of the iteration budget; the result counts both phases
+            femd_cg_result r64{};
+            FEMD_TRY(cg_run(ctx, K, true, b_in, x_out, max_iter - sh.it, tol, &r64));
+            res->iterations = sh.it + r64.iterations;
+            res->residual = r64.residual;
+            res->breakdown = r64.breakdown;
+            res->converged = r64.converged;
+            res->seconds += r64.seconds;
+        }
     }
     return status;
 }
