@@ -455,9 +455,12 @@ unsigned red_grid(femd_ctx ctx, int n)
 int pick_tpr(femd_matrix K)
 {
     if (K->spmv_tpr) return K->spmv_tpr;
+    // 4 loads in flight per lane and the fewest lanes (a power of 2) that cover the mean row in
+    // one round: 2 lanes for P1, 4 for P2 and P3 (what the autotuner picks at those sizes)
     const double avg = K->pattern->nrows ? (double)K->pattern->nnz / K->pattern->nrows : 1.0;
-    const int tpr = avg <= 6 ? 4 : avg <= 14 ? 8 : avg <= 28 ? 16 : 32;
-    return tpr | (2 << 8);
+    int tpr = 2;
+    while (tpr * 4 < avg && tpr < 32) tpr <<= 1;
+    return tpr | (4 << 8);
 }
 
 // shape = threads per row (low byte) | loads in flight per lane (next byte)

@@ -180,10 +180,12 @@ class Server:
     updates (True) or FP64 Jacobi-PCG; iters: iterations per member per launch.  Admission: the
     device's free memory (free_memory(), default cudaMemGetInfo through torch) less
     reserve_bytes, and, when hbm_budget is given, that budget less what the requests in flight
-    hold."""
+    hold.  big_nnz: requests whose matrix has at least that many nonzeros are solved one at a time
+    on the whole GPU (femd_b200.cg_solve, the same precision) between batch launches -- a large
+    system streams HBM better with every block on it than as one team among many."""
 
     def __init__(self, lib, sessions=(), *, mixed=True, iters=64, tol=1e-10, reserve_bytes=2 << 30, free_memory=None,
-                 hbm_budget=None, max_members=1024, keep_solutions=False, shape=None):
+                 hbm_budget=None, max_members=1024, keep_solutions=False, shape=None, big_nnz=None):
         torch = _torch()
         self.lib, self.sessions = lib, list(sessions)
         self.mixed, self.iters, self.tol = bool(mixed), int(iters), float(tol)
@@ -192,14 +194,19 @@ class Server:
         self.hbm_budget = hbm_budget
         self.max_members = int(max_members)
         self.keep = keep_solutions
+        self.big_nnz = big_nnz
         self.batch = Batch()
         if shape:
             self.batch.configure(*shape)
         for S in self.sessions:
-            S.member = self.batch.add(S.A)
+            S.member = None if self._big(S.A.nnz) else self.batch.add(S.A)
         self.launches = 0
         self.active = {}
+        self.direct = collections.deque()           # admitted requests for the whole-GPU path
         self.last_launch_s = 0.0
+
+    def _big(self, nnz):
+        return self.big_nnz is not None and nnz >= self.big_nnz
 
     def _admit(self, r, budget):
         """Set the request up and arm it; the bytes it takes, or None when it has to wait."""
@@ -214,16 +221,43 @@ class Server:
             S.busy = True
             b = S.M.matvec(S.u)
             x = S.u.clone()
-            self.batch.arm(S.member, b, x, tol=self.tol)
-            self.active[S.member] = (r, S, None, b, x, need)
+            if S.member is None:
+                self.direct.append((r, S, S.A, b, x, need))
+            else:
+                self.batch.arm(S.member, b, x, tol=self.tol)
+                self.active[S.member] = (r, S, None, b, x, need)
         else:
             K = stiffness(self.lib, r.N, r.k, r.c)
             b = _rhs(r, K.nrows)
             x = torch.zeros(K.nrows, dtype=torch.float64, device=b.device)
-            mid = self.batch.add(K)
-            self.batch.arm(mid, b, x, tol=self.tol)
-            self.active[mid] = (r, None, K, b, x, need)
+            if self._big(K.nnz):
+                self.direct.append((r, None, K, b, x, need))
+            else:
+                mid = self.batch.add(K)
+                self.batch.arm(mid, b, x, tol=self.tol)
+                self.active[mid] = (r, None, K, b, x, need)
         return need
+
+    def _finish(self, r, S, x, res, t_done):
+        r.t_done = t_done
+        r.iterations, r.converged = res["iterations"], res["converged"]
+        r.residual, r.status, r.outer = res["residual"], res["status"], res["reliable_updates"]
+        if self.keep:
+            r.x = x
+        if r.out is not None:
+            r.out.copy_(x, non_blocking=True)
+        if S is not None:
+            S.u = x
+            S.busy = False
+
+    def _solve_direct(self, t0):
+        """One request of the whole-GPU path."""
+        r, S, K, b, x, _ = self.direct.popleft()
+        x, conv, its, res, brk = fb.cg_solve(K, fb.JacobiPreconditioner(K), b, x, max(1000, 10 * K.nrows), self.tol,
+                                             mixed=self.mixed)
+        last = fb.cg_solve.last
+        self._finish(r, S, x, dict(iterations=its, converged=conv, residual=res, status=0,
+                                   reliable_updates=int(last.outer)), time.perf_counter() - t0)
 
     def run(self, trace, *, realtime=True, max_seconds=600.0):
         """Serve the trace (arrivals in real time from now, or all at once); returns the summary
@@ -237,17 +271,19 @@ class Server:
         pending = collections.deque(sorted(trace, key=lambda r: r.t))
         queue = []
         self.active = {}
+        self.direct.clear()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: math.inf)
-        while pending or queue or self.active:
+        while pending or queue or self.active or self.direct:
             now = clock()
             while pending and pending[0].t <= now:
                 queue.append(pending.popleft())
             if queue:
                 budget = self.free_memory() - self.reserve
                 if self.hbm_budget is not None:
-                    budget = min(budget, self.hbm_budget - sum(a[5] for a in self.active.values()))
+                    held = sum(a[5] for a in self.active.values()) + sum(a[5] for a in self.direct)
+                    budget = min(budget, self.hbm_budget - held)
                 keep = []
                 for i, r in enumerate(queue):
                     if len(self.active) >= self.max_members or len(keep) >= 256:
@@ -266,22 +302,15 @@ class Server:
                 t_done = time.perf_counter() - t0
                 for mid, res in fin:
                     r, S, K, b, x, _ = self.active.pop(mid)
-                    r.t_done = t_done
-                    r.iterations, r.converged = res["iterations"], res["converged"]
-                    r.residual, r.status, r.outer = res["residual"], res["status"], res["reliable_updates"]
                     self.last_launch_s = res["seconds"]
-                    if self.keep:
-                        r.x = x
-                    if r.out is not None:
-                        r.out.copy_(x, non_blocking=True)
-                    if S is not None:
-                        S.u = x
-                        S.busy = False
-                    else:
+                    self._finish(r, S, x, res, t_done)
+                    if S is None:
                         self.batch.remove(mid)
                 if self.batch.last_status != 0:
                     raise RuntimeError(f"serve: batch launch failed with status {self.batch.last_status}")
-            elif pending:
+            if self.direct:
+                self._solve_direct(t0)
+            elif not self.active and pending:
                 wait = pending[0].t - clock()
                 if wait > 2e-3:
                     time.sleep(wait - 1e-3)
