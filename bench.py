@@ -388,21 +388,11 @@ def c4_rhs(spec):
 
 
 def batch_bytes(reqs, lib, mixed=True):
-    """Algorithmic HBM bytes of one batched launch: per member and iteration the SpMV's matrix
-    (8 B / nonzero in FP32: value + column index; 12 in FP64) and vectors (gathers of z and the
-    previous direction, stores of the direction and A p; the update's loads of r, A p, inv, x or
-    d, p and stores of r, z, x or d: 12 accesses of 4 or 8 B per row), plus per reliable update and
-    at the start an FP64 residual (12 B / nonzero, b, x, inv, r, z: 40 B / row) and, in mixed mode,
-    the FP32 copy of the matrix (12 B / nonzero)."""
-    tot = 0
-    for r in reqs:
-        sp = lib.get(r.N, r.k)
-        n, nnz = sp["n"], sp["nnz"]
-        if mixed:
-            tot += r.iterations * (8 * nnz + 48 * n) + (r.outer + 1) * (12 * nnz + 40 * n) + 12 * nnz
-        else:
-            tot += r.iterations * (12 * nnz + 96 * n) + 2 * (12 * nnz + 40 * n)
-    return tot
+    """Algorithmic HBM bytes of the batched launch that served these requests
+    (femd_b200.workloads.batch_bytes)."""
+    from femd_b200.workloads import batch_bytes as bb
+    sizes = [(lib.get(r.N, r.k)["n"], lib.get(r.N, r.k)["nnz"]) for r in reqs]
+    return bb(sizes, [dict(iterations=r.iterations, reliable_updates=r.outer) for r in reqs], mixed)
 
 
 def ours_c4(args, rank, world, dist):
