@@ -309,11 +309,8 @@ def ours_c2(args, rank, world, dist):
 
 
 def _max_over_ranks(torch, dist, t):
-    if dist is None:
-        return t
-    v = torch.tensor([t], dtype=torch.float64, device="cuda")
-    dist.all_reduce(v, op=dist.ReduceOp.MAX)
-    return float(v.item())
+    from femd_b200.replicas import max_over_ranks
+    return max_over_ranks(t, dist, "cuda")
 
 
 def cpu_baseline(gpu_its):
@@ -622,19 +619,16 @@ def main():
         return
     dist = None
     if world > 1:
-        import datetime
-
         import torch
-        import torch.distributed as D
+        from femd_b200 import replicas
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        dist = D
+        dist = replicas.init("nccl", 120.0)
     line = (ours_c4 if args.workload == "c4s" else ours_c2)(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+        from femd_b200 import replicas
+        replicas.finish(dist)
 
 
 if __name__ == "__main__":
