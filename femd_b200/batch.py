@@ -61,6 +61,10 @@ class Batch:
         """Set the launch shape (femd_cuda_batch_configure)."""
         check(lib.femd_cuda_batch_configure(self.h, int(block), int(nnz_per_block), int(nnz_per_thread)))
 
+    def configure_lockstep(self, nnz_per_entry=0, chunk=0):
+        """Shape of the lockstep engine (femd_cuda_batch_lockstep_configure; 0 keeps a value)."""
+        check(lib.femd_cuda_batch_lockstep_configure(self.h, int(nnz_per_entry), int(chunk)))
+
     def params(self):
         b, n, t, g = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         check(lib.femd_cuda_batch_params(self.h, C.byref(b), C.byref(n), C.byref(t), C.byref(g)))
@@ -95,14 +99,19 @@ class Batch:
         check(st)
         return self.params(), sec.value
 
-    def solve(self, bs, xs=None, *, tol=1e-10, max_iter=0, mixed=True):
-        """Solve every member (in id order) to completion in one launch.  bs: right-hand sides;
-        xs: initial guesses (default 0), overwritten.  Returns (xs, results) with one dict per
-        member (converged, iterations, residual, breakdown, status, reliable_updates, seconds)."""
+    def solve(self, bs, xs=None, *, tol=1e-10, max_iter=0, mixed=True, engine="persistent"):
+        """Solve every member (in id order) to completion.  bs: right-hand sides; xs: initial
+        guesses (default 0), overwritten.  engine "persistent": one cooperative launch (teams of
+        blocks per member); "lockstep": a few whole-GPU kernels per iteration over all the members
+        still running.  Returns (xs, results) with one dict per member (converged, iterations,
+        residual, breakdown, status, reliable_updates, seconds)."""
+        if engine not in ("persistent", "lockstep"):
+            raise ValueError(f"batch: unknown engine {engine!r}")
         bs, xs, bp, xp = self._vectors(bs, xs)
         res = (N.femd_cg_result * len(bs))()
+        fn = lib.femd_cuda_batch_solve if engine == "persistent" else lib.femd_cuda_batch_solve_lockstep
         self.ctx.enter()
-        st = lib.femd_cuda_batch_solve(self.ctx.h, self.h, bp, xp, int(max_iter), float(tol), int(bool(mixed)), res)
+        st = fn(self.ctx.h, self.h, bp, xp, int(max_iter), float(tol), int(bool(mixed)), res)
         self.ctx.leave()
         self.last_status = st
         if st not in (N.FEMD_OK, N.FEMD_ETIMEOUT, N.FEMD_EABORT):

@@ -60,6 +60,7 @@ struct BState {
 
 struct BProb {
     int n, team, max_iter, nch, nnz;
+    int tpr;               // lockstep engine: lanes per row of its SpMV
     double tol;
     const int *indptr, *indices;
     const int *crow, *cq;  // chunk c = rows [crow[c], crow[c+1]) = nonzeros [cq[c], cq[c+1])
@@ -803,6 +804,359 @@ static BatchKernel batch_kernel(bool mixed, int block, int npt)
     return mixed ? batch_kernel_m<true>(block, npt) : batch_kernel_m<false>(block, npt);
 }
 
+
+// ==== the lockstep engine ====================================================================
+// Every iteration is a few whole-grid kernels over all the members still running: an SpMV
+// (direction formed on the fly, p.Ap) and the update; in mixed precision also a flush and an
+// FP64 residual over the members that asked for a reliable update in this iteration.  An entry
+// of the block table is a fixed range of one member's rows (warp row groups, TPR lanes per row,
+// 4 loads in flight per lane, no block barriers in the row loop).  A member's sums are entry
+// partials summed in entry order by the member's last block (a ticket per member and kernel), so
+// a member's iterates depend on the member alone, whatever else is in the batch.
+
+struct LState {
+    double rz, alpha, beta, nb, maxr, rz_prev, rn_rec, prt, res;
+    int it, done, want_ru, breakdown, conv, rus, stall, fallback, zero, started;
+    unsigned t1, t2, t3;   // last-block tickets of the SpMV, the update and the residual
+    int pad;
+};
+
+struct LBlock {
+    int m, r0, r1, b0, b1;  // member, its rows [r0, r1), the member's entries [b0, b1)
+};
+
+static constexpr int LS_BB = 256;
+
+// y = A g on rows [r0, r1) with TPR lanes per row; out(row, sum) by the row's first lane
+template <int TPR, class V, class F, class Gather, class Out>
+__device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int r1, Gather g, Out out)
+{
+    constexpr int U = 4, GPW = 32 / TPR;
+    const int lane = threadIdx.x % TPR;
+    for (int i0 = r0 + (int)(threadIdx.x >> 5) * GPW; i0 < r1; i0 += (LS_BB / 32) * GPW) {
+        const int i = i0 + (int)(threadIdx.x & 31) / TPR;
+        F s = F(0);
+        if (i < r1) {
+            const int lo = P.indptr[i], hi = P.indptr[i + 1];
+            for (int base = lo + lane; base < hi; base += U * TPR) {
+                int c[U];
+                V v[U];
+                F xv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int q = base + u * TPR;
+                    c[u] = q < hi ? __ldcs(&P.indices[q]) : 0;
+                    v[u] = q < hi ? __ldcs(&A[q]) : V(0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) xv[u] = base + u * TPR < hi ? g(c[u]) : F(0);
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (base + u * TPR < hi) s += (F)v[u] * xv[u];
+            }
+        }
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
+        if (lane == 0 && i < r1) out(i, s);
+    }
+}
+
+template <class V, class F, class Gather, class Out>
+__device__ __forceinline__ void ls_rows_any(const BProb &P, const V *A, int r0, int r1, Gather g, Out out)
+{
+    switch (P.tpr) {
+    case 2: ls_rows<2, V, F>(P, A, r0, r1, g, out); break;
+    case 4: ls_rows<4, V, F>(P, A, r0, r1, g, out); break;
+    case 8: ls_rows<8, V, F>(P, A, r0, r1, g, out); break;
+    case 16: ls_rows<16, V, F>(P, A, r0, r1, g, out); break;
+    default: ls_rows<32, V, F>(P, A, r0, r1, g, out); break;
+    }
+}
+
+// The member's totals of NV sums.  The block's sums go to part[k * NE + e]; in the member's last
+// block the function returns true (in every thread) with tot = the member's entry partials
+// summed in entry order, and resets the ticket.
+template <int NV>
+__device__ __forceinline__ bool ls_member_sum(const double (&v)[NV], double *part, int NE, int e, const LBlock &L,
+                                              unsigned *ticket, double (&tot)[NV])
+{
+    __shared__ double sh[NV][LS_BB / 32];
+    __shared__ int last;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const double t = warp_sum(v[k]);
+        if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < LS_BB / 32; ++w) t += sh[k][w];
+            part[(size_t)k * NE + e] = t;
+        }
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == (unsigned)(L.b1 - L.b0 - 1);
+    }
+    __syncthreads();
+    const bool is_last = last;
+    if (!is_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double t = 0.0;
+        for (int b = L.b0 + (int)threadIdx.x; b < L.b1; b += LS_BB) t += __ldcg(part + (size_t)k * NE + b);
+        t = warp_sum(t);
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = t;
+        __syncthreads();
+        double u = 0.0;
+#pragma unroll
+        for (int w = 0; w < LS_BB / 32; ++w) u += sh[k][w];
+        tot[k] = u;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *ticket = 0;
+    return true;
+}
+
+__device__ __forceinline__ void ls_finish(LState &S, int *active)
+{
+    S.done = 1;
+    atomicSub(active, 1);
+}
+
+// SpMV with the direction formed on the fly: p = z + beta pold (pold = 0 at the start); p.Ap.
+// Block 0 also empties the reliable-update list of the iteration.
+template <bool MIXED>
+__global__ void __launch_bounds__(LS_BB) k_ls_spmv(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
+                                                   LState *st, double *part, int *active, int *ru_count)
+{
+    using F = typename std::conditional<MIXED, float, double>::type;
+    if (MIXED && blockIdx.x == 0 && threadIdx.x == 0) *ru_count = 0;
+    const int e = blockIdx.x;
+    const LBlock L = blks[e];
+    const BProb P = probs[L.m];
+    LState &S = st[L.m];
+    if (S.done) return;
+    const F *z = MIXED ? (const F *)P.z32 : (const F *)P.z64;
+    F *pa = MIXED ? (F *)P.pa32 : (F *)P.pa64;
+    F *pb = MIXED ? (F *)P.pb32 : (F *)P.pb64;
+    F *Ap = MIXED ? (F *)P.Ap32 : (F *)P.Ap64;
+    const F *A = MIXED ? (const F *)P.A32 : (const F *)P.A64;
+    const int it = S.it;
+    const F beta = (F)S.beta;
+    const F *pold = (it & 1) ? pa : pb;
+    F *pnew = (it & 1) ? pb : pa;
+    double dot = 0.0;
+    ls_rows_any<F, F>(
+        P, A, L.r0, L.r1, [&](int j) { return pdir(z, pold, beta, j); },
+        [&](int i, F s) {
+            const F pi = pdir(z, pold, beta, i);
+            pnew[i] = pi;
+            Ap[i] = s;
+            dot += (double)pi * (double)s;
+        });
+    const double v[1] = {dot};
+    double tot[1];
+    if (ls_member_sum<1>(v, part, NE, e, L, &S.t1, tot) && threadIdx.x == 0) {
+        if (!(tot[0] > 0.0)) {
+            S.breakdown = 1;
+            ls_finish(S, active);
+        } else {
+            S.alpha = S.rz / tot[0];
+        }
+    }
+}
+
+// r -= alpha Ap, (x or d) += alpha p, z = inv r; ||r||^2 and r.z; then the member's stopping
+// test.  In mixed precision a member that wants a reliable update puts its entries on the list.
+template <bool MIXED>
+__global__ void __launch_bounds__(LS_BB) k_ls_update(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
+                                                     LState *st, double *part, int *active, int *ru_list, int *ru_count)
+{
+    using F = typename std::conditional<MIXED, float, double>::type;
+    __shared__ int s_ru;
+    const int e = blockIdx.x;
+    const LBlock L = blks[e];
+    const BProb P = probs[L.m];
+    LState &S = st[L.m];
+    if (S.done) return;
+    F *r = MIXED ? (F *)P.r32 : (F *)P.r64;
+    F *z = MIXED ? (F *)P.z32 : (F *)P.z64;
+    const int it = S.it;
+    const F *p = (it & 1) ? (MIXED ? (const F *)P.pb32 : (const F *)P.pb64) : (MIXED ? (const F *)P.pa32 : (const F *)P.pa64);
+    const F *Ap = MIXED ? (const F *)P.Ap32 : (const F *)P.Ap64;
+    const F *inv = MIXED ? (const F *)P.inv32 : (const F *)P.inv64;
+    F *acc = MIXED ? (F *)P.d32 : (F *)P.x;
+    const F alpha = (F)S.alpha;
+    double v[2] = {0.0, 0.0};
+    for (int i = L.r0 + (int)threadIdx.x; i < L.r1; i += LS_BB) {
+        const F ri = r[i] - alpha * Ap[i];
+        const F zi = inv[i] * ri;
+        r[i] = ri;
+        z[i] = zi;
+        acc[i] = acc[i] + alpha * p[i];
+        v[0] += (double)ri * (double)ri;
+        v[1] += (double)ri * (double)zi;
+    }
+    double tot[2];
+    if (!ls_member_sum<2>(v, part, NE, e, L, &S.t2, tot)) return;
+    if (threadIdx.x == 0) {
+        s_ru = 0;
+        const int it1 = it + 1;
+        S.it = it1;
+        const double rn = sqrt(tot[0]), rzn = tot[1];
+        if (!MIXED) {
+            S.res = rn / S.nb;
+            if (rn <= P.tol * S.nb || it1 >= P.max_iter) {
+                ls_finish(S, active);
+            } else {
+                S.beta = rzn / S.rz;
+                S.rz = rzn;
+                if (!(rzn > 0.0)) { S.breakdown = 1; ls_finish(S, active); }
+            }
+        } else if (rn <= 0.1 * S.maxr || rn <= P.tol * S.nb || it1 >= P.max_iter || !(rzn > 0.0)) {
+            S.want_ru = 1;
+            S.rz_prev = S.rz;
+            S.rn_rec = rn;
+            s_ru = atomicAdd(ru_count, L.b1 - L.b0) + 1;
+        } else {
+            S.beta = rzn / S.rz;
+            S.rz = rzn;
+        }
+    }
+    __syncthreads();
+    if (MIXED && s_ru)
+        for (int k = (int)threadIdx.x; k < L.b1 - L.b0; k += LS_BB) ru_list[s_ru - 1 + k] = L.b0 + k;
+}
+
+// the reliable update's first half, x += d and d = 0: on the listed entries (ALL false) or on
+// every entry of a member that broke down (ALL true)
+template <bool ALL>
+__global__ void __launch_bounds__(LS_BB) k_ls_flush(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
+                                                    const LState *__restrict__ st, const int *ru_list, const int *ru_count)
+{
+    const int cnt = ALL ? NE : *ru_count;
+    for (int w = blockIdx.x; w < cnt; w += gridDim.x) {
+        const LBlock L = blks[ALL ? w : ru_list[w]];
+        const BProb P = probs[L.m];
+        if (ALL && !st[L.m].breakdown) continue;
+        for (int i = L.r0 + (int)threadIdx.x; i < L.r1; i += LS_BB) {
+            P.x[i] += (double)P.d32[i];
+            P.d32[i] = 0.0f;
+        }
+    }
+}
+
+// The FP64 residual r = b - A64 x (stored as FP32 in mixed precision), z = inv r, and the
+// member's decisions.  MODE 0: the start (also ||b||, pold = 0, d = 0), every entry; MODE 1: a
+// reliable update (mixed), the listed entries; MODE 2: the final true residual, every entry.
+template <bool MIXED, int MODE>
+__global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
+                                                    LState *st, double *part, int *active, const int *ru_list,
+                                                    const int *ru_count)
+{
+    using F = typename std::conditional<MIXED, float, double>::type;
+    const int cnt = MODE == 1 ? *ru_count : NE;
+    for (int w = blockIdx.x; w < cnt; w += gridDim.x) {
+        const int e = MODE == 1 ? ru_list[w] : w;
+        const LBlock L = blks[e];
+        const BProb P = probs[L.m];
+        LState &S = st[L.m];
+        if (MODE == 0 && S.started) continue;
+        if (MODE == 2 && S.zero) continue;
+        F *pb = MIXED ? (F *)P.pb32 : (F *)P.pb64;
+        const double *x = P.x;
+        double v[3] = {0.0, 0.0, 0.0};
+        ls_rows_any<double, double>(
+            P, P.A64, L.r0, L.r1, [&](int j) { return x[j]; },
+            [&](int i, double s) {
+                const double bi = P.b[i], ri = bi - s;
+                v[0] += ri * ri;
+                if (MODE != 2) {
+                    if (MIXED) {
+                        const float rf = (float)ri, zf = (float)P.inv64[i] * rf;
+                        P.r32[i] = rf;
+                        P.z32[i] = zf;
+                        v[1] += (double)rf * (double)zf;
+                    } else {
+                        const double zi = P.inv64[i] * ri;
+                        P.r64[i] = ri;
+                        P.z64[i] = zi;
+                        v[1] += ri * zi;
+                    }
+                }
+                if (MODE == 0) {
+                    v[2] += bi * bi;
+                    pb[i] = F(0);
+                    if (MIXED) P.d32[i] = 0.0f;
+                }
+            });
+        double tot[3];
+        if (!ls_member_sum<3>(v, part, NE, e, L, &S.t3, tot) || threadIdx.x != 0) continue;
+        const double rn = sqrt(tot[0]);
+        if (MODE == 0) {
+            const double nb = sqrt(tot[2]);
+            S.started = 1;
+            S.nb = nb;
+            S.rz = tot[1];
+            S.maxr = rn;
+            S.prt = rn;
+            S.beta = 0.0;
+            S.res = nb == 0.0 ? 0.0 : rn / nb;
+            if (nb == 0.0) {
+                S.zero = 1;
+                S.conv = 1;
+                ls_finish(S, active);
+            } else if (rn <= P.tol * nb) {
+                S.conv = 1;
+                ls_finish(S, active);
+            } else if (!(S.rz > 0.0)) {
+                S.breakdown = 1;
+                ls_finish(S, active);
+            }
+        } else if (MODE == 1) {
+            S.want_ru = 0;
+            S.rus += 1;
+            S.res = rn / S.nb;
+            S.maxr = rn;
+            if (rn <= P.tol * S.nb || S.it >= P.max_iter) {
+                ls_finish(S, active);
+                continue;
+            }
+            // stagnation of the FP32 recurrence: the host goes on in FP64 from this iterate
+            S.stall = rn > 0.5 * S.prt ? S.stall + 1 : 0;
+            S.prt = rn;
+            if (S.stall >= 2 || !(rn < 1e300)) {
+                S.fallback = 1;
+                ls_finish(S, active);
+                continue;
+            }
+            if (!(tot[1] > 0.0)) {
+                S.breakdown = 1;
+                ls_finish(S, active);
+                continue;
+            }
+            // drifted recurrence (true residual over twice its own): restart the direction
+            S.beta = rn > 2.0 * S.rn_rec ? 0.0 : tot[1] / S.rz_prev;
+            S.rz = tot[1];
+        } else {
+            S.res = rn / S.nb;
+        }
+    }
+}
+
+// x = 0 for the members with b = 0
+__global__ void __launch_bounds__(LS_BB) k_ls_zero(const BProb *__restrict__ probs, const LBlock *__restrict__ blks,
+                                                   const LState *__restrict__ st)
+{
+    const LBlock L = blks[blockIdx.x];
+    if (!st[L.m].zero) return;
+    for (int i = L.r0 + (int)threadIdx.x; i < L.r1; i += LS_BB) probs[L.m].x[i] = 0.0;
+}
+
 }  // namespace femd
 
 using namespace femd;
@@ -857,6 +1211,8 @@ struct femd_batch_s : femd::HandleBase {
     int ghost = -1;                             // test hook: this member waits for a rank that never comes
     long long spin_limit = SPIN_LIMIT;
     int *abort_host = nullptr;                  // mapped pinned flag
+    // the lockstep engine: nonzeros per table entry, iterations enqueued between state reads
+    int ls_nnz = 16384, ls_chunk = 8;
     int *abort_dev = nullptr;
     femd_batch_s() : HandleBase(femd::KIND_BATCH) {}
     void drop_graphs()
@@ -1320,6 +1676,243 @@ static int arm_member(femd_batch_s *B, int id, const double *b, double *x, int m
     return FEMD_OK;
 }
 
+// ---- the lockstep engine: host side ----------------------------------------------------------
+
+// lanes per row of a member's SpMV: the fewest (a power of two, at least 2) whose 4 loads in
+// flight each cover the mean row
+static int ls_tpr(const Member &M)
+{
+    const double avg = (double)M.nnz / (double)M.n;
+    int tpr = 2;
+    while (tpr * 4 < avg && tpr < 32) tpr <<= 1;
+    return tpr;
+}
+
+// rows of one table entry of a member: about nnz_per_entry nonzeros
+static int ls_rows_per_entry(const femd_batch_s *B, const Member &M)
+{
+    const long long r = (long long)B->ls_nnz * M.n / std::max(1LL, M.nnz);
+    return (int)std::max(32LL, std::min((long long)M.n, r));
+}
+
+namespace {
+struct PinnedBuf {
+    void *p = nullptr;
+    ~PinnedBuf()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+}  // namespace
+
+// One lockstep solve of the members `ids` (armed, one precision).  The final states go to out.
+static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bool mx, std::vector<LState> &out, double *seconds)
+{
+    cudaStream_t s = ctx->stream;
+    int st;
+    const int nm = (int)ids.size();
+    *seconds = 0.0;
+    out.assign(nm, LState{});
+    if (nm == 0) return FEMD_OK;
+    for (int id : ids)
+        if ((st = member_vectors(B, *B->mem[id], mx))) return st;
+    std::vector<BProb> desc(nm);
+    std::vector<int> rows(nm), nent(nm);
+    int NEfull = 0, max_it = 1;
+    for (int k = 0; k < nm; ++k) {
+        Member &M = *B->mem[ids[k]];
+        desc[k] = describe(B, ids[k], mx);
+        desc[k].tpr = ls_tpr(M);
+        rows[k] = ls_rows_per_entry(B, M);
+        nent[k] = (M.n + rows[k] - 1) / rows[k];
+        FEMD_CHECK_ARG((long long)NEfull + nent[k] < INT_MAX / 4, "batch: too many table entries");
+        NEfull += nent[k];
+        max_it = std::max(max_it, M.max_iter);
+        if (mx && M.need_f32) {
+            k_batch_f32<<<grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count), 256, 0, counted(s)>>>(
+                M.K->data.p, desc[k].A32, M.nnz, M.K->inv.p, desc[k].inv32, M.n);
+            FEMD_TRY_CUDA(cudaGetLastError());
+            M.need_f32 = false;
+        }
+    }
+    DevBuf<BProb> d_desc;
+    DevBuf<LState> d_state;
+    DevBuf<LBlock> d_tab;
+    DevBuf<double> d_part;
+    DevBuf<int> d_int;                                  // active, ru_count, ru_list (NEfull)
+    if ((st = d_desc.alloc(nm)) || (st = d_state.alloc(nm)) || (st = d_tab.alloc(NEfull)) || (st = d_part.alloc(3 * (size_t)NEfull)) ||
+        (st = d_int.alloc(2 + (size_t)NEfull)))
+        return st;
+    // pinned staging: two tables, two state copies, the descriptors
+    PinnedBuf pin;
+    const size_t tab_b = (size_t)NEfull * sizeof(LBlock), st_b = (size_t)nm * sizeof(LState);
+    FEMD_TRY_CUDA(cudaHostAlloc(&pin.p, 2 * tab_b + 2 * st_b + nm * sizeof(BProb) + 64, cudaHostAllocDefault));
+    LBlock *h_tab[2] = {static_cast<LBlock *>(pin.p), static_cast<LBlock *>(pin.p) + NEfull};
+    LState *h_st[2] = {reinterpret_cast<LState *>(h_tab[1] + NEfull), nullptr};
+    h_st[1] = h_st[0] + nm;
+    BProb *h_desc = reinterpret_cast<BProb *>(h_st[1] + nm);
+    std::copy(desc.begin(), desc.end(), h_desc);
+    // the table of the live members (all of them when live is null)
+    auto build = [&](LBlock *T, const LState *live) {
+        int e = 0;
+        for (int k = 0; k < nm; ++k) {
+            if (live && live[k].done) continue;
+            const int b0 = e;
+            for (int j = 0; j < nent[k]; ++j) {
+                T[e] = LBlock{k, j * rows[k], std::min(desc[k].n, (j + 1) * rows[k]), b0, b0 + nent[k]};
+                ++e;
+            }
+        }
+        return e;
+    };
+    const int G1 = std::max(1, 8 * ctx->sm_count);     // grid of the reliable-update kernels
+    int *active = d_int.p, *ru_count = d_int.p + 1, *ru_list = d_int.p + 2;
+    int NE = build(h_tab[0], nullptr);
+    int tb = 0;                                         // the host table buffer last uploaded
+    cudaEvent_t ev[2] = {nullptr, nullptr}, t0 = nullptr, t1 = nullptr;
+    struct EvGuard {
+        cudaEvent_t *e;
+        int n;
+        ~EvGuard()
+        {
+            for (int i = 0; i < n; ++i)
+                if (e[i]) cudaEventDestroy(e[i]);
+        }
+    };
+    cudaEvent_t evs[4] = {nullptr, nullptr, nullptr, nullptr};
+    EvGuard guard{evs, 4};
+    for (int i = 0; i < 4; ++i) FEMD_TRY_CUDA(cudaEventCreateWithFlags(&evs[i], i < 2 ? cudaEventDisableTiming : cudaEventDefault));
+    ev[0] = evs[0];
+    ev[1] = evs[1];
+    t0 = evs[2];
+    t1 = evs[3];
+    *(volatile int *)B->abort_host = 0;
+    FEMD_TRY_CUDA(cudaEventRecord(t0, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(d_desc.p, h_desc, nm * sizeof(BProb), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(d_tab.p, h_tab[0], NE * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaMemsetAsync(d_state.p, 0, st_b, s));
+    FEMD_TRY_CUDA(cudaMemsetAsync(d_int.p, 0, 2 * sizeof(int), s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(active, &nm, sizeof(int), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));           // &nm is a host stack value
+    if (mx)
+        k_ls_resid<true, 0><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
+    else
+        k_ls_resid<false, 0><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    const int C = std::max(1, B->ls_chunk);
+    const long long max_chunks = (long long)max_it / C + 4;
+    int aborted = 0;
+    for (long long j = 0; j <= max_chunks; ++j) {
+        for (int c = 0; c < C; ++c) {
+            if (mx) {
+                k_ls_spmv<true><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count);
+                k_ls_update<true><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
+                k_ls_flush<false><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, ru_list, ru_count);
+                k_ls_resid<true, 1><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active,
+                                                                                 ru_list, ru_count);
+            } else {
+                k_ls_spmv<false><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count);
+                k_ls_update<false><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list,
+                                                                   ru_count);
+            }
+        }
+        FEMD_TRY_CUDA(cudaGetLastError());
+        FEMD_TRY_CUDA(cudaMemcpyAsync(h_st[j & 1], d_state.p, st_b, cudaMemcpyDeviceToHost, s));
+        FEMD_TRY_CUDA(cudaEventRecord(ev[j & 1], s));
+        if (j == 0) continue;
+        // the states after the previous chunk (one chunk stays queued behind them)
+        FEMD_TRY_CUDA(cudaEventSynchronize(ev[(j - 1) & 1]));
+        const LState *S = h_st[(j - 1) & 1];
+        int live = 0, live_e = 0;
+        for (int k = 0; k < nm; ++k)
+            if (!S[k].done) { ++live; live_e += nent[k]; }
+        if (live == 0) break;
+        if (*(volatile int *)B->abort_host) { aborted = 1; break; }
+        if (live_e <= (NE * 7) / 10) {
+            // compact the table to the live members (their entries keep their order)
+            tb ^= 1;
+            NE = build(h_tab[tb], S);
+            FEMD_TRY_CUDA(cudaMemcpyAsync(d_tab.p, h_tab[tb], NE * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+        }
+    }
+    // the end: the final true residual (FP64) or the flush of the members that broke down (mixed),
+    // over the whole table; x = 0 for b = 0
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));           // no upload from a table buffer is pending
+    tb ^= 1;
+    NE = build(h_tab[tb], nullptr);
+    FEMD_TRY_CUDA(cudaMemcpyAsync(d_tab.p, h_tab[tb], NE * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+    if (!aborted) {
+        if (mx)
+            k_ls_flush<true><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, ru_list, ru_count);
+        else
+            k_ls_resid<false, 2><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list,
+                                                                ru_count);
+        k_ls_zero<<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, d_state.p);
+        FEMD_TRY_CUDA(cudaGetLastError());
+    }
+    FEMD_TRY_CUDA(cudaMemcpyAsync(h_st[0], d_state.p, st_b, cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaEventRecord(t1, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    *seconds = ms * 1e-3;
+    std::copy(h_st[0], h_st[0] + nm, out.begin());
+    if (aborted) { set_error("batch: aborted by the host"); return FEMD_EABORT; }
+    return FEMD_OK;
+}
+
+// a member's result from its lockstep state (the acceptance of the persistent engine)
+static void ls_result(const Member &M, const LState &S, femd_cg_result &r, double seconds)
+{
+    r.iterations = S.it + M.prior_its;
+    r.outer = S.rus + M.prior_rus;
+    r.residual = S.res;
+    r.breakdown = S.breakdown;
+    r.status = 0;
+    r.seconds = seconds;
+    int conv = S.conv;
+    if (!conv && !S.breakdown && S.done) {
+        conv = S.res <= M.tol * (1.0 + 1e-6) + 1e-15;
+        if (!conv && S.res <= 10.0 * M.tol && S.it < M.max_iter) conv = 1;
+    }
+    r.converged = conv;
+}
+
+// every member of the batch solved by the lockstep engine; in mixed precision the members whose
+// FP32 recurrence stagnated go on in an FP64 lockstep solve from their iterate
+static int ls_solve(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bool mx, femd_cg_result *results)
+{
+    std::vector<LState> S;
+    double sec = 0.0;
+    int st = ls_run(ctx, B, ids, mx, S, &sec);
+    if (st && st != FEMD_EABORT) return st;
+    std::vector<int> fb_ids, fb_pos;
+    for (size_t p = 0; p < ids.size(); ++p) {
+        Member &M = *B->mem[ids[p]];
+        if (st == FEMD_OK && mx && S[p].fallback) {
+            M.prior_its = S[p].it;
+            M.prior_rus = S[p].rus;
+            M.max_iter = std::max(1, M.max_iter - S[p].it);
+            fb_ids.push_back(ids[p]);
+            fb_pos.push_back((int)p);
+            continue;
+        }
+        ls_result(M, S[p], results[p], sec);
+        if (st) results[p].status = st;
+    }
+    if (fb_ids.empty()) return st;
+    std::vector<LState> S2;
+    double sec2 = 0.0;
+    const int st2 = ls_run(ctx, B, fb_ids, false, S2, &sec2);
+    if (st2 && st2 != FEMD_EABORT) return st2;
+    for (size_t q = 0; q < fb_ids.size(); ++q) {
+        ls_result(*B->mem[fb_ids[q]], S2[q], results[fb_pos[q]], sec + sec2);
+        if (st2) results[fb_pos[q]].status = st2;
+    }
+    for (size_t p = 0; p < ids.size(); ++p) results[p].seconds = sec + sec2;
+    return st2;
+}
+
 extern "C" {
 
 int femd_cuda_batch_create(femd_ctx ctx, int nprob, const femd_matrix *mats, int nnz_per_block, femd_batch *out)
@@ -1448,6 +2041,35 @@ int femd_cuda_batch_solve(femd_ctx ctx, femd_batch handle, const double *const *
         B->mem[ids[p]]->armed = false;
     }
     return st;
+}
+
+int femd_cuda_batch_solve_lockstep(femd_ctx ctx, femd_batch handle, const double *const *b_dev, double *const *x_dev,
+                                   int max_iter, double tol, int mixed, femd_cg_result *results)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(ctx && B && b_dev && x_dev && results && ctx == B->ctx, "batch_solve_lockstep: bad arguments");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    std::vector<int> ids;
+    for (int id = 0; id < (int)B->mem.size(); ++id)
+        if (B->mem[id]) ids.push_back(id);
+    int st;
+    for (size_t p = 0; p < ids.size(); ++p)
+        if ((st = arm_member(B, ids[p], b_dev[p], x_dev[p], max_iter, tol))) return st;
+    st = ls_solve(ctx, B, ids, mixed != 0, results);
+    for (int id : ids) B->mem[id]->armed = false;
+    return st;
+}
+
+int femd_cuda_batch_lockstep_configure(femd_batch handle, int nnz_per_entry, int chunk)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(B, "batch_lockstep_configure: bad handle");
+    FEMD_CHECK_ARG(nnz_per_entry >= 0 && chunk >= 0, "batch_lockstep_configure: negative argument");
+    if (nnz_per_entry) B->ls_nnz = nnz_per_entry;
+    if (chunk) B->ls_chunk = chunk;
+    return FEMD_OK;
 }
 
 int femd_cuda_batch_tune(femd_ctx ctx, femd_batch handle, const double *const *b_dev, double *const *x_dev, int max_iter,

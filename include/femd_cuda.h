@@ -266,6 +266,18 @@ FEMD_API int femd_cuda_batch_create(femd_ctx ctx, int nprob, const femd_matrix *
  * per member.  results[p] per member; res.seconds = the launch. */
 FEMD_API int femd_cuda_batch_solve(femd_ctx ctx, femd_batch B, const double *const *b_dev, double *const *x_dev,
                                    int max_iter, double tol, int mixed, femd_cg_result *results);
+/* The same solve by the lockstep engine: every iteration is a few whole-GPU kernels over all the
+ * members still running (an SpMV with the direction and p.Ap, the update; in mixed precision a
+ * flush and an FP64 residual for the members due a reliable update), the members' sums taken in a
+ * fixed order, so each member's iterates do not depend on the other members.  Same stopping rule,
+ * acceptance and mixed-precision fallback as femd_cuda_batch_solve; results[p].seconds = the whole
+ * solve.  No reference counterpart (the batched form of cg_jacobi, solver/cg.hpp:118). */
+FEMD_API int femd_cuda_batch_solve_lockstep(femd_ctx ctx, femd_batch B, const double *const *b_dev, double *const *x_dev,
+                                            int max_iter, double tol, int mixed, femd_cg_result *results);
+/* Shape of the lockstep engine: nonzeros per row range of a member (one thread block each;
+ * default 16384) and iterations enqueued between two reads of the members' states (default 8);
+ * 0 keeps the current value.  No reference counterpart. */
+FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry, int chunk);
 /* Add a member (a square matrix with its Jacobi inverse diagonal); *id_out its id (a free id is
  * reused).  Remove frees its solver vectors; a removed member's solve is dropped. */
 FEMD_API int femd_cuda_batch_add(femd_batch B, femd_matrix K, int *id_out);
