@@ -61,9 +61,11 @@ class Batch:
         """Set the launch shape (femd_cuda_batch_configure)."""
         check(lib.femd_cuda_batch_configure(self.h, int(block), int(nnz_per_block), int(nnz_per_thread)))
 
-    def configure_lockstep(self, nnz_per_entry=0, chunk=0):
-        """Shape of the lockstep engine (femd_cuda_batch_lockstep_configure; 0 keeps a value)."""
-        check(lib.femd_cuda_batch_lockstep_configure(self.h, int(nnz_per_entry), int(chunk)))
+    def configure_lockstep(self, nnz_per_entry=0, chunk=0, windows=None):
+        """Shape of the lockstep engine (femd_cuda_batch_lockstep_configure; 0 / None keep a
+        value).  windows: SpMV by windows of whole rows (True) or by row groups (False)."""
+        w = -1 if windows is None else int(bool(windows))
+        check(lib.femd_cuda_batch_lockstep_configure(self.h, int(nnz_per_entry), int(chunk), w))
 
     def params(self):
         b, n, t, g = C.c_int(), C.c_int(), C.c_int(), C.c_int()

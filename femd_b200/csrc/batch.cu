@@ -33,6 +33,7 @@
 // FP32 vectors and SpMV accumulation; FP64 residual b - A x on the FP64 matrix and FP64 solution
 // update at reliable updates.
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -60,7 +61,8 @@ struct BState {
 
 struct BProb {
     int n, team, max_iter, nch, nnz;
-    int tpr;               // lockstep engine: lanes per row of its SpMV
+    int tpr;               // lockstep engine: lanes per row of its row-group SpMV
+    const int *wrow;       // lockstep engine: first rows of its SpMV windows (null: row groups)
     double tol;
     const int *indptr, *indices;
     const int *crow, *cq;  // chunk c = rows [crow[c], crow[c+1]) = nonzeros [cq[c], cq[c+1])
@@ -823,6 +825,7 @@ struct LState {
 
 struct LBlock {
     int m, r0, r1, b0, b1;  // member, its rows [r0, r1), the member's entries [b0, b1)
+    int w0, w1;             // its SpMV windows [w0, w1) (window mode)
 };
 
 static constexpr int LS_BB = 256;
@@ -861,15 +864,68 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
     }
 }
 
+// SpMV windows: whole rows with at most LS_W nonzeros each (a window's rows start within LS_W -
+// maxlen nonzeros of each other).  A window's column indices and values are read by coalesced
+// loads, LS_NPT per thread, all issued before the gathers; the products go to shared memory
+// (two buffers, one barrier per window) and each row is summed in order by one thread.
+static constexpr int LS_NPT = 4, LS_W = LS_BB * LS_NPT;
+
 template <class V, class F, class Gather, class Out>
-__device__ __forceinline__ void ls_rows_any(const BProb &P, const V *A, int r0, int r1, Gather g, Out out)
+__device__ __forceinline__ void ls_windows(const BProb &P, const V *A, int w0, int w1, Gather g, Out out)
 {
+    __shared__ F prod[2][LS_W];
+    const int tid = (int)threadIdx.x;
+    for (int w = w0; w < w1; ++w) {
+        F *pb = prod[(w - w0) & 1];
+        const int rs = P.wrow[w], re = P.wrow[w + 1];
+        const int qs = P.indptr[rs], qe = P.indptr[re];
+        int col[LS_NPT];
+        V a[LS_NPT];
+#pragma unroll
+        for (int t = 0; t < LS_NPT; ++t) {
+            const int q = qs + t * LS_BB + tid;
+            col[t] = q < qe ? __ldcs(&P.indices[q]) : -1;
+            a[t] = q < qe ? __ldcs(&A[q]) : V(0);
+        }
+        const int row0 = rs + tid;
+        int lo = 0, hi = 0;
+        if (row0 < re) {
+            lo = P.indptr[row0];
+            hi = P.indptr[row0 + 1];
+        }
+        F gv[LS_NPT];
+#pragma unroll
+        for (int t = 0; t < LS_NPT; ++t) gv[t] = col[t] >= 0 ? g(col[t]) : F(0);
+#pragma unroll
+        for (int t = 0; t < LS_NPT; ++t)
+            if (col[t] >= 0) pb[t * LS_BB + tid] = (F)a[t] * gv[t];
+        __syncthreads();
+        for (int row = row0; row < re; row += LS_BB) {
+            if (row != row0) {
+                lo = P.indptr[row];
+                hi = P.indptr[row + 1];
+            }
+            F s = F(0);
+            for (int q = lo; q < hi; ++q) s += pb[q - qs];
+            out(row, s);
+        }
+    }
+}
+
+// y = A g over an entry: by windows when the member has a window table, else by row groups
+template <class V, class F, class Gather, class Out>
+__device__ __forceinline__ void ls_spmv_entry(const BProb &P, const V *A, const LBlock &L, Gather g, Out out)
+{
+    if (P.wrow) {
+        ls_windows<V, F>(P, A, L.w0, L.w1, g, out);
+        return;
+    }
     switch (P.tpr) {
-    case 2: ls_rows<2, V, F>(P, A, r0, r1, g, out); break;
-    case 4: ls_rows<4, V, F>(P, A, r0, r1, g, out); break;
-    case 8: ls_rows<8, V, F>(P, A, r0, r1, g, out); break;
-    case 16: ls_rows<16, V, F>(P, A, r0, r1, g, out); break;
-    default: ls_rows<32, V, F>(P, A, r0, r1, g, out); break;
+    case 2: ls_rows<2, V, F>(P, A, L.r0, L.r1, g, out); break;
+    case 4: ls_rows<4, V, F>(P, A, L.r0, L.r1, g, out); break;
+    case 8: ls_rows<8, V, F>(P, A, L.r0, L.r1, g, out); break;
+    case 16: ls_rows<16, V, F>(P, A, L.r0, L.r1, g, out); break;
+    default: ls_rows<32, V, F>(P, A, L.r0, L.r1, g, out); break;
     }
 }
 
@@ -950,8 +1006,8 @@ __global__ void __launch_bounds__(LS_BB) k_ls_spmv(const BProb *__restrict__ pro
     const F *pold = (it & 1) ? pa : pb;
     F *pnew = (it & 1) ? pb : pa;
     double dot = 0.0;
-    ls_rows_any<F, F>(
-        P, A, L.r0, L.r1, [&](int j) { return pdir(z, pold, beta, j); },
+    ls_spmv_entry<F, F>(
+        P, A, L, [&](int j) { return pdir(z, pold, beta, j); },
         [&](int i, F s) {
             const F pi = pdir(z, pold, beta, i);
             pnew[i] = pi;
@@ -1070,8 +1126,8 @@ __global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ pr
         F *pb = MIXED ? (F *)P.pb32 : (F *)P.pb64;
         const double *x = P.x;
         double v[3] = {0.0, 0.0, 0.0};
-        ls_rows_any<double, double>(
-            P, P.A64, L.r0, L.r1, [&](int j) { return x[j]; },
+        ls_spmv_entry<double, double>(
+            P, P.A64, L, [&](int j) { return x[j]; },
             [&](int i, double s) {
                 const double bi = P.b[i], ri = bi - s;
                 v[0] += ri * ri;
@@ -1179,6 +1235,8 @@ struct Member {
     bool need_f32 = false;                      // armed: the FP32 copies are made before its first mixed launch
     bool force_fp64 = false;                    // its FP32 recurrence stagnated: FP64 for the rest of the solve
     int prior_its = 0, prior_rus = 0;           // iterations and reliable updates before the switch
+    DevBuf<int> ls_tab;                         // lockstep SpMV windows: first rows (nw + 1), scratch
+    std::vector<int> ls_wrow;                   // the same on the host (empty: not built)
 };
 
 }  // namespace
@@ -1213,6 +1271,7 @@ struct femd_batch_s : femd::HandleBase {
     int *abort_host = nullptr;                  // mapped pinned flag
     // the lockstep engine: nonzeros per table entry, iterations enqueued between state reads
     int ls_nnz = 16384, ls_chunk = 8;
+    bool ls_windows = true;                     // SpMV by windows (else by row groups)
     int *abort_dev = nullptr;
     femd_batch_s() : HandleBase(femd::KIND_BATCH) {}
     void drop_graphs()
@@ -1695,6 +1754,27 @@ static int ls_rows_per_entry(const femd_batch_s *B, const Member &M)
     return (int)std::max(32LL, std::min((long long)M.n, r));
 }
 
+// a member's SpMV windows for the lockstep engine (built once): window c holds the rows that start
+// at nonzeros [c cp, (c + 1) cp), cp = LS_W - the longest row, so at most LS_W - 1 nonzeros.  A
+// member whose longest row is over LS_W / 2 keeps none (row groups).
+static int ls_windows_of(femd_batch_s *B, Member &M)
+{
+    if (!M.ls_wrow.empty() || M.maxlen > LS_W / 2) return FEMD_OK;
+    cudaStream_t s = B->ctx->stream;
+    const int cp = LS_W - M.maxlen;
+    const int nw = (int)std::max<long long>(1, (M.nnz + cp - 1) / cp);
+    int st;
+    if ((st = M.ls_tab.alloc(2 * (size_t)(nw + 1)))) return st;
+    k_chunk_table<<<grid_for((size_t)nw + 1, 256), 256, 0, counted(s)>>>(M.K->pattern->indptr.p, M.n, (int)M.nnz, cp, nw,
+                                                                         M.ls_tab.p, M.ls_tab.p + nw + 1);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    std::vector<int> h((size_t)nw + 1);
+    FEMD_TRY_CUDA(cudaMemcpyAsync(h.data(), M.ls_tab.p, (nw + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    M.ls_wrow.swap(h);
+    return FEMD_OK;
+}
+
 namespace {
 struct PinnedBuf {
     void *p = nullptr;
@@ -1717,14 +1797,30 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     for (int id : ids)
         if ((st = member_vectors(B, *B->mem[id], mx))) return st;
     std::vector<BProb> desc(nm);
-    std::vector<int> rows(nm), nent(nm);
+    std::vector<std::vector<std::array<int, 4>>> ents(nm);   // per member: r0, r1, w0, w1 of its entries
+    std::vector<int> nent(nm);
     int NEfull = 0, max_it = 1;
     for (int k = 0; k < nm; ++k) {
         Member &M = *B->mem[ids[k]];
         desc[k] = describe(B, ids[k], mx);
         desc[k].tpr = ls_tpr(M);
-        rows[k] = ls_rows_per_entry(B, M);
-        nent[k] = (M.n + rows[k] - 1) / rows[k];
+        desc[k].wrow = nullptr;
+        if (B->ls_windows && (st = ls_windows_of(B, M))) return st;
+        auto &E = ents[k];
+        E.clear();
+        if (B->ls_windows && !M.ls_wrow.empty()) {
+            desc[k].wrow = M.ls_tab.p;
+            const int nw = (int)M.ls_wrow.size() - 1;
+            const int G = std::max(1, B->ls_nnz / LS_W);
+            for (int w = 0; w < nw; w += G) {
+                const int w1 = std::min(nw, w + G);
+                E.push_back({M.ls_wrow[w], M.ls_wrow[w1], w, w1});
+            }
+        } else {
+            const int R = ls_rows_per_entry(B, M);
+            for (int r = 0; r < M.n; r += R) E.push_back({r, std::min(M.n, r + R), 0, 0});
+        }
+        nent[k] = (int)E.size();
         FEMD_CHECK_ARG((long long)NEfull + nent[k] < INT_MAX / 4, "batch: too many table entries");
         NEfull += nent[k];
         max_it = std::max(max_it, M.max_iter);
@@ -1758,10 +1854,7 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
         for (int k = 0; k < nm; ++k) {
             if (live && live[k].done) continue;
             const int b0 = e;
-            for (int j = 0; j < nent[k]; ++j) {
-                T[e] = LBlock{k, j * rows[k], std::min(desc[k].n, (j + 1) * rows[k]), b0, b0 + nent[k]};
-                ++e;
-            }
+            for (const auto &x : ents[k]) T[e++] = LBlock{k, x[0], x[1], b0, b0 + nent[k], x[2], x[3]};
         }
         return e;
     };
@@ -2061,14 +2154,15 @@ int femd_cuda_batch_solve_lockstep(femd_ctx ctx, femd_batch handle, const double
     return st;
 }
 
-int femd_cuda_batch_lockstep_configure(femd_batch handle, int nnz_per_entry, int chunk)
+int femd_cuda_batch_lockstep_configure(femd_batch handle, int nnz_per_entry, int chunk, int windows)
 {
     clear_error();
     femd_batch_s *B = as_batch(handle);
     FEMD_CHECK_ARG(B, "batch_lockstep_configure: bad handle");
-    FEMD_CHECK_ARG(nnz_per_entry >= 0 && chunk >= 0, "batch_lockstep_configure: negative argument");
+    FEMD_CHECK_ARG(nnz_per_entry >= 0 && chunk >= 0 && windows >= -1 && windows <= 1, "batch_lockstep_configure: bad argument");
     if (nnz_per_entry) B->ls_nnz = nnz_per_entry;
     if (chunk) B->ls_chunk = chunk;
+    if (windows >= 0) B->ls_windows = windows != 0;
     return FEMD_OK;
 }
 

@@ -275,9 +275,11 @@ FEMD_API int femd_cuda_batch_solve(femd_ctx ctx, femd_batch B, const double *con
 FEMD_API int femd_cuda_batch_solve_lockstep(femd_ctx ctx, femd_batch B, const double *const *b_dev, double *const *x_dev,
                                             int max_iter, double tol, int mixed, femd_cg_result *results);
 /* Shape of the lockstep engine: nonzeros per row range of a member (one thread block each;
- * default 16384) and iterations enqueued between two reads of the members' states (default 8);
- * 0 keeps the current value.  No reference counterpart. */
-FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry, int chunk);
+ * default 16384), iterations enqueued between two reads of the members' states (default 8), the
+ * SpMV by windows of whole rows read by coalesced loads (windows = 1, the default) or by row
+ * groups of a few lanes per row (0).  0 (-1 for windows) keeps the current value.  No reference
+ * counterpart. */
+FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry, int chunk, int windows);
 /* Add a member (a square matrix with its Jacobi inverse diagonal); *id_out its id (a free id is
  * reused).  Remove frees its solver vectors; a removed member's solve is dropped. */
 FEMD_API int femd_cuda_batch_add(femd_batch B, femd_matrix K, int *id_out);

@@ -31,12 +31,13 @@ def direct(K, b):
 
 
 @pytest.mark.parametrize("mixed", [False, True])
-@pytest.mark.parametrize("nnz_per_entry,chunk", [(0, 0), (256, 3), (4096, 1)])
-def test_lockstep_matches_direct_solve(fb, problems, mixed, nnz_per_entry, chunk):
+@pytest.mark.parametrize("nnz_per_entry,chunk,windows", [(0, 0, True), (256, 3, True), (4096, 1, True), (0, 0, False),
+                                                         (4096, 2, False)])
+def test_lockstep_matches_direct_solve(fb, problems, mixed, nnz_per_entry, chunk, windows):
     mats = [K for _, K, _ in problems]
     bs = [b for _, _, b in problems]
     B = fb.Batch(mats)
-    B.configure_lockstep(nnz_per_entry, chunk)
+    B.configure_lockstep(nnz_per_entry, chunk, windows)
     xs, res = B.solve(bs, tol=1e-10, mixed=mixed, engine="lockstep")
     assert B.last_status == 0
     for (s, K, b), x, r in zip(problems, xs, res):
@@ -70,8 +71,10 @@ def test_lockstep_same_bits_alone_in_the_mix_and_any_chunk(fb, problems, mixed):
     B1 = fb.Batch(mats)
     B1.configure_lockstep(chunk=1)
     xs1, _ = B1.solve(bs, tol=1e-10, mixed=mixed, engine="lockstep")
+    xs2, _ = B1.solve(bs, tol=1e-10, mixed=mixed, engine="lockstep")
     for p in range(len(mats)):
         assert np.array_equal(xs1[p].cpu().numpy(), xs[p].cpu().numpy())
+        assert np.array_equal(xs2[p].cpu().numpy(), xs[p].cpu().numpy())
     for p in (0, 6, 13):
         xa, _ = fb.Batch([mats[p]]).solve([bs[p]], tol=1e-10, mixed=mixed, engine="lockstep")
         assert np.array_equal(xa[0].cpu().numpy(), xs[p].cpu().numpy())
