@@ -276,8 +276,8 @@ FEMD_API int femd_cuda_batch_solve_lockstep(femd_ctx ctx, femd_batch B, const do
                                             int max_iter, double tol, int mixed, femd_cg_result *results);
 /* Shape of the lockstep engine: nonzeros per row range of a member (one thread block each;
  * default 16384), iterations enqueued between two reads of the members' states (default 8), the
- * SpMV by windows of whole rows read by coalesced loads (windows = 1, the default) or by row
- * groups of a few lanes per row (0).  0 (-1 for windows) keeps the current value.  No reference
+ * SpMV by windows of whole rows read by coalesced loads (windows = 1) or by row groups of a few
+ * lanes per row (0, the default).  0 (-1 for windows) keeps the current value.  No reference
  * counterpart. */
 FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry, int chunk, int windows);
 /* Add a member (a square matrix with its Jacobi inverse diagonal); *id_out its id (a free id is
