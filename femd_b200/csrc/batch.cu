@@ -63,7 +63,6 @@ struct BProb {
     int n, team, max_iter, nch, nnz;
     int tpr;               // lockstep engine: lanes per row of its row-group SpMV
     const int *wrow;       // lockstep engine: first rows of its SpMV windows (null: row groups)
-    void *zp[2];           // lockstep engine: pairs {z, p} (FP32 or FP64), ping-pong by iteration
     double tol;
     const int *indptr, *indices;
     const int *crow, *cq;  // chunk c = rows [crow[c], crow[c+1]) = nonzeros [cq[c], cq[c+1])
@@ -103,8 +102,6 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 
 __device__ __forceinline__ float pdir(const float *z, const float *p, float beta, int j) { return __fmaf_rn(beta, p[j], z[j]); }
 __device__ __forceinline__ double pdir(const double *z, const double *p, double beta, int j) { return __fma_rn(beta, p[j], z[j]); }
-__device__ __forceinline__ float pdir2(float2 v, float beta) { return __fmaf_rn(beta, v.y, v.x); }
-__device__ __forceinline__ double pdir2(double2 v, double beta) { return __fma_rn(beta, v.y, v.x); }
 
 // team barrier: false when the batch has to stop (timeout or abort).  lead_sync: the block has
 // not synchronised since its last global writes.
@@ -999,19 +996,21 @@ __global__ void __launch_bounds__(LS_BB) k_ls_spmv(const BProb *__restrict__ pro
     const BProb P = probs[L.m];
     LState &S = st[L.m];
     if (S.done) return;
-    using F2 = typename std::conditional<MIXED, float2, double2>::type;
+    const F *z = MIXED ? (const F *)P.z32 : (const F *)P.z64;
+    F *pa = MIXED ? (F *)P.pa32 : (F *)P.pa64;
+    F *pb = MIXED ? (F *)P.pb32 : (F *)P.pb64;
     F *Ap = MIXED ? (F *)P.Ap32 : (F *)P.Ap64;
     const F *A = MIXED ? (const F *)P.A32 : (const F *)P.A64;
     const int it = S.it;
     const F beta = (F)S.beta;
-    const F2 *zp = (const F2 *)((it & 1) ? P.zp[1] : P.zp[0]);             // {z, pold}: one gather brings both
-    F2 *zpn = (F2 *)((it & 1) ? P.zp[0] : P.zp[1]);
+    const F *pold = (it & 1) ? pa : pb;
+    F *pnew = (it & 1) ? pb : pa;
     double dot = 0.0;
     ls_spmv_entry<F, F>(
-        P, A, L, [&](int j) { return pdir2(zp[j], beta); },
+        P, A, L, [&](int j) { return pdir(z, pold, beta, j); },
         [&](int i, F s) {
-            const F pi = pdir2(zp[i], beta);
-            zpn[i].y = pi;
+            const F pi = pdir(z, pold, beta, i);
+            pnew[i] = pi;
             Ap[i] = s;
             dot += (double)pi * (double)s;
         });
@@ -1040,10 +1039,10 @@ __global__ void __launch_bounds__(LS_BB) k_ls_update(const BProb *__restrict__ p
     const BProb P = probs[L.m];
     LState &S = st[L.m];
     if (S.done) return;
-    using F2 = typename std::conditional<MIXED, float2, double2>::type;
     F *r = MIXED ? (F *)P.r32 : (F *)P.r64;
+    F *z = MIXED ? (F *)P.z32 : (F *)P.z64;
     const int it = S.it;
-    F2 *zp = (F2 *)((it & 1) ? P.zp[0] : P.zp[1]);                   // p of this iteration in, the next z out
+    const F *p = (it & 1) ? (MIXED ? (const F *)P.pb32 : (const F *)P.pb64) : (MIXED ? (const F *)P.pa32 : (const F *)P.pa64);
     const F *Ap = MIXED ? (const F *)P.Ap32 : (const F *)P.Ap64;
     const F *inv = MIXED ? (const F *)P.inv32 : (const F *)P.inv64;
     F *acc = MIXED ? (F *)P.d32 : (F *)P.x;
@@ -1052,10 +1051,9 @@ __global__ void __launch_bounds__(LS_BB) k_ls_update(const BProb *__restrict__ p
     for (int i = L.r0 + (int)threadIdx.x; i < L.r1; i += LS_BB) {
         const F ri = r[i] - alpha * Ap[i];
         const F zi = inv[i] * ri;
-        const F pi = zp[i].y;
         r[i] = ri;
-        zp[i].x = zi;
-        acc[i] = acc[i] + alpha * pi;
+        z[i] = zi;
+        acc[i] = acc[i] + alpha * p[i];
         v[0] += (double)ri * (double)ri;
         v[1] += (double)ri * (double)zi;
     }
@@ -1125,8 +1123,7 @@ __global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ pr
         LState &S = st[L.m];
         if (MODE == 0 && S.started) continue;
         if (MODE == 2 && S.zero) continue;
-        using F2 = typename std::conditional<MIXED, float2, double2>::type;
-        F2 *zp = (F2 *)((S.it & 1) ? P.zp[1] : P.zp[0]);                   // the z that the next SpMV reads
+        F *pb = MIXED ? (F *)P.pb32 : (F *)P.pb64;
         const double *x = P.x;
         double v[3] = {0.0, 0.0, 0.0};
         ls_spmv_entry<double, double>(
@@ -1138,18 +1135,18 @@ __global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ pr
                     if (MIXED) {
                         const float rf = (float)ri, zf = (float)P.inv64[i] * rf;
                         P.r32[i] = rf;
-                        zp[i].x = zf;
+                        P.z32[i] = zf;
                         v[1] += (double)rf * (double)zf;
                     } else {
                         const double zi = P.inv64[i] * ri;
                         P.r64[i] = ri;
-                        zp[i].x = zi;
+                        P.z64[i] = zi;
                         v[1] += ri * zi;
                     }
                 }
                 if (MODE == 0) {
                     v[2] += bi * bi;
-                    zp[i].y = F(0);
+                    pb[i] = F(0);
                     if (MIXED) P.d32[i] = 0.0f;
                 }
             });
@@ -1442,17 +1439,13 @@ static int add_member(femd_batch_s *B, femd_matrix K, int *id_out)
     return FEMD_OK;
 }
 
-// the spacing of the lockstep engine's vectors in a member's arenas (16-byte aligned pairs)
-static size_t ls_span(int n) { return ((size_t)n + 3) & ~(size_t)3; }
-
-// the member's vectors of one precision (stream-ordered allocation on the first use); the
-// arenas hold the persistent engine's vectors or the lockstep engine's (ls_layout)
+// the member's vectors of one precision (stream-ordered allocation on the first use)
 static int member_vectors(femd_batch_s *B, Member &M, bool mixed)
 {
     cudaStream_t s = B->ctx->stream;
     const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
     if (mixed && !M.f32) {
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 8 * ls_span(M.n) + 40) * sizeof(float), s);
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 7 * n + 32) * sizeof(float), s);
         if (e != cudaSuccess) { M.f32 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
         if (reinterpret_cast<uintptr_t>(M.f32) & 15) {
             // the FP32 values are read by 16-byte bulk copies
@@ -1463,7 +1456,7 @@ static int member_vectors(femd_batch_s *B, Member &M, bool mixed)
         }
     }
     if (!mixed && !M.f64) {
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f64), (6 * ls_span(M.n) + 8) * sizeof(double), s);
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f64), (5 * n + 8) * sizeof(double), s);
         if (e != cudaSuccess) { M.f64 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
     }
     return FEMD_OK;
@@ -1782,29 +1775,6 @@ static int ls_windows_of(femd_batch_s *B, Member &M)
     return FEMD_OK;
 }
 
-// the lockstep engine's vectors in the member's arena: FP32 (after A32 and inv32) r, {z, p} x 2,
-// A p, d; FP64 r, {z, p} x 2, A p
-static void ls_layout(const Member &M, bool mixed, BProb &P)
-{
-    const size_t nn = ls_span(M.n);
-    if (mixed) {
-        float *f = P.inv32 + nn;
-        P.r32 = f; f += nn;
-        P.zp[0] = f; f += 2 * nn;
-        P.zp[1] = f; f += 2 * nn;
-        P.Ap32 = f; f += nn;
-        P.d32 = f;
-        P.z32 = P.pa32 = P.pb32 = nullptr;
-    } else {
-        double *d = M.f64;
-        P.r64 = d; d += nn;
-        P.zp[0] = d; d += 2 * nn;
-        P.zp[1] = d; d += 2 * nn;
-        P.Ap64 = d;
-        P.z64 = P.pa64 = P.pb64 = nullptr;
-    }
-}
-
 namespace {
 struct PinnedBuf {
     void *p = nullptr;
@@ -1833,7 +1803,6 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     for (int k = 0; k < nm; ++k) {
         Member &M = *B->mem[ids[k]];
         desc[k] = describe(B, ids[k], mx);
-        ls_layout(M, mx, desc[k]);
         desc[k].tpr = ls_tpr(M);
         desc[k].wrow = nullptr;
         if (B->ls_windows && (st = ls_windows_of(B, M))) return st;
