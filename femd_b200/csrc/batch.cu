@@ -864,123 +864,62 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
     }
 }
 
-// SpMV windows: whole rows with at most LS_W - 1 nonzeros each (a window's rows start within
-// LS_W - maxlen nonzeros of each other).  A window's column indices and values are brought into
-// shared memory by bulk copies (two buffers: the next window streams in while this one is
-// computed, so the loads of the stream are many and long); row groups of TPR lanes then read
-// them from shared memory and only the gathers wait on global memory.
-static constexpr int LS_W = 1024, LS_IXN = LS_W + 8;
-
-struct LsStage {
-    int ix[2][LS_IXN];
-    double val[2][LS_IXN];     // FP64 values, or FP32 values in the first half
-    uint64_t mbar[2];
-};
-
-// thread 0: bulk copies of window w's indices and values [qa, qb) into buffer b (qa = the first
-// nonzero rounded down to 4, qb = the end rounded up but not past nnz rounded down to 4: 16-byte
-// aligned and sized; at most 3 nonzeros at the matrix's end are read directly)
-template <class V>
-__device__ __forceinline__ void ls_issue(const BProb &P, const V *A, int w, int b, LsStage &S)
-{
-    const int qs = P.indptr[P.wrow[w]], qe = P.indptr[P.wrow[w + 1]];
-    const int qa = qs & ~3, qb = staged_end(qa, qe, P.nnz & ~3);
-    const unsigned n = (unsigned)(qb - qa);
-    fence_proxy_async_smem();                         // the buffer's last readers were generic
-    mbar_arrive_tx(&S.mbar[b], n * (unsigned)(sizeof(int) + sizeof(V)));
-    if (n) {
-        bulk_g2s(S.ix[b], P.indices + qa, n * (unsigned)sizeof(int), &S.mbar[b]);
-        bulk_g2s(S.val[b], A + qa, n * (unsigned)sizeof(V), &S.mbar[b]);
-    }
-}
-
-// rows [rs, re) of a staged window by row groups of TPR lanes (U loads in flight per lane)
-template <int TPR, class V, class F, class Gather, class Out>
-__device__ __forceinline__ void ls_rows_staged(const BProb &P, const V *A, const int *ix, const V *vs, int qa, int qb, int rs,
-                                               int re, Gather g, Out out)
-{
-    constexpr int U = 4, GPW = 32 / TPR;
-    const int lane = threadIdx.x % TPR;
-    for (int i0 = rs + (int)(threadIdx.x >> 5) * GPW; i0 < re; i0 += (LS_BB / 32) * GPW) {
-        const int i = i0 + (int)(threadIdx.x & 31) / TPR;
-        F s = F(0);
-        if (i < re) {
-            const int lo = P.indptr[i], hi = P.indptr[i + 1];
-            for (int base = lo + lane; base < hi; base += U * TPR) {
-                int c[U];
-                V v[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int q = base + u * TPR;
-                    c[u] = 0;
-                    v[u] = V(0);
-                    if (q < qb) { c[u] = ix[q - qa]; v[u] = vs[q - qa]; }
-                    else if (q < hi) { c[u] = P.indices[q]; v[u] = A[q]; }
-                }
-                F xv[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) xv[u] = base + u * TPR < hi ? g(c[u]) : F(0);
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (base + u * TPR < hi) s += (F)v[u] * xv[u];
-            }
-        }
-#pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
-        if (lane == 0 && i < re) out(i, s);
-    }
-}
+// SpMV windows: whole rows with at most LS_W nonzeros each (a window's rows start within LS_W -
+// maxlen nonzeros of each other).  A window's column indices and values are read by coalesced
+// loads, LS_NPT per thread, all issued before the gathers; the products go to shared memory
+// (two buffers, one barrier per window) and each row is summed in order by one thread.
+static constexpr int LS_NPT = 4, LS_W = LS_BB * LS_NPT;
 
 template <class V, class F, class Gather, class Out>
-__device__ __forceinline__ void ls_staged_tpr(const BProb &P, const V *A, const int *ix, const V *vs, int qa, int qb, int rs,
-                                              int re, Gather g, Out out)
+__device__ __forceinline__ void ls_windows(const BProb &P, const V *A, int w0, int w1, Gather g, Out out)
 {
-    switch (P.tpr) {
-    case 2: ls_rows_staged<2, V, F>(P, A, ix, vs, qa, qb, rs, re, g, out); break;
-    case 4: ls_rows_staged<4, V, F>(P, A, ix, vs, qa, qb, rs, re, g, out); break;
-    case 8: ls_rows_staged<8, V, F>(P, A, ix, vs, qa, qb, rs, re, g, out); break;
-    case 16: ls_rows_staged<16, V, F>(P, A, ix, vs, qa, qb, rs, re, g, out); break;
-    default: ls_rows_staged<32, V, F>(P, A, ix, vs, qa, qb, rs, re, g, out); break;
-    }
-}
-
-// the windows [w0, w1) of a member, staged two ahead; par: the threads' copy of the buffers'
-// barrier phases.  false (in every thread): a staging copy did not land within the bounded wait
-// (the other buffer's copy was waited for, bounded, before returning).
-template <class V, class F, class Gather, class Out>
-__device__ __forceinline__ bool ls_windows_staged(const BProb &P, const V *A, int w0, int w1, LsStage &S, unsigned &par,
-                                                  Gather g, Out out)
-{
+    __shared__ F prod[2][LS_W];
     const int tid = (int)threadIdx.x;
-    __syncthreads();                                  // earlier readers of the buffers are done
-    if (tid == 0) {
-        if (w0 < w1) ls_issue<V>(P, A, w0, 0, S);
-        if (w0 + 1 < w1) ls_issue<V>(P, A, w0 + 1, 1, S);
-    }
     for (int w = w0; w < w1; ++w) {
-        const int b = (w - w0) & 1;
+        F *pb = prod[(w - w0) & 1];
         const int rs = P.wrow[w], re = P.wrow[w + 1];
-        const int qa = P.indptr[rs] & ~3, qb = staged_end(qa, P.indptr[re], P.nnz & ~3);
-        const bool ok = mbar_wait(&S.mbar[b], (par >> b) & 1u);
-        par ^= 1u << b;
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0 && w + 1 < w1) mbar_wait(&S.mbar[b ^ 1], (par >> (b ^ 1)) & 1u);
-            return false;
+        const int qs = P.indptr[rs], qe = P.indptr[re];
+        int col[LS_NPT];
+        V a[LS_NPT];
+#pragma unroll
+        for (int t = 0; t < LS_NPT; ++t) {
+            const int q = qs + t * LS_BB + tid;
+            col[t] = q < qe ? __ldcs(&P.indices[q]) : -1;
+            a[t] = q < qe ? __ldcs(&A[q]) : V(0);
         }
-        ls_staged_tpr<V, F>(P, A, S.ix[b], reinterpret_cast<const V *>(S.val[b]), qa, qb, rs, re, g, out);
-        __syncthreads();                              // every thread is done with buffer b
-        if (tid == 0 && w + 2 < w1) ls_issue<V>(P, A, w + 2, b, S);
+        const int row0 = rs + tid;
+        int lo = 0, hi = 0;
+        if (row0 < re) {
+            lo = P.indptr[row0];
+            hi = P.indptr[row0 + 1];
+        }
+        F gv[LS_NPT];
+#pragma unroll
+        for (int t = 0; t < LS_NPT; ++t) gv[t] = col[t] >= 0 ? g(col[t]) : F(0);
+#pragma unroll
+        for (int t = 0; t < LS_NPT; ++t)
+            if (col[t] >= 0) pb[t * LS_BB + tid] = (F)a[t] * gv[t];
+        __syncthreads();
+        for (int row = row0; row < re; row += LS_BB) {
+            if (row != row0) {
+                lo = P.indptr[row];
+                hi = P.indptr[row + 1];
+            }
+            F s = F(0);
+            for (int q = lo; q < hi; ++q) s += pb[q - qs];
+            out(row, s);
+        }
     }
-    return true;
 }
 
-// y = A g over an entry: by staged windows when the member has a window table, else by row groups
-// read straight from global memory.  false: a staging copy did not land.
+// y = A g over an entry: by windows when the member has a window table, else by row groups
 template <class V, class F, class Gather, class Out>
-__device__ __forceinline__ bool ls_spmv_entry(const BProb &P, const V *A, const LBlock &L, LsStage &S, unsigned &par,
-                                              Gather g, Out out)
+__device__ __forceinline__ void ls_spmv_entry(const BProb &P, const V *A, const LBlock &L, Gather g, Out out)
 {
-    if (P.wrow) return ls_windows_staged<V, F>(P, A, L.w0, L.w1, S, par, g, out);
+    if (P.wrow) {
+        ls_windows<V, F>(P, A, L.w0, L.w1, g, out);
+        return;
+    }
     switch (P.tpr) {
     case 2: ls_rows<2, V, F>(P, A, L.r0, L.r1, g, out); break;
     case 4: ls_rows<4, V, F>(P, A, L.r0, L.r1, g, out); break;
@@ -988,18 +927,6 @@ __device__ __forceinline__ bool ls_spmv_entry(const BProb &P, const V *A, const 
     case 16: ls_rows<16, V, F>(P, A, L.r0, L.r1, g, out); break;
     default: ls_rows<32, V, F>(P, A, L.r0, L.r1, g, out); break;
     }
-    return true;
-}
-
-// the staging barriers of a block (before any early return)
-__device__ __forceinline__ void ls_stage_init(LsStage &S)
-{
-    if (threadIdx.x == 0) {
-        mbar_init(&S.mbar[0], 1);
-        mbar_init(&S.mbar[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
 }
 
 // The member's totals of NV sums.  The block's sums go to part[k * NE + e]; in the member's last
@@ -1060,13 +987,10 @@ __device__ __forceinline__ void ls_finish(LState &S, int *active)
 // Block 0 also empties the reliable-update list of the iteration.
 template <bool MIXED>
 __global__ void __launch_bounds__(LS_BB) k_ls_spmv(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
-                                                   LState *st, double *part, int *active, int *ru_count, int *err)
+                                                   LState *st, double *part, int *active, int *ru_count)
 {
     using F = typename std::conditional<MIXED, float, double>::type;
-    __shared__ __align__(16) LsStage SG;
     if (MIXED && blockIdx.x == 0 && threadIdx.x == 0) *ru_count = 0;
-    ls_stage_init(SG);
-    unsigned par = 0;
     const int e = blockIdx.x;
     const LBlock L = blks[e];
     const BProb P = probs[L.m];
@@ -1082,18 +1006,14 @@ __global__ void __launch_bounds__(LS_BB) k_ls_spmv(const BProb *__restrict__ pro
     const F *pold = (it & 1) ? pa : pb;
     F *pnew = (it & 1) ? pb : pa;
     double dot = 0.0;
-    const bool ok = ls_spmv_entry<F, F>(
-        P, A, L, SG, par, [&](int j) { return pdir(z, pold, beta, j); },
+    ls_spmv_entry<F, F>(
+        P, A, L, [&](int j) { return pdir(z, pold, beta, j); },
         [&](int i, F s) {
             const F pi = pdir(z, pold, beta, i);
             pnew[i] = pi;
             Ap[i] = s;
             dot += (double)pi * (double)s;
         });
-    if (!ok) {
-        if (threadIdx.x == 0) atomicExch(err, FEMD_ETIMEOUT);
-        return;
-    }
     const double v[1] = {dot};
     double tot[1];
     if (ls_member_sum<1>(v, part, NE, e, L, &S.t1, tot) && threadIdx.x == 0) {
@@ -1192,12 +1112,9 @@ __global__ void __launch_bounds__(LS_BB) k_ls_flush(const BProb *__restrict__ pr
 template <bool MIXED, int MODE>
 __global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
                                                     LState *st, double *part, int *active, const int *ru_list,
-                                                    const int *ru_count, int *err)
+                                                    const int *ru_count)
 {
     using F = typename std::conditional<MIXED, float, double>::type;
-    __shared__ __align__(16) LsStage SG;
-    ls_stage_init(SG);
-    unsigned par = 0;
     const int cnt = MODE == 1 ? *ru_count : NE;
     for (int w = blockIdx.x; w < cnt; w += gridDim.x) {
         const int e = MODE == 1 ? ru_list[w] : w;
@@ -1209,8 +1126,8 @@ __global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ pr
         F *pb = MIXED ? (F *)P.pb32 : (F *)P.pb64;
         const double *x = P.x;
         double v[3] = {0.0, 0.0, 0.0};
-        const bool ok = ls_spmv_entry<double, double>(
-            P, P.A64, L, SG, par, [&](int j) { return x[j]; },
+        ls_spmv_entry<double, double>(
+            P, P.A64, L, [&](int j) { return x[j]; },
             [&](int i, double s) {
                 const double bi = P.b[i], ri = bi - s;
                 v[0] += ri * ri;
@@ -1233,10 +1150,6 @@ __global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ pr
                     if (MIXED) P.d32[i] = 0.0f;
                 }
             });
-        if (!ok) {
-            if (threadIdx.x == 0) atomicExch(err, FEMD_ETIMEOUT);
-            return;
-        }
         double tot[3];
         if (!ls_member_sum<3>(v, part, NE, e, L, &S.t3, tot) || threadIdx.x != 0) continue;
         const double rn = sqrt(tot[0]);
@@ -1922,20 +1835,18 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     DevBuf<LState> d_state;
     DevBuf<LBlock> d_tab;
     DevBuf<double> d_part;
-    DevBuf<int> d_int;                                  // active, ru_count, err, ru_list (NEfull)
+    DevBuf<int> d_int;                                  // active, ru_count, ru_list (NEfull)
     if ((st = d_desc.alloc(nm)) || (st = d_state.alloc(nm)) || (st = d_tab.alloc(NEfull)) || (st = d_part.alloc(3 * (size_t)NEfull)) ||
-        (st = d_int.alloc(3 + (size_t)NEfull)))
+        (st = d_int.alloc(2 + (size_t)NEfull)))
         return st;
     // pinned staging: two tables, two state copies, the descriptors
     PinnedBuf pin;
     const size_t tab_b = (size_t)NEfull * sizeof(LBlock), st_b = (size_t)nm * sizeof(LState);
-    FEMD_TRY_CUDA(cudaHostAlloc(&pin.p, 2 * tab_b + 2 * st_b + nm * sizeof(BProb) + 64 + 4 * sizeof(int), cudaHostAllocDefault));
+    FEMD_TRY_CUDA(cudaHostAlloc(&pin.p, 2 * tab_b + 2 * st_b + nm * sizeof(BProb) + 64, cudaHostAllocDefault));
     LBlock *h_tab[2] = {static_cast<LBlock *>(pin.p), static_cast<LBlock *>(pin.p) + NEfull};
     LState *h_st[2] = {reinterpret_cast<LState *>(h_tab[1] + NEfull), nullptr};
     h_st[1] = h_st[0] + nm;
     BProb *h_desc = reinterpret_cast<BProb *>(h_st[1] + nm);
-    int *h_err = reinterpret_cast<int *>(h_desc + nm);  // the error flag after each chunk (two slots)
-    h_err[0] = h_err[1] = 0;
     std::copy(desc.begin(), desc.end(), h_desc);
     // the table of the live members (all of them when live is null)
     auto build = [&](LBlock *T, const LState *live) {
@@ -1948,7 +1859,7 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
         return e;
     };
     const int G1 = std::max(1, 8 * ctx->sm_count);     // grid of the reliable-update kernels
-    int *active = d_int.p, *ru_count = d_int.p + 1, *err = d_int.p + 2, *ru_list = d_int.p + 3;
+    int *active = d_int.p, *ru_count = d_int.p + 1, *ru_list = d_int.p + 2;
     int NE = build(h_tab[0], nullptr);
     int tb = 0;                                         // the host table buffer last uploaded
     cudaEvent_t ev[2] = {nullptr, nullptr}, t0 = nullptr, t1 = nullptr;
@@ -1973,13 +1884,13 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     FEMD_TRY_CUDA(cudaMemcpyAsync(d_desc.p, h_desc, nm * sizeof(BProb), cudaMemcpyHostToDevice, s));
     FEMD_TRY_CUDA(cudaMemcpyAsync(d_tab.p, h_tab[0], NE * sizeof(LBlock), cudaMemcpyHostToDevice, s));
     FEMD_TRY_CUDA(cudaMemsetAsync(d_state.p, 0, st_b, s));
-    FEMD_TRY_CUDA(cudaMemsetAsync(d_int.p, 0, 3 * sizeof(int), s));
+    FEMD_TRY_CUDA(cudaMemsetAsync(d_int.p, 0, 2 * sizeof(int), s));
     FEMD_TRY_CUDA(cudaMemcpyAsync(active, &nm, sizeof(int), cudaMemcpyHostToDevice, s));
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));           // &nm is a host stack value
     if (mx)
-        k_ls_resid<true, 0><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count, err);
+        k_ls_resid<true, 0><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
     else
-        k_ls_resid<false, 0><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count, err);
+        k_ls_resid<false, 0><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
     FEMD_TRY_CUDA(cudaGetLastError());
     const int C = std::max(1, B->ls_chunk);
     const long long max_chunks = (long long)max_it / C + 4;
@@ -1987,20 +1898,19 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     for (long long j = 0; j <= max_chunks; ++j) {
         for (int c = 0; c < C; ++c) {
             if (mx) {
-                k_ls_spmv<true><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count, err);
+                k_ls_spmv<true><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count);
                 k_ls_update<true><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
                 k_ls_flush<false><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, ru_list, ru_count);
                 k_ls_resid<true, 1><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active,
-                                                                                 ru_list, ru_count, err);
+                                                                                 ru_list, ru_count);
             } else {
-                k_ls_spmv<false><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count, err);
+                k_ls_spmv<false><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count);
                 k_ls_update<false><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list,
                                                                    ru_count);
             }
         }
         FEMD_TRY_CUDA(cudaGetLastError());
         FEMD_TRY_CUDA(cudaMemcpyAsync(h_st[j & 1], d_state.p, st_b, cudaMemcpyDeviceToHost, s));
-        FEMD_TRY_CUDA(cudaMemcpyAsync(h_err + (j & 1), err, sizeof(int), cudaMemcpyDeviceToHost, s));
         FEMD_TRY_CUDA(cudaEventRecord(ev[j & 1], s));
         if (j == 0) continue;
         // the states after the previous chunk (one chunk stays queued behind them)
@@ -2010,8 +1920,7 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
         for (int k = 0; k < nm; ++k)
             if (!S[k].done) { ++live; live_e += nent[k]; }
         if (live == 0) break;
-        if (h_err[(j - 1) & 1]) { aborted = h_err[(j - 1) & 1]; break; }
-        if (*(volatile int *)B->abort_host) { aborted = FEMD_EABORT; break; }
+        if (*(volatile int *)B->abort_host) { aborted = 1; break; }
         if (live_e <= (NE * 7) / 10) {
             // compact the table to the live members (their entries keep their order)
             tb ^= 1;
@@ -2030,7 +1939,7 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
             k_ls_flush<true><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, ru_list, ru_count);
         else
             k_ls_resid<false, 2><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list,
-                                                                ru_count, err);
+                                                                ru_count);
         k_ls_zero<<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, d_state.p);
         FEMD_TRY_CUDA(cudaGetLastError());
     }
@@ -2041,8 +1950,7 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     cudaEventElapsedTime(&ms, t0, t1);
     *seconds = ms * 1e-3;
     std::copy(h_st[0], h_st[0] + nm, out.begin());
-    if (aborted == FEMD_EABORT) { set_error("batch: aborted by the host"); return FEMD_EABORT; }
-    if (aborted) { set_error("batch: a staging copy did not land in time"); return FEMD_ETIMEOUT; }
+    if (aborted) { set_error("batch: aborted by the host"); return FEMD_EABORT; }
     return FEMD_OK;
 }
 
@@ -2070,7 +1978,7 @@ static int ls_solve(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, 
     std::vector<LState> S;
     double sec = 0.0;
     int st = ls_run(ctx, B, ids, mx, S, &sec);
-    if (st && st != FEMD_EABORT && st != FEMD_ETIMEOUT) return st;
+    if (st && st != FEMD_EABORT) return st;
     std::vector<int> fb_ids, fb_pos;
     for (size_t p = 0; p < ids.size(); ++p) {
         Member &M = *B->mem[ids[p]];
@@ -2089,7 +1997,7 @@ static int ls_solve(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, 
     std::vector<LState> S2;
     double sec2 = 0.0;
     const int st2 = ls_run(ctx, B, fb_ids, false, S2, &sec2);
-    if (st2 && st2 != FEMD_EABORT && st2 != FEMD_ETIMEOUT) return st2;
+    if (st2 && st2 != FEMD_EABORT) return st2;
     for (size_t q = 0; q < fb_ids.size(); ++q) {
         ls_result(*B->mem[fb_ids[q]], S2[q], results[fb_pos[q]], sec + sec2);
         if (st2) results[fb_pos[q]].status = st2;
