@@ -409,7 +409,7 @@ def ours_c4(args, rank, world, dist):
     b_dev = [torch.as_tensor(b).cuda() for b in rhs]
     b_host = [torch.as_tensor(b).pin_memory() for b in rhs]
     x_host = [torch.empty(b.size, dtype=torch.float64).pin_memory() for b in rhs]
-    srv = serve.Server(lib, [], mixed=True, iters=1 << 30, keep_solutions=False)
+    srv = serve.Server(lib, [], mixed=True, iters=1 << 30, keep_solutions=False, engine=args.engine)
     setup_s = time.time() - t_setup
     ctx = fb.context()
     s = ctx.stream
@@ -458,7 +458,7 @@ def ours_c4(args, rank, world, dist):
     e2e_value = world * args.steps * NPROB / te
     # ---- the plain FP64 GPU path on the same stream (one pass), and the served-vs-plain error
     served = reqs()
-    srv_keep = serve.Server(lib, [], mixed=True, iters=1 << 30, keep_solutions=True)
+    srv_keep = serve.Server(lib, [], mixed=True, iters=1 << 30, keep_solutions=True, engine=args.engine)
     srv_keep.run(served, realtime=False)
     xs_served = {r.rid: r.x for r in served}
     plain = reqs()
@@ -474,7 +474,8 @@ def ours_c4(args, rank, world, dist):
     t_launch = launch_s[-1]
     achieved = alg / t_launch / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "k_batch_pcg_traffic.json")
+    lockstep = args.engine == "lockstep"
+    tp = os.path.join(ROOT, "profiles", "k_ls_spmv_traffic.json" if lockstep else "k_batch_pcg_traffic.json")
     if os.path.exists(tp):
         try:
             traffic = int(json.load(open(tp))["dram_over_algorithmic"] * alg)
@@ -488,8 +489,8 @@ def ours_c4(args, rank, world, dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (FP32 inner PCG, FP64 assembly/residual/update)",
         "data": "synthetic (seeded: meshes, coefficients, N(0,1) load vectors)",
         "config": {"workload": "config-4 stream: 256 Poisson problems, rectangle N x N (N in 16..256), P1-P3, "
-                               "c log-uniform [0.1,10], served (all arrive at t=0; continuous batching, one "
-                               "persistent launch), FP32-inner / FP64-refined Jacobi-PCG to 1e-10",
+                               "c log-uniform [0.1,10], served (all arrive at t=0: one wave of the batched "
+                               f"solver, {args.engine} engine), FP32-inner / FP64-refined Jacobi-PCG to 1e-10",
                    "problems": NPROB, "n_total": n, "nnz_total": nnz, "arrivals": "burst at t=0",
                    "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
                    "mean_iterations": round(st["mean_iterations"], 1), "all_converged": st["all_converged"],
@@ -497,11 +498,16 @@ def ours_c4(args, rank, world, dist):
                    "plain_fp64_gpu": {"solves_per_s": round(pst["solves_per_s"], 3), "p50_ms": round(pst["p50_ms"], 2),
                                       "p99_ms": round(pst["p99_ms"], 2), "mean_iterations": round(pst["mean_iterations"], 1),
                                       "path": "per request: FP64 assembly + cg_solve (CUDA-graph CG), FIFO"},
-                   "batch_shape": srv.batch.params(), "l2": "working set > 4 GB, larger than L2; no flush",
+                   "engine": args.engine,
+                   "batch_shape": srv.batch.params() if not lockstep else {"nnz_per_entry": 16384, "chunk": 8,
+                                                                          "spmv": "row groups"},
+                   "l2": "working set > 4 GB, larger than L2; no flush",
                    "parallelism": f"replicas x{world}", "setup_s": round(setup_s, 2)},
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(sum(b.nbytes for b in rhs)),
                 "d2h_bytes_per_step": int(sum(b.nbytes for b in rhs))},
-        "roofline": {"kernel": "k_batch_pcg (batched persistent Jacobi-PCG, mixed)", "bound": "hbm",
+        "roofline": {"kernel": ("lockstep solve: k_ls_spmv / k_ls_update / k_ls_flush / k_ls_resid over the wave, "
+                                "bytes and time of the whole solve" if lockstep else
+                                "k_batch_pcg (batched persistent Jacobi-PCG, mixed)"), "bound": "hbm",
                      "achieved": round(achieved, 1), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "traffic": traffic, "algorithmic_bytes": alg,
                      "launch_ms": round(t_launch * 1e3, 3)},
@@ -605,6 +611,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--engine", default="lockstep", choices=["lockstep", "persistent"],
+                    help="batched engine of the config-4 stream")
     ap.add_argument("--workload", default="c4s", choices=["c4s", "c2"],
                     help="c4s: the served config-4 stream (default); c2: one P2 solve on 1024x1024")
     args = ap.parse_args()

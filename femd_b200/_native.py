@@ -81,6 +81,7 @@ SIGNATURES = {
     "femd_cuda_batch_solve": (_I, [_P, _P, _P, _P, _I, _D, _I, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_solve_lockstep": (_I, [_P, _P, _P, _P, _I, _D, _I, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_lockstep_configure": (_I, [_P, _I, _I, _I]),
+    "femd_cuda_batch_step_lockstep": (_I, [_P, _P, _I, _PI, _PI, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_abort": (_I, [_P]),
     "femd_cuda_batch_info": (_I, [_P, _PI, _PI, _PI, _PI]),
     "femd_cuda_batch_debug": (_I, [_P, _I, C.c_longlong]),

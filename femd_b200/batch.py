@@ -1,10 +1,13 @@
-"""Batched Jacobi-PCG: many independent systems in one persistent launch (femd_cuda_batch_*).
+"""Batched Jacobi-PCG: many independent systems solved together (femd_cuda_batch_*).
 
-A Batch holds member systems (CSR matrices with their Jacobi inverse diagonals).  solve() runs
-every member to completion in one cooperative launch; arm() / step() advance armed members a
-bounded number of iterations per launch, so members can join and leave between launches (the
-continuous batching of femd_b200.serve).  A member's iterates depend on the member and the
-launch shape alone: the same bits alone or in any mix.
+A Batch holds member systems (CSR matrices with their Jacobi inverse diagonals) and two engines.
+The persistent engine runs every member in one cooperative launch (teams of blocks per member);
+arm() / step() advance armed members a bounded number of iterations per launch, so members can
+join and leave between launches (the continuous batching of femd_b200.serve).  The lockstep
+engine runs each iteration as a few whole-GPU kernels over every member still running, to
+completion (solve(..., engine="lockstep"), or step(engine="lockstep") for a wave of armed
+members).  In either engine a member's iterates depend on the member and the engine's shape
+alone: the same bits alone or in any mix.
 """
 from __future__ import annotations
 
@@ -147,15 +150,21 @@ class Batch:
         check(st)
         self._armed[i] = (b, x)
 
-    def step(self, iters: int, *, mixed=True):
-        """One launch advancing every armed member by at most iters iterations.  Returns
-        [(id, result dict)] of the members that finished."""
+    def step(self, iters: int, *, mixed=True, engine="persistent"):
+        """Advance the armed members.  engine "persistent": one launch, every armed member by at
+        most iters iterations; "lockstep": every armed member to completion (iters unused).
+        Returns [(id, result dict)] of the members that finished."""
+        if engine not in ("persistent", "lockstep"):
+            raise ValueError(f"batch: unknown engine {engine!r}")
         n = max(len(self._armed), 1)
         ids = (C.c_int * n)()
         res = (N.femd_cg_result * n)()
         nf = C.c_int()
         self.ctx.enter()
-        st = lib.femd_cuda_batch_step(self.ctx.h, self.h, int(iters), int(bool(mixed)), C.byref(nf), ids, res)
+        if engine == "persistent":
+            st = lib.femd_cuda_batch_step(self.ctx.h, self.h, int(iters), int(bool(mixed)), C.byref(nf), ids, res)
+        else:
+            st = lib.femd_cuda_batch_step_lockstep(self.ctx.h, self.h, int(bool(mixed)), C.byref(nf), ids, res)
         self.ctx.leave()
         self.last_status = st
         if st not in (N.FEMD_OK, N.FEMD_ETIMEOUT, N.FEMD_EABORT):

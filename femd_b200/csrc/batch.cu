@@ -2071,6 +2071,30 @@ int femd_cuda_batch_step(femd_ctx ctx, femd_batch handle, int iters, int mixed, 
     return batch_step(ctx, B, iters, mixed != 0, nfinished, finished_ids, finished, nullptr);
 }
 
+int femd_cuda_batch_step_lockstep(femd_ctx ctx, femd_batch handle, int mixed, int *nfinished, int *finished_ids,
+                                  femd_cg_result *finished)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(ctx && B && ctx == B->ctx, "batch_step_lockstep: bad arguments");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    if (nfinished) *nfinished = 0;
+    std::vector<int> ids;
+    for (int id = 0; id < (int)B->mem.size(); ++id)
+        if (B->mem[id] && B->mem[id]->armed) ids.push_back(id);
+    if (ids.empty()) return FEMD_OK;
+    std::vector<femd_cg_result> res(ids.size());
+    const int st = ls_solve(ctx, B, ids, mixed != 0, res.data());
+    if (st && st != FEMD_EABORT && st != FEMD_ETIMEOUT) return st;
+    for (size_t p = 0; p < ids.size(); ++p) {
+        B->mem[ids[p]]->armed = false;
+        if (finished_ids) finished_ids[p] = ids[p];
+        if (finished) finished[p] = res[p];
+    }
+    if (nfinished) *nfinished = (int)ids.size();
+    return st;
+}
+
 int femd_cuda_batch_configure(femd_batch handle, int block, int nnz_per_block, int nnz_per_thread)
 {
     clear_error();

@@ -4,12 +4,15 @@
     python -m femd_b200.profile_kernels assemble --n 640 --k 2 --reps 3
     python -m femd_b200.profile_kernels cg --n 640 --k 2
     python -m femd_b200.profile_kernels batch --nmin 150 --nmax 256 --nprob 24 --iters 100 --mixed
+    python -m femd_b200.profile_kernels lockstep --nmin 0 --kmin 1 --nprob 16 --iters 0 --reps 1
 
 Workload: -Lap u + u = f on rectangle_mesh(0, 0, 1, 1, n, n), P_k, zero Dirichlet (the form of
 the config-2 benchmark at another size).  Prints the sizes and a CUDA-event time per launch.
 batch: the problems of the config-4 stream (seed 0) with N in [nmin, nmax] and k >= kmin, the
 first nprob of them, solved together by the batched PCG capped at iters iterations; prints the
-launch time and its algorithmic bytes (femd_b200.workloads.batch_bytes).
+launch time and its algorithmic bytes (femd_b200.workloads.batch_bytes).  lockstep: the same
+problems solved by the lockstep engine (iters 0: to convergence); prints the solve time and its
+algorithmic bytes.
 """
 from __future__ import annotations
 
@@ -21,7 +24,7 @@ PI = math.pi
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("kernel", choices=["spmv", "assemble", "rhs", "cg", "cg_mixed", "pattern", "batch"])
+    ap.add_argument("kernel", choices=["spmv", "assemble", "rhs", "cg", "cg_mixed", "pattern", "batch", "lockstep"])
     ap.add_argument("--n", type=int, default=640)
     ap.add_argument("--k", type=int, default=2)
     ap.add_argument("--reps", type=int, default=3)
@@ -32,7 +35,7 @@ def main():
     ap.add_argument("--iters", type=int, default=100)
     ap.add_argument("--mixed", action="store_true")
     a = ap.parse_args()
-    if a.kernel == "batch":
+    if a.kernel in ("batch", "lockstep"):
         return batch(a)
     import torch
 
@@ -85,11 +88,18 @@ def batch(a):
     probs = [W.build_poisson(s, cache) for s in spec]
     B = fb.Batch([K for K, _ in probs])
     bs = [b for _, b in probs]
+    engine = "lockstep" if a.kernel == "lockstep" else "persistent"
     for _ in range(a.reps):
-        xs, res = B.solve(bs, tol=1e-10, max_iter=a.iters, mixed=a.mixed)
+        xs, res = B.solve(bs, tol=1e-10, max_iter=a.iters, mixed=a.mixed, engine=engine)
     sizes = [(K.nrows, K.nnz) for K, _ in probs]
     alg = W.batch_bytes(sizes, res, a.mixed)
     t = res[0]["seconds"]
+    if engine == "lockstep":
+        its = [r["iterations"] for r in res]
+        print(f"lockstep ({'mixed' if a.mixed else 'fp64'}): {len(probs)} problems, n {sum(n for n, _ in sizes)} "
+              f"nnz {sum(z for _, z in sizes)}, iterations max {max(its)} sum {sum(its)}: {t * 1e3:.3f} ms, "
+              f"algorithmic {alg} B = {alg / t / 1e9:.1f} GB/s")
+        return
     pr = B.profile()
     print(f"batch ({'mixed' if a.mixed else 'fp64'}): {len(probs)} problems, n {sum(n for n, _ in sizes)} "
           f"nnz {sum(z for _, z in sizes)}, {B.info()['slots']} team slots on a grid of {B.info()['grid']}: "

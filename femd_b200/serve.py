@@ -182,11 +182,18 @@ class Server:
     reserve_bytes, and, when hbm_budget is given, that budget less what the requests in flight
     hold.  big_nnz: requests whose matrix has at least that many nonzeros are solved one at a time
     on the whole GPU (femd_b200.cg_solve, the same precision) between batch launches -- a large
-    system streams HBM better with every block on it than as one team among many."""
+    system streams HBM better with every block on it than as one team among many.  engine:
+    "persistent" (members join and leave between launches of at most iters iterations) or
+    "lockstep" (the admitted requests are solved together to completion, one wave at a time;
+    requests that arrive meanwhile wait for the next wave)."""
 
     def __init__(self, lib, sessions=(), *, mixed=True, iters=64, tol=1e-10, reserve_bytes=2 << 30, free_memory=None,
-                 hbm_budget=None, max_members=1024, keep_solutions=False, shape=None, big_nnz=None):
+                 hbm_budget=None, max_members=1024, keep_solutions=False, shape=None, big_nnz=None,
+                 engine="persistent"):
         torch = _torch()
+        if engine not in ("persistent", "lockstep"):
+            raise ValueError(f"serve: unknown engine {engine!r}")
+        self.engine = engine
         self.lib, self.sessions = lib, list(sessions)
         self.mixed, self.iters, self.tol = bool(mixed), int(iters), float(tol)
         self.reserve = int(reserve_bytes)
@@ -297,7 +304,7 @@ class Server:
                         budget -= need
                 queue = keep
             if self.active:
-                fin = self.batch.step(self.iters, mixed=self.mixed)
+                fin = self.batch.step(self.iters, mixed=self.mixed, engine=self.engine)
                 self.launches += 1
                 t_done = time.perf_counter() - t0
                 for mid, res in fin:

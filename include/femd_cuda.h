@@ -274,6 +274,11 @@ FEMD_API int femd_cuda_batch_solve(femd_ctx ctx, femd_batch B, const double *con
  * solve.  No reference counterpart (the batched form of cg_jacobi, solver/cg.hpp:118). */
 FEMD_API int femd_cuda_batch_solve_lockstep(femd_ctx ctx, femd_batch B, const double *const *b_dev, double *const *x_dev,
                                             int max_iter, double tol, int mixed, femd_cg_result *results);
+/* Every armed member solved to completion by the lockstep engine (one wave: the members armed
+ * now start together, members armed later wait for the next call), then disarmed and listed like
+ * femd_cuda_batch_step's finished members.  No reference counterpart. */
+FEMD_API int femd_cuda_batch_step_lockstep(femd_ctx ctx, femd_batch B, int mixed, int *nfinished, int *finished_ids,
+                                           femd_cg_result *finished);
 /* Shape of the lockstep engine: nonzeros per row range of a member (one thread block each;
  * default 16384), iterations enqueued between two reads of the members' states (default 8), the
  * SpMV by windows of whole rows read by coalesced loads (windows = 1) or by row groups of a few

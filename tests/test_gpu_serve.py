@@ -40,7 +40,7 @@ def exact13(t):
                          + np.exp(-13 * np.pi ** 2 * t) * np.sin(3 * np.pi * x) * np.sin(2 * np.pi * y))
 
 
-@pytest.mark.parametrize("path", ["served_mixed", "served_fp64", "plain"])
+@pytest.mark.parametrize("path", ["served_mixed", "served_fp64", "served_lockstep", "plain"])
 def test_example13_heat_loop_pin(sv, lib, path):
     """100 backward-Euler steps to t = 0.1: the reference prints L2 error 1.35e-03."""
     from femd_b200.workloads import l2_error
@@ -49,17 +49,19 @@ def test_example13_heat_loop_pin(sv, lib, path):
     if path == "plain":
         st = sv.run_plain(lib, [S], trace, tol=1e-12, realtime=False)
     else:
-        srv = sv.Server(lib, [S], mixed=(path == "served_mixed"), iters=16, tol=1e-12)
+        srv = sv.Server(lib, [S], mixed=(path != "served_fp64"), iters=16, tol=1e-12,
+                        engine="lockstep" if path == "served_lockstep" else "persistent")
         st = srv.run(trace, realtime=False)
     assert st["completed"] == 100 and st["all_converged"]
     err = l2_error(lib.get(20, 2)["V"], S.u, exact13(0.1))
     assert f"{err:.2e}" == "1.35e-03", err
 
 
-def test_served_results_alone_and_in_the_mix(sv, lib):
+@pytest.mark.parametrize("engine", ["persistent", "lockstep"])
+def test_served_results_alone_and_in_the_mix(sv, lib, engine):
     sessions = sv.make_sessions(lib, 5, 3, sizes=SMALL)
     trace = sv.make_trace(11, 1e6, 24, len(sessions), sizes=SMALL)
-    srv = sv.Server(lib, sessions, mixed=True, iters=8, keep_solutions=True)
+    srv = sv.Server(lib, sessions, mixed=True, iters=8, keep_solutions=True, engine=engine)
     st = srv.run(trace, realtime=False)
     assert st["completed"] == len(trace) and st["all_converged"]
     first_heat = {}
@@ -70,19 +72,20 @@ def test_served_results_alone_and_in_the_mix(sv, lib):
         S.reset()
     for r in [r for r in trace if r.kind == "poisson"][:6] + list(first_heat.values()):
         alone = sv.Request(0, 0.0, r.kind, session=r.session, N=r.N, k=r.k, c=r.c, seed=r.seed)
-        srv1 = sv.Server(lib, sessions, mixed=True, iters=8, keep_solutions=True)
+        srv1 = sv.Server(lib, sessions, mixed=True, iters=8, keep_solutions=True, engine=engine)
         srv1.run([alone], realtime=False)
         assert np.array_equal(alone.x.cpu().numpy(), r.x.cpu().numpy()), r
         if r.kind == "heat":
             sessions[r.session].reset()
 
 
-def test_served_matches_plain_fp64(sv, lib):
+@pytest.mark.parametrize("engine", ["persistent", "lockstep"])
+def test_served_matches_plain_fp64(sv, lib, engine):
     sessions = sv.make_sessions(lib, 6, 2, sizes=SMALL)
     trace = sv.make_trace(12, 1e6, 16, len(sessions), sizes=SMALL)
     for S in sessions:
         S.reset()
-    srv = sv.Server(lib, sessions, mixed=True, iters=16, keep_solutions=True, tol=1e-12)
+    srv = sv.Server(lib, sessions, mixed=True, iters=16, keep_solutions=True, tol=1e-12, engine=engine)
     srv.run(trace, realtime=False)
     served = {r.rid: r.x.clone() for r in trace}
     for S in sessions:
