@@ -108,9 +108,9 @@ def test_admission_by_free_memory(sv, lib):
     peak = [0]
     step = srv.batch.step
 
-    def counting_step(iters, mixed=True):
+    def counting_step(iters, mixed=True, **kw):
         peak[0] = max(peak[0], len(srv.active))
-        return step(iters, mixed=mixed)
+        return step(iters, mixed=mixed, **kw)
 
     srv.batch.step = counting_step
     st = srv.run(trace, realtime=False)
