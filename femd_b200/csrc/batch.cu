@@ -831,36 +831,52 @@ struct LBlock {
 static constexpr int LS_BB = 256;
 
 // y = A g on rows [r0, r1) with TPR lanes per row; out(row, sum) by the row's first lane
-template <int TPR, class V, class F, class Gather, class Out>
-__device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int r1, Gather g, Out out)
+template <int TPR, class V, class F, class Gather, class Pre, class Out>
+__device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int r1, Gather g, Pre pre, Out out)
 {
-    constexpr int U = 4, GPW = 32 / TPR;
+    constexpr int U = 4, GPW = 32 / TPR, STEP = (LS_BB / 32) * GPW;
     const int lane = threadIdx.x % TPR;
-    for (int i0 = r0 + (int)(threadIdx.x >> 5) * GPW; i0 < r1; i0 += (LS_BB / 32) * GPW) {
-        const int i = i0 + (int)(threadIdx.x & 31) / TPR;
+    const int sub = (int)(threadIdx.x & 31) / TPR;
+    int i0 = r0 + (int)(threadIdx.x >> 5) * GPW;
+    int i = i0 + sub;
+    int lo = 0, hi = 0;
+    if (i < r1) {
+        lo = P.indptr[i];
+        hi = P.indptr[i + 1];
+    }
+    for (; i0 < r1; i0 += STEP) {
+        // the next pass's row pointers and this row's own values are loaded ahead of the gathers
+        const int inext = i + STEP;
+        int lo_n = 0, hi_n = 0;
+        if (inext < r1) {
+            lo_n = P.indptr[inext];
+            hi_n = P.indptr[inext + 1];
+        }
+        decltype(pre(0)) pv{};
+        if (i < r1) pv = pre(i);
         F s = F(0);
-        if (i < r1) {
-            const int lo = P.indptr[i], hi = P.indptr[i + 1];
-            for (int base = lo + lane; base < hi; base += U * TPR) {
-                int c[U];
-                V v[U];
-                F xv[U];
+        for (int base = lo + lane; base < hi; base += U * TPR) {
+            int c[U];
+            V v[U];
+            F xv[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int q = base + u * TPR;
-                    c[u] = q < hi ? __ldcs(&P.indices[q]) : 0;
-                    v[u] = q < hi ? __ldcs(&A[q]) : V(0);
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u) xv[u] = base + u * TPR < hi ? g(c[u]) : F(0);
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (base + u * TPR < hi) s += (F)v[u] * xv[u];
+            for (int u = 0; u < U; ++u) {
+                const int q = base + u * TPR;
+                c[u] = q < hi ? __ldcs(&P.indices[q]) : 0;
+                v[u] = q < hi ? __ldcs(&A[q]) : V(0);
             }
+#pragma unroll
+            for (int u = 0; u < U; ++u) xv[u] = base + u * TPR < hi ? g(c[u]) : F(0);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (base + u * TPR < hi) s += (F)v[u] * xv[u];
         }
 #pragma unroll
         for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
-        if (lane == 0 && i < r1) out(i, s);
+        if (lane == 0 && i < r1) out(i, s, pv);
+        i = inext;
+        lo = lo_n;
+        hi = hi_n;
     }
 }
 
@@ -870,8 +886,8 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
 // (two buffers, one barrier per window) and each row is summed in order by one thread.
 static constexpr int LS_NPT = 4, LS_W = LS_BB * LS_NPT;
 
-template <class V, class F, class Gather, class Out>
-__device__ __forceinline__ void ls_windows(const BProb &P, const V *A, int w0, int w1, Gather g, Out out)
+template <class V, class F, class Gather, class Pre, class Out>
+__device__ __forceinline__ void ls_windows(const BProb &P, const V *A, int w0, int w1, Gather g, Pre pre, Out out)
 {
     __shared__ F prod[2][LS_W];
     const int tid = (int)threadIdx.x;
@@ -907,25 +923,25 @@ __device__ __forceinline__ void ls_windows(const BProb &P, const V *A, int w0, i
             }
             F s = F(0);
             for (int q = lo; q < hi; ++q) s += pb[q - qs];
-            out(row, s);
+            out(row, s, pre(row));
         }
     }
 }
 
 // y = A g over an entry: by windows when the member has a window table, else by row groups
-template <class V, class F, class Gather, class Out>
-__device__ __forceinline__ void ls_spmv_entry(const BProb &P, const V *A, const LBlock &L, Gather g, Out out)
+template <class V, class F, class Gather, class Pre, class Out>
+__device__ __forceinline__ void ls_spmv_entry(const BProb &P, const V *A, const LBlock &L, Gather g, Pre pre, Out out)
 {
     if (P.wrow) {
-        ls_windows<V, F>(P, A, L.w0, L.w1, g, out);
+        ls_windows<V, F>(P, A, L.w0, L.w1, g, pre, out);
         return;
     }
     switch (P.tpr) {
-    case 2: ls_rows<2, V, F>(P, A, L.r0, L.r1, g, out); break;
-    case 4: ls_rows<4, V, F>(P, A, L.r0, L.r1, g, out); break;
-    case 8: ls_rows<8, V, F>(P, A, L.r0, L.r1, g, out); break;
-    case 16: ls_rows<16, V, F>(P, A, L.r0, L.r1, g, out); break;
-    default: ls_rows<32, V, F>(P, A, L.r0, L.r1, g, out); break;
+    case 2: ls_rows<2, V, F>(P, A, L.r0, L.r1, g, pre, out); break;
+    case 4: ls_rows<4, V, F>(P, A, L.r0, L.r1, g, pre, out); break;
+    case 8: ls_rows<8, V, F>(P, A, L.r0, L.r1, g, pre, out); break;
+    case 16: ls_rows<16, V, F>(P, A, L.r0, L.r1, g, pre, out); break;
+    default: ls_rows<32, V, F>(P, A, L.r0, L.r1, g, pre, out); break;
     }
 }
 
@@ -984,9 +1000,10 @@ __device__ __forceinline__ void ls_finish(LState &S, int *active)
 }
 
 // SpMV with the direction formed on the fly: p = z + beta pold (pold = 0 at the start); p.Ap.
-// Block 0 also empties the reliable-update list of the iteration.
+// Block 0 also empties the reliable-update list of the iteration.  At most 51 registers: 5
+// blocks per SM (with the loads issued ahead, 60 registers and 4 blocks ran 14 % slower).
 template <bool MIXED>
-__global__ void __launch_bounds__(LS_BB) k_ls_spmv(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
+__global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
                                                    LState *st, double *part, int *active, int *ru_count)
 {
     using F = typename std::conditional<MIXED, float, double>::type;
@@ -1007,9 +1024,8 @@ __global__ void __launch_bounds__(LS_BB) k_ls_spmv(const BProb *__restrict__ pro
     F *pnew = (it & 1) ? pb : pa;
     double dot = 0.0;
     ls_spmv_entry<F, F>(
-        P, A, L, [&](int j) { return pdir(z, pold, beta, j); },
-        [&](int i, F s) {
-            const F pi = pdir(z, pold, beta, i);
+        P, A, L, [&](int j) { return pdir(z, pold, beta, j); }, [&](int i) { return pdir(z, pold, beta, i); },
+        [&](int i, F s, F pi) {
             pnew[i] = pi;
             Ap[i] = s;
             dot += (double)pi * (double)s;
@@ -1110,7 +1126,7 @@ __global__ void __launch_bounds__(LS_BB) k_ls_flush(const BProb *__restrict__ pr
 // member's decisions.  MODE 0: the start (also ||b||, pold = 0, d = 0), every entry; MODE 1: a
 // reliable update (mixed), the listed entries; MODE 2: the final true residual, every entry.
 template <bool MIXED, int MODE>
-__global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
+__global__ void __launch_bounds__(LS_BB, 5) k_ls_resid(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
                                                     LState *st, double *part, int *active, const int *ru_list,
                                                     const int *ru_count)
 {
@@ -1128,17 +1144,18 @@ __global__ void __launch_bounds__(LS_BB) k_ls_resid(const BProb *__restrict__ pr
         double v[3] = {0.0, 0.0, 0.0};
         ls_spmv_entry<double, double>(
             P, P.A64, L, [&](int j) { return x[j]; },
-            [&](int i, double s) {
-                const double bi = P.b[i], ri = bi - s;
+            [&](int i) { return make_double2(P.b[i], MODE == 2 ? 0.0 : P.inv64[i]); },
+            [&](int i, double s, double2 own) {
+                const double bi = own.x, ri = bi - s;
                 v[0] += ri * ri;
                 if (MODE != 2) {
                     if (MIXED) {
-                        const float rf = (float)ri, zf = (float)P.inv64[i] * rf;
+                        const float rf = (float)ri, zf = (float)own.y * rf;
                         P.r32[i] = rf;
                         P.z32[i] = zf;
                         v[1] += (double)rf * (double)zf;
                     } else {
-                        const double zi = P.inv64[i] * ri;
+                        const double zi = own.y * ri;
                         P.r64[i] = ri;
                         P.z64[i] = zi;
                         v[1] += ri * zi;
