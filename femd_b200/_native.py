@@ -93,6 +93,7 @@ SIGNATURES = {
     "femd_cuda_batch_remove": (_I, [_P, _I]),
     "femd_cuda_batch_arm": (_I, [_P, _I, _P, _P, _I, _D]),
     "femd_cuda_batch_step": (_I, [_P, _P, _I, _I, _PI, _PI, C.POINTER(femd_cg_result)]),
+    "femd_cuda_lagrange_numbering": (_I, [_P, _I, _I, _P, _I, _I, _P, _PI, _PI]),
     "femd_host_rectangle_mesh": (_I, [_D, _D, _D, _D, _I, _I, _P, _P]),
     "femd_host_lagrange_numbering": (_I, [_I, _I, _P, _I, _I, _P, _PI, _PI]),
     "femd_host_triangle_quadrature": (_I, [_I, _P, _P, _P]),

@@ -221,22 +221,39 @@ class LagrangeSpace2D:
     """Continuous P_k on a triangle mesh; bc="dirichlet" eliminates every exterior node
     (python/femd/spaces2d.py:113-152, include/femd/fe/space_2d.hpp:390-526)."""
 
-    def __init__(self, mesh: Mesh2D, degree: int, bc: str = "free"):
+    def __init__(self, mesh: Mesh2D, degree: int, bc: str = "free", *, numbering: str = "host"):
+        """numbering: "host" (C++ on the host) or "device" (femd_cuda_lagrange_numbering on the
+        GPU; the same map, and the dofs stay on the device as well)."""
         if bc not in ("free", "dirichlet"):
             raise ValueError(f"LagrangeSpace2D: bc is 'free' or 'dirichlet' (every exterior side), got {bc!r}")
+        if numbering not in ("host", "device"):
+            raise ValueError(f"LagrangeSpace2D: numbering is 'host' or 'device', got {numbering!r}")
         k = int(degree)
         if k < 1:
             raise ValueError("LagrangeSpace2D: degree must be >= 1 (P0 is a DG space)")
         self.mesh, self.degree, self.bc = mesh, k, bc
         self.nloc = (k + 1) * (k + 2) // 2
-        self.cell_dofs = np.empty((mesh.ncells, self.nloc), dtype=np.int32)
-        dim, raw = C.c_int(), C.c_int()
-        check(lib.femd_host_lagrange_numbering(mesh.nverts, mesh.ncells, _np_ptr(mesh.tris), k, int(bc == "dirichlet"),
-                                               _np_ptr(self.cell_dofs), C.byref(dim), C.byref(raw)))
-        self.dim, self.raw_dim = dim.value, raw.value
         self._caches = {}
         self._pattern = None
         self._dofs_dev = None
+        dim, raw = C.c_int(), C.c_int()
+        if numbering == "device":
+            torch = _torch()
+            ctx = context()
+            _, tris = mesh.device(ctx)
+            dofs = torch.empty((mesh.ncells, self.nloc), dtype=torch.int32, device=f"cuda:{ctx.device}")
+            ctx.enter()
+            st = lib.femd_cuda_lagrange_numbering(ctx.h, mesh.nverts, mesh.ncells, tris.data_ptr(), k,
+                                                  int(bc == "dirichlet"), dofs.data_ptr(), C.byref(dim), C.byref(raw))
+            ctx.leave()
+            check(st)
+            self._dofs_dev = dofs
+            self.cell_dofs = dofs.cpu().numpy()
+        else:
+            self.cell_dofs = np.empty((mesh.ncells, self.nloc), dtype=np.int32)
+            check(lib.femd_host_lagrange_numbering(mesh.nverts, mesh.ncells, _np_ptr(mesh.tris), k, int(bc == "dirichlet"),
+                                                   _np_ptr(self.cell_dofs), C.byref(dim), C.byref(raw)))
+        self.dim, self.raw_dim = dim.value, raw.value
 
     def cache(self, degree: int) -> Cache2D:
         c = self._caches.get(degree)

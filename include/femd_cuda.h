@@ -332,6 +332,15 @@ FEMD_API int femd_cuda_batch_debug(femd_batch B, int ghost_member, long long spi
  * reference counterpart. */
 FEMD_API int femd_cuda_batch_profile(femd_batch B, long long *cycles_out);
 
+/* The same numbering on the device (replaces the host setup of LagrangeSpace2D,
+ * include/femd/fe/space_2d.hpp:390-526 -- build_edges / build_dofs / number): tris_dev is the
+ * mesh's ncells x 3 vertex indices in device memory, cell_dofs_dev receives ncells x nloc dofs
+ * (-1: eliminated), identical to femd_host_lagrange_numbering's.  Rejects meshes with a vertex
+ * that is the smaller end of more than 512 edges (FEMD_EINVAL; the host numbering takes them).
+ * Synchronises the context's stream. */
+FEMD_API int femd_cuda_lagrange_numbering(femd_ctx ctx, int nverts, int ncells, const int *tris_dev, int k, int all_exterior,
+                                          int *cell_dofs_dev, int *dim, int *raw_dim);
+
 /* ======================================================================================
  * Host-side setup of the synthetic problems (the reference's own setup code runs on the
  * host too).  No GPU work.
