@@ -668,3 +668,193 @@ int or_cg_jacobi(int n, const int *indptr, const int *indices, const double *v, 
     free(r); free(p); free(Ap);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------------------
+ * ILU(0) and SSOR preconditioned CG (the preconditioners beyond Jacobi, natural ordering).
+ * ILU(0): Saad's IKJ variant (Iterative Methods for Sparse Linear Systems, 2nd ed., Alg.
+ * 10.4) on the matrix's own pattern in row order, the factorization sparse/precond.hpp:151-183
+ * builds (unit lower L below the diagonal, U on and above it, in one array); its solve is the
+ * forward then backward substitution of precond.hpp:185-200.  SSOR with relaxation w:
+ * M = w/(2-w) (D/w + L) (D/w)^-1 (D/w + U), applied as precond.hpp:116-147 does (forward
+ * sweep, diagonal scaling, backward sweep).  The CG loop is the generic preconditioned CG of
+ * krylov/cg.hpp:245-293 with the ordered reductions above.  Rows must have sorted columns.
+ * ------------------------------------------------------------------------------------- */
+
+/* the diagonal position of every row; -1 on success, else the first row whose diagonal is
+ * missing or zero (the reference's diagonal check, precond.hpp:69-79) */
+int or_diag_positions(int n, const int *indptr, const int *indices, const double *v, int *diag)
+{
+    for (int i = 0; i < n; ++i)
+    {
+        diag[i] = -1;
+        for (int p = indptr[i]; p < indptr[i + 1]; ++p)
+            if (indices[p] == i) { diag[i] = p; break; }
+        if (diag[i] < 0 || v[diag[i]] == 0.0) return i;
+    }
+    return -1;
+}
+
+/* lu: the factors (nnz doubles), diag: diagonal positions.  Returns -1 on success, the row of
+ * a missing or zero diagonal, or -(2 + i) for a zero pivot in row i; *min_pivot: the smallest
+ * pivot met (negative: the factorization is indefinite). */
+int or_ilu0(int n, const int *indptr, const int *indices, const double *v, double *lu, int *diag, double *min_pivot)
+{
+    const long long nnz = indptr[n];
+    for (long long q = 0; q < nnz; ++q) lu[q] = v[q];
+    const int bad = or_diag_positions(n, indptr, indices, lu, diag);
+    if (bad >= 0) return bad;
+    int *where = (int *)malloc((size_t)n * sizeof(int));
+    if (!where) return -(2 + n);
+    for (int i = 0; i < n; ++i) where[i] = -1;
+    double mp = INFINITY;
+    for (int i = 0; i < n; ++i)
+    {
+        for (int p = indptr[i]; p < indptr[i + 1]; ++p) where[indices[p]] = p;
+        /* eliminate with every earlier row k this row reaches, in increasing k */
+        for (int p = indptr[i]; p < diag[i]; ++p)
+        {
+            const int k = indices[p];
+            lu[p] = lu[p] / lu[diag[k]];
+            const double l = lu[p];
+            for (int q = diag[k] + 1; q < indptr[k + 1]; ++q)
+            {
+                const int t = where[indices[q]];
+                if (t >= 0) lu[t] = lu[t] - l * lu[q];
+            }
+        }
+        for (int p = indptr[i]; p < indptr[i + 1]; ++p) where[indices[p]] = -1;
+        const double d = lu[diag[i]];
+        if (d == 0.0) { free(where); return -(2 + i); }
+        if (d < mp) mp = d;
+    }
+    free(where);
+    *min_pivot = mp;
+    return -1;
+}
+
+/* z = (L U)^-1 r */
+void or_ilu0_apply(int n, const int *indptr, const int *indices, const double *lu, const int *diag, const double *r, double *z)
+{
+    for (int i = 0; i < n; ++i)
+    {
+        double s = r[i];
+        for (int p = indptr[i]; p < diag[i]; ++p) s = s - lu[p] * z[indices[p]];
+        z[i] = s;
+    }
+    for (int i = n - 1; i >= 0; --i)
+    {
+        double s = z[i];
+        for (int p = diag[i] + 1; p < indptr[i + 1]; ++p) s = s - lu[p] * z[indices[p]];
+        z[i] = s / lu[diag[i]];
+    }
+}
+
+/* z = M_SSOR(w)^-1 r */
+void or_ssor_apply(int n, const int *indptr, const int *indices, const double *v, const int *diag, double w, const double *r,
+                   double *z)
+{
+    for (int i = 0; i < n; ++i)
+    {
+        double s = r[i];
+        for (int p = indptr[i]; p < diag[i]; ++p) s = s - v[p] * z[indices[p]];
+        z[i] = s * w / v[diag[i]];
+    }
+    const double c = (2.0 - w) / w;
+    for (int i = 0; i < n; ++i) z[i] = z[i] * (c * v[diag[i]] / w);
+    for (int i = n - 1; i >= 0; --i)
+    {
+        double s = z[i];
+        for (int p = diag[i] + 1; p < indptr[i + 1]; ++p) s = s - v[p] * z[indices[p]];
+        z[i] = s * w / v[diag[i]];
+    }
+}
+
+/* x += alpha p, r -= alpha Ap; returns ||r||^2 in ordered chunks of eight lanes */
+static double or_update_plain_chunk(double *x, double *r, const double *p, const double *Ap, double alpha, size_t lo, size_t hi)
+{
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    size_t i = lo;
+    for (; i + 8 <= hi; i += 8)
+        for (int k = 0; k < 8; ++k)
+        {
+            r[i + k] = r[i + k] - alpha * Ap[i + k];
+            x[i + k] = x[i + k] + alpha * p[i + k];
+            s[k] += r[i + k] * r[i + k];
+        }
+    for (; i < hi; ++i)
+    {
+        r[i] -= alpha * Ap[i];
+        x[i] += alpha * p[i];
+        s[0] += r[i] * r[i];
+    }
+    return ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
+}
+
+static double or_update_plain(double *x, double *r, const double *p, const double *Ap, double alpha, size_t n)
+{
+    if (n <= OR_CHUNK) return or_update_plain_chunk(x, r, p, Ap, alpha, 0, n);
+    double s = 0.0;
+    for (size_t lo = 0; lo < n; lo += OR_CHUNK) s += or_update_plain_chunk(x, r, p, Ap, alpha, lo, lo + OR_CHUNK < n ? lo + OR_CHUNK : n);
+    return s;
+}
+
+/* CG preconditioned by ILU(0) (kind 0: lu, diag from or_ilu0) or SSOR (kind 1: diag, w).
+ * result as or_cg_jacobi's.  Returns 0, or -1 on allocation failure. */
+int or_cg_pc(int n, const int *indptr, const int *indices, const double *v, int kind, const double *lu, const int *diag,
+             double w, const double *b, double *x, int max_iter, double tol, double *result)
+{
+    const size_t N = (size_t)n;
+    int converged = 0, breakdown = 0, it = 0;
+    const double nb = sqrt(or_ddot(b, b, N));
+    if (nb == 0.0)
+    {
+        for (size_t i = 0; i < N; ++i) x[i] = 0.0;
+        result[0] = 1; result[1] = 0; result[2] = 0.0; result[3] = 0;
+        return 0;
+    }
+    double *r = (double *)malloc(N * sizeof(double)), *z = (double *)malloc(N * sizeof(double));
+    double *p = (double *)malloc(N * sizeof(double)), *Ap = (double *)malloc(N * sizeof(double));
+    if (!r || !z || !p || !Ap) { free(r); free(z); free(p); free(Ap); return -1; }
+#define OR_APPLY(in, out)                                                        \
+    do {                                                                         \
+        if (kind == 0) or_ilu0_apply(n, indptr, indices, lu, diag, in, out);     \
+        else or_ssor_apply(n, indptr, indices, v, diag, w, in, out);             \
+    } while (0)
+    or_spmv(n, indptr, indices, v, x, Ap);
+    for (size_t i = 0; i < N; ++i) r[i] = b[i] - Ap[i];
+    double rn = sqrt(or_ddot(r, r, N));
+    if (rn <= tol * nb)
+    {
+        result[0] = 1; result[1] = 0; result[2] = rn / nb; result[3] = 0;
+        free(r); free(z); free(p); free(Ap);
+        return 0;
+    }
+    OR_APPLY(r, z);
+    for (size_t i = 0; i < N; ++i) p[i] = z[i];
+    double rz = or_ddot(r, z, N);
+    while (it < max_iter)
+    {
+        if (!(rz > 0.0)) { breakdown = 1; break; }
+        or_spmv(n, indptr, indices, v, p, Ap);
+        const double pAp = or_ddot(p, Ap, N);
+        if (!(pAp > 0.0)) { breakdown = 1; break; }
+        const double alpha = rz / pAp;
+        rn = sqrt(or_update_plain(x, r, p, Ap, alpha, N));
+        ++it;
+        if (rn <= tol * nb) break;
+        OR_APPLY(r, z);
+        const double rz_new = or_ddot(r, z, N);
+        const double beta = rz_new / rz;
+        rz = rz_new;
+        for (size_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
+    }
+#undef OR_APPLY
+    or_spmv(n, indptr, indices, v, x, Ap);
+    for (size_t i = 0; i < N; ++i) r[i] = b[i] - Ap[i];
+    const double residual = sqrt(or_ddot(r, r, N)) / nb;
+    converged = !breakdown && residual <= tol * (1.0 + 1e-6) + 1e-15;
+    if (!converged && !breakdown && residual <= 10.0 * tol && it < max_iter) converged = 1;
+    result[0] = converged; result[1] = it; result[2] = residual; result[3] = breakdown;
+    free(r); free(z); free(p); free(Ap);
+    return 0;
+}

@@ -213,6 +213,61 @@ def cg_jacobi(indptr, indices, data, inv, b, x0=None, max_iter=None, tol=1e-10):
     return x, dict(converged=bool(res[0]), iterations=int(res[1]), residual=float(res[2]), breakdown=bool(res[3]))
 
 
+def ilu0(indptr, indices, data):
+    """ILU(0) on the matrix's pattern (ILU0Preconditioner, natural ordering): (lu, diag, min_pivot)."""
+    n = indptr.size - 1
+    lu = np.empty(int(indptr[-1]))
+    diag = np.empty(n, dtype=np.int32)
+    mp = C.c_double()
+    st = lib().or_ilu0(n, _p(_i32(indptr)), _p(_i32(indices)), _p(_f64(data)), _p(lu), _p(diag), C.byref(mp))
+    if st >= 0:
+        raise ValueError(f"ILU(0): zero diagonal entry in row {st}")
+    if st < -1:
+        raise RuntimeError(f"ILU(0): zero pivot in row {-st - 2}")
+    return lu, diag, mp.value
+
+
+def ilu0_apply(indptr, indices, lu, diag, r):
+    z = np.empty(indptr.size - 1)
+    lib().or_ilu0_apply(indptr.size - 1, _p(_i32(indptr)), _p(_i32(indices)), _p(_f64(lu)), _p(_i32(diag)), _p(_f64(r)), _p(z))
+    return z
+
+
+def diag_positions(indptr, indices, data):
+    diag = np.empty(indptr.size - 1, dtype=np.int32)
+    st = lib().or_diag_positions(indptr.size - 1, _p(_i32(indptr)), _p(_i32(indices)), _p(_f64(data)), _p(diag))
+    if st >= 0:
+        raise ValueError(f"SSOR: zero diagonal entry in row {st}")
+    return diag
+
+
+def ssor_apply(indptr, indices, data, diag, r, omega=1.0):
+    z = np.empty(indptr.size - 1)
+    lib().or_ssor_apply(indptr.size - 1, _p(_i32(indptr)), _p(_i32(indices)), _p(_f64(data)), _p(_i32(diag)),
+                        C.c_double(omega), _p(_f64(r)), _p(z))
+    return z
+
+
+def cg_pc(indptr, indices, data, b, kind, x0=None, max_iter=None, tol=1e-10, omega=1.0):
+    """CG preconditioned by ILU(0) (kind "ilu0") or SSOR (kind "ssor"), natural ordering
+    (krylov::cg with ILU0Preconditioner / SSORPreconditioner)."""
+    n = indptr.size - 1
+    x = np.zeros(n) if x0 is None else _f64(x0).copy()
+    max_iter = max(1000, 10 * n) if max_iter is None else int(max_iter)
+    if kind == "ilu0":
+        lu, diag, _ = ilu0(indptr, indices, data)
+        k = 0
+    elif kind == "ssor":
+        lu, diag, k = np.zeros(1), diag_positions(indptr, indices, data), 1
+    else:
+        raise ValueError(f"cg_pc: kind is 'ilu0' or 'ssor', got {kind!r}")
+    res = np.zeros(4)
+    if lib().or_cg_pc(n, _p(_i32(indptr)), _p(_i32(indices)), _p(_f64(data)), k, _p(_f64(lu)), _p(_i32(diag)),
+                      C.c_double(omega), _p(_f64(b)), _p(x), max_iter, C.c_double(tol), _p(res)):
+        raise MemoryError("oracle cg")
+    return x, dict(converged=bool(res[0]), iterations=int(res[1]), residual=float(res[2]), breakdown=bool(res[3]))
+
+
 # ---- quadrature degree of the reference's form compiler (forms.py:2487-2500) -----------------
 def qdeg(form, k):
     return max({"gradgrad": 2 * (k - 1), "helmholtz": 2 * k, "varcoef": 3 * k - 1, "rhs_data": 2 * k + 1,

@@ -15,6 +15,8 @@
 //   Cache2D::eval_multi         include/femd/fe/cache_2d.hpp:245            (a field f at points)
 //   JacobiPreconditioner        include/femd/sparse/precond.hpp:82
 //   krylov::cg_jacobi           include/femd/krylov/cg.hpp:296
+//   ILU0Preconditioner, SSORPreconditioner (natural ordering), krylov::cg with them
+//                               include/femd/sparse/precond.hpp:105-200, krylov/cg.hpp:245   (--pc)
 //   SparseCholesky              include/femd/sparse/cholesky.hpp:144        (the FP64 solution oracle)
 //   asymmetry                   include/femd/sparse/csr.hpp:632
 //
@@ -31,7 +33,7 @@
 //                         k = 1 + 0.5 sin(2 pi x) sin(2 pi y)
 //           poisson_vec   a = c grad.grad,            b read from --b (dim entries)
 //           heat          M = u v and K = grad.grad (both written), no solve
-//   options: --c <value> --tol <t> --f <file> --b <file> --nocg --chol --nodump
+//   options: --c <value> --tol <t> --f <file> --b <file> --nocg --chol --nodump --pc
 //            --time <reps> --cg-sample <iters> --full-first (the first timed step runs CG to convergence)
 #include "femd/mesh/structured.hpp"
 #include "femd/fe/lagrange_space_2d.hpp"
@@ -100,6 +102,7 @@ struct Opts {
     bool cg = true, chol = false, dumpall = true;
     int time_reps = 0, cg_sample = 0;
     bool full_first = false;
+    bool pc = false;                 // also ILU(0)- and SSOR-preconditioned CG
 };
 
 static std::vector<double> const_coeff(const Cache2D &Q, double v)
@@ -126,6 +129,7 @@ int main(int argc, char **argv)
         else if (a == "--time") o.time_reps = std::atoi(next().c_str());
         else if (a == "--cg-sample") o.cg_sample = std::atoi(next().c_str());
         else if (a == "--full-first") o.full_first = true;
+        else if (a == "--pc") o.pc = true;
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     const std::string &dir = o.out;
@@ -287,6 +291,33 @@ int main(int argc, char **argv)
         std::fprintf(meta, "t_cg %.6f\ncg_converged %d\ncg_iterations %d\ncg_residual %.17g\ncg_breakdown %d\n", t_cg,
                      r.converged ? 1 : 0, r.iterations, r.residual, r.breakdown ? 1 : 0);
         dump(dir, "x_cg", x);
+    }
+    if (o.pc)
+    {
+        // the ILU(0) and SSOR (omega 1) preconditioners on the natural ordering: one application
+        // to the fixed vector of the SpMV test, and CG preconditioned by each
+        auto op = [&K](const std::vector<double> &in, std::vector<double> &out) {
+            out.resize(static_cast<std::size_t>(K.nrows()));
+            K.apply(in.data(), out.data());
+        };
+        std::vector<double> xs(static_cast<std::size_t>(n));
+        for (int i = 0; i < n; ++i) xs[i] = 1.0 + 0.5 * std::sin(1.0 + 0.7 * i);
+        ILU0Preconditioner ilu(K);
+        SSORPreconditioner ssor(K, 1.0);
+        std::fprintf(meta, "ilu0_min_pivot %.17g\n", ilu.min_pivot());
+        const SparsePreconditioner *pcs[2] = {&ilu, &ssor};
+        const char *names[2] = {"ilu0", "ssor"};
+        for (int m = 0; m < 2; ++m)
+        {
+            std::vector<double> z;
+            (*pcs[m])(xs, z);
+            dump(dir, std::string(names[m]) + "_apply_y", z);
+            std::vector<double> x(static_cast<std::size_t>(n), 0.0);
+            krylov::CGResult r = krylov::cg(op, *pcs[m], x, b, maxiter, o.tol);
+            std::fprintf(meta, "%s_converged %d\n%s_iterations %d\n%s_residual %.17g\n%s_breakdown %d\n", names[m],
+                         r.converged ? 1 : 0, names[m], r.iterations, names[m], r.residual, names[m], r.breakdown ? 1 : 0);
+            dump(dir, std::string("x_") + names[m], x);
+        }
     }
     if (o.chol)
     {

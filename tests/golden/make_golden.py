@@ -30,6 +30,10 @@ CASES = {
     "p2_heat_n4": ("heat", 4, 2, [], None, None),
     "p2_varcoef_n16": ("varcoef_field", 16, 2, [], "f", 0),
     "c1_p3_poisson_n32": ("poisson_sin", 32, 3, [], None, None),
+    # with the ILU(0)- and SSOR-preconditioned CG of the same system (--pc)
+    "p2_poisson_pc_n16": ("poisson_sin", 16, 2, ["--pc"], None, None),
+    "p3_varcoef_pc_n6": ("varcoef_field", 6, 3, ["--pc"], "f", 5),
+    "p1_vec_pc_n20": ("poisson_vec", 20, 1, ["--c", "1.7", "--pc"], "b", 6),
 }
 
 INT_ARRAYS = ("tris", "cell_dofs", "cell_raw_dofs", "indptr", "indices", "scatter_map")

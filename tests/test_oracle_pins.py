@@ -105,6 +105,30 @@ def test_jacobi_and_cg_bit_exact(name):
     assert np.linalg.norm(x - xc) / np.linalg.norm(xc) < 1e-8
 
 
+@pytest.mark.parametrize("name", [n for n in GOLDEN_CASES if "_pc_" in n])
+def test_ilu0_ssor_and_preconditioned_cg_bit_exact(name):
+    """ILU(0) and SSOR (omega 1, natural ordering) applied to the fixed vector, and CG
+    preconditioned by each, against ILU0Preconditioner / SSORPreconditioner and krylov::cg."""
+    z, meta = golden(name)
+    ip, ix, data, rhs = z["indptr"], z["indices"], z["data"], z["rhs"]
+    n = ip.size - 1
+    xs = 1.0 + 0.5 * np.sin(1.0 + 0.7 * np.arange(n))
+    lu, diag, min_pivot = O.ilu0(ip, ix, data)
+    assert min_pivot == float(meta["ilu0_min_pivot"])
+    assert np.array_equal(O.ilu0_apply(ip, ix, lu, diag, xs), z["ilu0_apply_y"])
+    assert np.array_equal(O.ssor_apply(ip, ix, data, O.diag_positions(ip, ix, data), xs), z["ssor_apply_y"])
+    xc = z["x_chol"]
+    for kind in ("ilu0", "ssor"):
+        x, info = O.cg_pc(ip, ix, data, rhs, kind, tol=1e-10)
+        assert info["iterations"] == int(meta[kind + "_iterations"])
+        assert info["residual"] == float(meta[kind + "_residual"])
+        assert info["converged"] == bool(int(meta[kind + "_converged"]))
+        assert np.array_equal(x, z["x_" + kind])
+        assert np.linalg.norm(x - xc) / np.linalg.norm(xc) < 1e-8
+    # the stronger preconditioners take fewer iterations than Jacobi on these systems
+    assert int(meta["ilu0_iterations"]) < int(meta["cg_iterations"])
+
+
 def test_known_answers_from_reference_docs():
     # examples/example13.ipynb cells 3/7: P2 on rectangle_mesh(0,0,1,1,20,20): 800 triangles, 1521 unknowns
     pts, tris = O.rectangle_mesh(20)
