@@ -858,3 +858,98 @@ int or_cg_pc(int n, const int *indptr, const int *indices, const double *v, int 
     free(r); free(z); free(p); free(Ap);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------------------
+ * The coefficient evaluator, real values (Integrand, forms/integrand.hpp:33-45 instruction
+ * set, :47-66 checks, :300-342 run): a program of 4-integer instructions (op, out, a, b) over
+ * registers of one value per point; the result is the last instruction's register.  Each
+ * point is independent, so this evaluates point by point with nreg doubles of scratch.
+ * ------------------------------------------------------------------------------------- */
+enum { OR_CONST, OR_X, OR_Y, OR_NX, OR_NY, OR_INPUT, OR_ADD, OR_MUL, OR_POW, OR_SIN, OR_COS, OR_EXP, OR_LOG, OR_TANH,
+       OR_SQRT, OR_SINH, OR_COSH, OR_SECH, OR_ABS, OR_SIGN };
+
+/* 0 when the program is well formed, else a code: 1 bad length, 2 no register, 3 register,
+ * 4 constant, 5 input, 6 pow operands, 7 unknown instruction */
+int or_integrand_check(const int *code, int ncode, int nreg, int nconst, int ninput)
+{
+    if (ncode % 4 != 0) return 1;
+    if (nreg < 1) return 2;
+    for (int k = 0; k < ncode; k += 4)
+    {
+        const int op = code[k], out = code[k + 1], a = code[k + 2], b = code[k + 3];
+        if (out < 0 || out >= nreg) return 3;
+        if (op == OR_CONST && (a < 0 || a >= nconst)) return 4;
+        if (op == OR_INPUT && (a < 0 || a >= ninput)) return 5;
+        if ((op == OR_ADD || op == OR_MUL) && (a < 0 || a >= nreg || b < 0 || b >= nreg)) return 3;
+        if (op == OR_POW && (a < 0 || a >= nreg || b < 0 || b >= nconst)) return 6;
+        if (op >= OR_SIN && op <= OR_SIGN && (a < 0 || a >= nreg)) return 3;
+        if (op < 0 || op > OR_SIGN) return 7;
+    }
+    return 0;
+}
+
+/* sech z = 2 e / (1 + e^2) with e = exp(-|z|), which neither overflows nor loses the tail */
+static double or_sech(double z)
+{
+    const double e = exp(-fabs(z));
+    return 2.0 * e / (1.0 + e * e);
+}
+
+/* out[q] for npts points; inputs: ninput arrays of npts values (an array of pointers).
+ * Returns the check's code (nothing is written unless it is 0), or -1 on allocation failure. */
+int or_integrand_eval(const int *code, int ncode, int nreg, const double *consts, int nconst, const double *const *inputs,
+                      int ninput, const double *xs, const double *ys, const double *nx, const double *ny, long long npts,
+                      double *out)
+{
+    const int bad = or_integrand_check(code, ncode, nreg, nconst, ninput);
+    if (bad) return bad;
+    if (ncode == 0) return 1;
+    double *r = (double *)calloc((size_t)nreg, sizeof(double));   /* registers start at 0, as the reference's do */
+    if (!r) return -1;
+    const int result = code[ncode - 4 + 1];
+    for (long long q = 0; q < npts; ++q)
+    {
+        for (int k = 0; k < ncode; k += 4)
+        {
+            const int op = code[k], o = code[k + 1], a = code[k + 2], b = code[k + 3];
+            double v = 0.0;
+            switch (op)
+            {
+            case OR_CONST: v = consts[a]; break;
+            case OR_X: v = xs[q]; break;
+            case OR_Y: v = ys[q]; break;
+            case OR_NX: v = (a < 0 ? -1.0 : 1.0) * nx[q]; break;
+            case OR_NY: v = (a < 0 ? -1.0 : 1.0) * ny[q]; break;
+            case OR_INPUT: v = inputs[a][q]; break;
+            case OR_ADD: v = r[a] + r[b]; break;
+            case OR_MUL: v = r[a] * r[b]; break;
+            case OR_POW:
+            {
+                /* squares, reciprocals and square roots are exact operations, not pow */
+                const double n = consts[b];
+                if (n == 2.0) v = r[a] * r[a];
+                else if (n == -1.0) v = 1.0 / r[a];
+                else if (n == 0.5) v = sqrt(r[a]);
+                else v = pow(r[a], n);
+                break;
+            }
+            case OR_SIN: v = sin(r[a]); break;
+            case OR_COS: v = cos(r[a]); break;
+            case OR_EXP: v = exp(r[a]); break;
+            case OR_LOG: v = log(r[a]); break;
+            case OR_TANH: v = tanh(r[a]); break;
+            case OR_SQRT: v = sqrt(r[a]); break;
+            case OR_SINH: v = sinh(r[a]); break;
+            case OR_COSH: v = cosh(r[a]); break;
+            case OR_SECH: v = or_sech(r[a]); break;
+            case OR_ABS: v = fabs(r[a]); break;
+            case OR_SIGN: v = r[a] > 0.0 ? 1.0 : (r[a] < 0.0 ? -1.0 : 0.0); break;
+            default: break;
+            }
+            r[o] = v;
+        }
+        out[q] = r[result];
+    }
+    free(r);
+    return 0;
+}

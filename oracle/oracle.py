@@ -268,6 +268,28 @@ def cg_pc(indptr, indices, data, b, kind, x0=None, max_iter=None, tol=1e-10, ome
     return x, dict(converged=bool(res[0]), iterations=int(res[1]), residual=float(res[2]), breakdown=bool(res[3]))
 
 
+def integrand_eval(code, nreg, consts, inputs, xs=None, ys=None, nx=None, ny=None):
+    """Integrand(code, nreg, nconst, ninput).evaluate(...) on real values: code is (ninstr, 4)
+    int (op, out, a, b); inputs (ninput, npts).  Raises ValueError on a malformed program."""
+    code = _i32(code).reshape(-1)
+    consts = _f64(consts).reshape(-1)
+    inputs = [_f64(v) for v in inputs]
+    npts = max([v.size for v in inputs] + [0 if xs is None else np.asarray(xs).size, 0 if nx is None else np.asarray(nx).size])
+    ptrs = (C.c_void_p * max(len(inputs), 1))(*[v.ctypes.data for v in inputs])
+    arrs = [None if a is None else _f64(a) for a in (xs, ys, nx, ny)]
+    out = np.empty(npts)
+    f = lib().or_integrand_eval
+    f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                  C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p]
+    st = f(code.ctypes.data, code.size, int(nreg), consts.ctypes.data if consts.size else None, consts.size, ptrs,
+           len(inputs), *[None if a is None else a.ctypes.data for a in arrs], npts, out.ctypes.data)
+    if st == -1:
+        raise MemoryError("oracle integrand")
+    if st:
+        raise ValueError(f"Integrand: malformed program (check {st})")
+    return out
+
+
 # ---- quadrature degree of the reference's form compiler (forms.py:2487-2500) -----------------
 def qdeg(form, k):
     return max({"gradgrad": 2 * (k - 1), "helmholtz": 2 * k, "varcoef": 3 * k - 1, "rhs_data": 2 * k + 1,

@@ -9,7 +9,7 @@ when given the reference's matrix.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, golden
+from conftest import GOLDEN_CASES, INTEGRAND_CASES, golden
 from oracle import oracle as O
 
 FORM_ARGS = {
@@ -127,6 +127,31 @@ def test_ilu0_ssor_and_preconditioned_cg_bit_exact(name):
         assert np.linalg.norm(x - xc) / np.linalg.norm(xc) < 1e-8
     # the stronger preconditioners take fewer iterations than Jacobi on these systems
     assert int(meta["ilu0_iterations"]) < int(meta["cg_iterations"])
+
+
+@pytest.mark.parametrize("name", INTEGRAND_CASES)
+def test_integrand_programs_bit_exact(name):
+    """The coefficient evaluator (Integrand::evaluate, real values) on the convection term, a
+    variable coefficient and a program with every instruction, 1,000 points each."""
+    import os
+    from conftest import GOLDEN
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    kw = {}
+    if z["has_xy"]:
+        kw.update(xs=z["xs"], ys=z["ys"])
+    if z["has_normal"]:
+        kw.update(nx=z["nx"], ny=z["ny"])
+    out = O.integrand_eval(z["code"], int(z["nreg"]), z["consts"], list(z["inputs"]), **kw)
+    assert np.array_equal(out, z["out"])
+
+
+def test_integrand_rejects_malformed_programs():
+    with pytest.raises(ValueError):
+        O.integrand_eval([[6, 0, 0, 5]], 2, [], [np.zeros(3)])          # register out of range
+    with pytest.raises(ValueError):
+        O.integrand_eval([[0, 0, 1, 0]], 1, [1.0], [np.zeros(3)])       # constant out of range
+    with pytest.raises(ValueError):
+        O.integrand_eval([[42, 0, 0, 0]], 1, [], [np.zeros(3)])         # unknown instruction
 
 
 def test_known_answers_from_reference_docs():
