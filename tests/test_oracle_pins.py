@@ -9,7 +9,9 @@ when given the reference's matrix.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, INTEGRAND_CASES, golden
+from conftest import GOLDEN_CASES, INTEGRAND_CASES, PC_CASES, golden
+
+CASES = GOLDEN_CASES + PC_CASES
 from oracle import oracle as O
 
 FORM_ARGS = {
@@ -37,7 +39,7 @@ def _problem(z, meta):
     return O.problem(form, N, k, c=c, **kw), form, c
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", CASES)
 def test_integer_work_bit_exact(name):
     z, meta = golden(name)
     P, form, _ = _problem(z, meta)
@@ -51,7 +53,7 @@ def test_integer_work_bit_exact(name):
     assert np.array_equal(P["map"], z["scatter_map"])
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", CASES)
 def test_quadrature_and_tabulation(name):
     z, meta = golden(name)
     P, _, _ = _problem(z, meta)
@@ -61,7 +63,7 @@ def test_quadrature_and_tabulation(name):
     assert np.abs(P["ref"] - ref).max() <= 1e-13
 
 
-@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("name", CASES)
 def test_assembly(name):
     z, meta = golden(name)
     P, form, c = _problem(z, meta)
@@ -86,7 +88,7 @@ def test_assembly(name):
     assert O.asymmetry(P["indptr"], P["indices"], data) == pytest.approx(float(meta["asymmetry"]), abs=1e-17)
 
 
-@pytest.mark.parametrize("name", [n for n in GOLDEN_CASES if "heat" not in n])
+@pytest.mark.parametrize("name", [n for n in CASES if "heat" not in n])
 def test_jacobi_and_cg_bit_exact(name):
     z, meta = golden(name)
     ip, ix, data, rhs = z["indptr"], z["indices"], z["data"], z["rhs"]
@@ -105,7 +107,7 @@ def test_jacobi_and_cg_bit_exact(name):
     assert np.linalg.norm(x - xc) / np.linalg.norm(xc) < 1e-8
 
 
-@pytest.mark.parametrize("name", [n for n in GOLDEN_CASES if "_pc_" in n])
+@pytest.mark.parametrize("name", PC_CASES)
 def test_ilu0_ssor_and_preconditioned_cg_bit_exact(name):
     """ILU(0) and SSOR (omega 1, natural ordering) applied to the fixed vector, and CG
     preconditioned by each, against ILU0Preconditioner / SSORPreconditioner and krylov::cg."""
