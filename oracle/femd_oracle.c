@@ -423,8 +423,19 @@ int or_scatter_map(int ne, int nloc, const int *dofs, const int *indptr, const i
  * ref: nq x 3 nloc tabulation; w, Ji: per point (or_cache_points); coef: nterms arrays of
  * ne nq values.
  * ------------------------------------------------------------------------------------- */
+int or_assemble_matrix_v(int ne, int nloc, int nq, const double *ref, const int *var, const double *w, const double *Ji,
+                         int nterms, const int *a, const int *b, const double *const *coef, const int *map, double *data);
+
 int or_assemble_matrix(int ne, int nloc, int nq, const double *ref, const double *w, const double *Ji, int nterms,
                        const int *a, const int *b, const double *const *coef, const int *map, double *data)
+{
+    return or_assemble_matrix_v(ne, nloc, nq, ref, NULL, w, Ji, nterms, a, b, coef, map, data);
+}
+
+/* the same with a tabulation per entry variant (a facet cache's local edge): entry e reads
+ * ref + var[e] nq 3 nloc (var NULL: variant 0 for every entry) */
+int or_assemble_matrix_v(int ne, int nloc, int nq, const double *ref, const int *var, const double *w, const double *Ji,
+                         int nterms, const int *a, const int *b, const double *const *coef, const int *map, double *data)
 {
     double *RT = (double *)malloc((size_t)3 * nq * nloc * sizeof(double));
     double *Ke = (double *)malloc((size_t)nloc * nloc * sizeof(double));
@@ -433,7 +444,8 @@ int or_assemble_matrix(int ne, int nloc, int nq, const double *ref, const double
     {
         for (int m = 0; m < 3; ++m)
             for (int q = 0; q < nq; ++q)
-                or_row(ref + (size_t)q * 3 * nloc, Ji + 4 * ((size_t)e * nq + q), nloc, m, RT + ((size_t)m * nq + q) * nloc);
+                or_row(ref + ((size_t)(var ? var[e] : 0) * nq + q) * 3 * nloc, Ji + 4 * ((size_t)e * nq + q), nloc, m,
+                       RT + ((size_t)m * nq + q) * nloc);
         memset(Ke, 0, (size_t)nloc * nloc * sizeof(double));
         for (int t = 0; t < nterms; ++t)
             for (int q = 0; q < nq; ++q)
@@ -457,8 +469,18 @@ int or_assemble_matrix(int ne, int nloc, int nq, const double *ref, const double
 }
 
 /* assemble_vector_2d, assembly_2d.hpp:173-211 (one term per call, code a) */
+int or_assemble_vector_v(int ne, int nloc, int nq, const double *ref, const int *var, const double *w, const double *Ji, int a,
+                         const double *coef, const int *dofs, double *f);
+
 int or_assemble_vector(int ne, int nloc, int nq, const double *ref, const double *w, const double *Ji, int a,
                        const double *coef, const int *dofs, double *f)
+{
+    return or_assemble_vector_v(ne, nloc, nq, ref, NULL, w, Ji, a, coef, dofs, f);
+}
+
+/* the same with a tabulation per entry variant, as or_assemble_matrix_v */
+int or_assemble_vector_v(int ne, int nloc, int nq, const double *ref, const int *var, const double *w, const double *Ji, int a,
+                         const double *coef, const int *dofs, double *f)
 {
     double *r = (double *)malloc((size_t)nloc * sizeof(double)), *fe = (double *)malloc((size_t)nloc * sizeof(double));
     if (!r || !fe) { free(r); free(fe); return -1; }
@@ -470,7 +492,7 @@ int or_assemble_vector(int ne, int nloc, int nq, const double *ref, const double
             const size_t kq = (size_t)e * nq + q;
             const double s = w[kq] * coef[kq];
             if (s == 0.0) continue;
-            or_row(ref + (size_t)q * 3 * nloc, Ji + 4 * kq, nloc, a, r);
+            or_row(ref + ((size_t)(var ? var[e] : 0) * nq + q) * 3 * nloc, Ji + 4 * kq, nloc, a, r);
             for (int l = 0; l < nloc; ++l) fe[l] += s * r[l];
         }
         const int *d = dofs + (size_t)e * nloc;
@@ -952,4 +974,117 @@ int or_integrand_eval(const int *code, int ncode, int nreg, const double *consts
     }
     free(r);
     return 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * Exterior facets (ds) on a rectangle mesh (the next row f2).  The facet list of
+ * fe/space_2d.hpp:430-446 keeps, in (cell, local edge) order, every edge with no neighbour,
+ * with the marker of its boundary segment; on rectangle_mesh the segments carry the markers
+ * {bottom, right, top, left} of their side (mesh/structured.hpp:26-31, default {1, 2, 3, 4}).
+ * The facet cache of fe/cache_2d.hpp:126-184: Gauss-Legendre with max(1, (degree + 2) / 2)
+ * points along each edge, reference points (1 - t) a + t b at t = (node + 1) / 2 between the
+ * edge's reference vertices, mapped by the cell's affine map; weight gw len / 2; outward normal
+ * (dy, -dx) / len for a counter-clockwise cell; J^{-1} of the cell per point; the tabulation
+ * per local edge (3 x nq x 3 nloc).
+ * ------------------------------------------------------------------------------------- */
+static int or_cmp_u64(const void *a, const void *b)
+{
+    const uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+    return (x > y) - (x < y);
+}
+
+static uint64_t or_edge_key(int a, int b)
+{
+    const uint64_t lo = (uint64_t)(a < b ? a : b), hi = (uint64_t)(a < b ? b : a);
+    return (lo << 32) | hi;
+}
+
+/* cell, local, marker: room for 3 ne entries.  Returns the number of exterior facets, or -1 on
+ * allocation failure. */
+int or_rect_exterior_facets(int ne, const int *tris, const double *pts, double x0, double y0, double x1, double y1,
+                            const int *markers, int *cell, int *local, int *marker)
+{
+    const size_t nh = (size_t)ne * 3;
+    uint64_t *keys = (uint64_t *)malloc(nh * sizeof(uint64_t));
+    if (!keys) return -1;
+    for (size_t t = 0; t < nh; ++t)
+    {
+        const size_t c = t / 3;
+        const int i = (int)(t % 3);
+        keys[t] = or_edge_key(tris[3 * c + (i + 1) % 3], tris[3 * c + (i + 2) % 3]);
+    }
+    qsort(keys, nh, sizeof(uint64_t), or_cmp_u64);
+    int nf = 0;
+    for (int c = 0; c < ne; ++c)
+        for (int i = 0; i < 3; ++i)
+        {
+            const int a = tris[3 * c + (i + 1) % 3], b = tris[3 * c + (i + 2) % 3];
+            const uint64_t k = or_edge_key(a, b);
+            size_t lo = 0, hi = nh;                          /* first key >= k */
+            while (lo < hi) { const size_t mid = (lo + hi) / 2; if (keys[mid] < k) lo = mid + 1; else hi = mid; }
+            const int count = (int)(lo + 1 < nh && keys[lo + 1] == k) + 1;
+            if (count != 1) continue;
+            const double ax = pts[2 * a], ay = pts[2 * a + 1], bx = pts[2 * b], by = pts[2 * b + 1];
+            int m = 0;
+            if (ay == y0 && by == y0) m = markers[0];
+            else if (ax == x1 && bx == x1) m = markers[1];
+            else if (ay == y1 && by == y1) m = markers[2];
+            else if (ax == x0 && bx == x0) m = markers[3];
+            cell[nf] = c; local[nf] = i; marker[nf] = m;
+            ++nf;
+        }
+    free(keys);
+    return nf;
+}
+
+/* x, y, w, nx, ny: nf nq; Ji: 4 nf nq; ref: 3 nq 3 nloc.  Returns nq (at most 64), or a
+ * negative status. */
+int or_facet_cache(int nf, const int *cell, const int *local, const double *pts, const int *tris, int k, int degree,
+                   double *x, double *y, double *w, double *nx, double *ny, double *Ji, double *ref)
+{
+    const int n = (degree + 2) / 2 > 1 ? (degree + 2) / 2 : 1;
+    if (n > 64) return -1;
+    double gx[64], gw[64];
+    or_gauss_legendre(n, gx, gw);
+    static const double vx[3] = {0.0, 1.0, 0.0}, vy[3] = {0.0, 0.0, 1.0};
+    double fx[3 * 64], fy[3 * 64];
+    const int nloc = (k + 1) * (k + 2) / 2;
+    for (int i = 0; i < 3; ++i)
+    {
+        const int a = (i + 1) % 3, b = (i + 2) % 3;
+        for (int q = 0; q < n; ++q)
+        {
+            const double t = 0.5 * (gx[q] + 1.0);
+            fx[i * n + q] = (1.0 - t) * vx[a] + t * vx[b];
+            fy[i * n + q] = (1.0 - t) * vy[a] + t * vy[b];
+        }
+        const int st = or_tabulate(k, n, fx + i * n, fy + i * n, ref + (size_t)i * n * 3 * nloc);
+        if (st < 0) return st;
+    }
+    for (int e = 0; e < nf; ++e)
+    {
+        const int c = cell[e], i = local[e];
+        const int *T = tris + 3 * c;
+        const double *P0 = pts + 2 * T[0], *P1 = pts + 2 * T[1], *P2 = pts + 2 * T[2];
+        double J[4];
+        J[0] = P1[0] - P0[0]; J[1] = P2[0] - P0[0];
+        J[2] = P1[1] - P0[1]; J[3] = P2[1] - P0[1];
+        const double *A = pts + 2 * T[(i + 1) % 3], *B = pts + 2 * T[(i + 2) % 3];
+        const double dx = B[0] - A[0], dy = B[1] - A[1], len = hypot(dx, dy);
+        for (int q = 0; q < n; ++q)
+        {
+            const size_t kq = (size_t)e * n + q;
+            const double xi = fx[i * n + q], eta = fy[i * n + q];
+            x[kq] = P0[0] + J[0] * xi + J[1] * eta;
+            y[kq] = P0[1] + J[2] * xi + J[3] * eta;
+            w[kq] = 0.5 * gw[q] * len;
+            nx[kq] = dy / len;
+            ny[kq] = -dx / len;
+            const double d = J[0] * J[3] - J[1] * J[2];
+            double *Jk = Ji + 4 * kq;
+            Jk[0] = J[3] / d; Jk[1] = -J[1] / d;
+            Jk[2] = -J[2] / d; Jk[3] = J[0] / d;
+        }
+    }
+    return n;
 }

@@ -156,6 +156,64 @@ def assemble_vector(n, ref, w, Ji, a, coef, dofs):
     return f
 
 
+def exterior_facets(pts, tris, bounds=(0.0, 0.0, 1.0, 1.0), markers=(1, 2, 3, 4)):
+    """The exterior facets of a rectangle mesh in (cell, local edge) order with the markers of
+    their sides {bottom, right, top, left}: (cell, local, marker)."""
+    pts, tris = _f64(pts), _i32(tris)
+    ne = tris.shape[0]
+    cell, local, marker = (np.empty(3 * ne, dtype=np.int32) for _ in range(3))
+    mk = np.asarray(markers, dtype=np.int32)
+    nf = lib().or_rect_exterior_facets(ne, _p(tris), _p(pts), *[C.c_double(v) for v in bounds], _p(mk), _p(cell),
+                                       _p(local), _p(marker))
+    if nf < 0:
+        raise MemoryError("oracle facets")
+    return cell[:nf].copy(), local[:nf].copy(), marker[:nf].copy()
+
+
+def facet_cache(pts, tris, cell, local, k, degree):
+    """The exterior-facet quadrature cache: x, y, w, nx, ny (nf nq), Ji (4 per point) and the
+    tabulation per local edge (3, nq, 3, nloc)."""
+    pts, tris, cell, local = _f64(pts), _i32(tris), _i32(cell), _i32(local)
+    nf = cell.size
+    nq = max(1, (degree + 2) // 2)
+    nloc = (k + 1) * (k + 2) // 2
+    x, y, w, nx, ny = (np.empty(nf * nq) for _ in range(5))
+    Ji = np.empty(4 * nf * nq)
+    ref = np.empty((3, nq, 3, nloc))
+    got = lib().or_facet_cache(nf, _p(cell), _p(local), _p(pts), _p(tris), k, degree, _p(x), _p(y), _p(w), _p(nx), _p(ny),
+                               _p(Ji), _p(ref))
+    if got != nq:
+        raise ValueError("oracle facet cache")
+    return dict(x=x, y=y, w=w, nx=nx, ny=ny, Ji=Ji, ref=ref, nq=nq)
+
+
+def assemble_matrix_v(nnz, ref, var, w, Ji, a, b, coefs, smap, into=None):
+    """assemble_matrix with a tabulation per entry variant: ref (nvar, nq, 3, nloc), var[e];
+    the element matrices are added onto a copy of `into` (default zeros), in entry order."""
+    ref, w, Ji = _f64(ref), _f64(w), _f64(Ji)
+    _, nq, _, nloc = ref.shape
+    ne = w.size // nq
+    coefs = [_f64(c) for c in coefs]
+    arr = (C.c_void_p * len(coefs))(*[c.ctypes.data for c in coefs])
+    data = np.zeros(nnz) if into is None else _f64(into).copy()
+    rc = lib().or_assemble_matrix_v(ne, nloc, nq, _p(ref), _p(_i32(var)), _p(w), _p(Ji), len(coefs), _p(_i32(a)),
+                                    _p(_i32(b)), arr, _p(_i32(smap)), _p(data))
+    if rc:
+        raise MemoryError("oracle assembly")
+    return data
+
+
+def assemble_vector_v(n, ref, var, w, Ji, a, coef, dofs, into=None):
+    ref, w, Ji, coef = _f64(ref), _f64(w), _f64(Ji), _f64(coef)
+    _, nq, _, nloc = ref.shape
+    ne = w.size // nq
+    f = np.zeros(n) if into is None else _f64(into).copy()
+    if lib().or_assemble_vector_v(ne, nloc, nq, _p(ref), _p(_i32(var)), _p(w), _p(Ji), int(a), _p(coef), _p(_i32(dofs)),
+                                  _p(f)):
+        raise MemoryError("oracle assembly")
+    return f
+
+
 def eval_field(ref, dofs, c):
     ref, c, dofs = _f64(ref), _f64(c), _i32(dofs)
     nq, _, nloc = ref.shape
@@ -305,14 +363,17 @@ def kcoef(x, y):
     return 1.0 + 0.5 * np.sin(2.0 * PI * x) * np.sin(2.0 * PI * y)
 
 
-def problem(form, N, k, c=1.0, f_dofs=None, b_vec=None):
+def problem(form, N, k, c=1.0, f_dofs=None, b_vec=None, free=False, robin=0.0, facet_ref=None):
     """The whole reference pipeline for one synthetic problem, on the CPU.
 
     form: "poisson_sin" | "helmholtz_sin" | "varcoef_field" | "poisson_vec" | "heat"
+    free: no Dirichlet elimination; robin: alpha of alpha u v ds, with g v ds (g = 1 + x y) added
+    to the load, over every exterior facet (ds degrees 2k and k + 2); facet_ref: the facet
+    tabulation to use for the ds matrix (default: this oracle's).
     Returns a dict with pts, tris, dofs, dim, indptr, indices, map, data, rhs (and data_K for heat).
     """
     pts, tris = rectangle_mesh(N)
-    dofs, raw, dim, raw_dim = lagrange_numbering(pts.shape[0], tris, k, True)
+    dofs, raw, dim, raw_dim = lagrange_numbering(pts.shape[0], tris, k, not free)
     ga = {"poisson_sin": "gradgrad", "poisson_vec": "gradgrad", "helmholtz_sin": "helmholtz",
           "varcoef_field": "varcoef", "heat": "mass"}[form]
     xi, eta, w = triangle_quadrature(qdeg(ga, k))
@@ -348,4 +409,17 @@ def problem(form, N, k, c=1.0, f_dofs=None, b_vec=None):
         out["rhs"] = assemble_vector(dim, reff, pw, pJ, 0, fc, dofs)
     else:
         out["rhs"] = _f64(b_vec)
+    if robin:
+        fcell, flocal, fmarker = exterior_facets(pts, tris)
+        fdofs = dofs[fcell]
+        fsmap = scatter_map(fdofs, indptr, indices)
+        Fa = facet_cache(pts, tris, fcell, flocal, k, 2 * k)
+        ra = Fa["ref"] if facet_ref is None else facet_ref
+        out["data"] = assemble_matrix_v(nnz, ra, flocal, Fa["w"], Fa["Ji"], [0], [0], [robin * np.ones(Fa["w"].size)], fsmap,
+                                        into=out["data"])
+        Fb = facet_cache(pts, tris, fcell, flocal, k, k + 2)
+        out["rhs"] = assemble_vector_v(dim, Fb["ref"], flocal, Fb["w"], Fb["Ji"], 0, 1.0 + Fb["x"] * Fb["y"], fdofs,
+                                       into=out["rhs"])
+        out["facets"] = (fcell, flocal, fmarker)
+        out["facet_cache"] = Fa
     return out

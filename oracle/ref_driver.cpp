@@ -15,6 +15,7 @@
 //   Cache2D::eval_multi         include/femd/fe/cache_2d.hpp:245            (a field f at points)
 //   JacobiPreconditioner        include/femd/sparse/precond.hpp:82
 //   krylov::cg_jacobi           include/femd/krylov/cg.hpp:296
+//   Cache2D(V, degree, {}, true)  include/femd/fe/cache_2d.hpp:126   (exterior facets, ds; --robin)
 //   ILU0Preconditioner, SSORPreconditioner (natural ordering), krylov::cg with them
 //                               include/femd/sparse/precond.hpp:105-200, krylov/cg.hpp:245   (--pc)
 //   SparseCholesky              include/femd/sparse/cholesky.hpp:144        (the FP64 solution oracle)
@@ -34,6 +35,8 @@
 //           poisson_vec   a = c grad.grad,            b read from --b (dim entries)
 //           heat          M = u v and K = grad.grad (both written), no solve
 //   options: --c <value> --tol <t> --f <file> --b <file> --nocg --chol --nodump --pc
+//            --free (no Dirichlet elimination) --robin <alpha> (adds alpha u v ds to A and
+//            g v ds to b, g = 1 + x y, over every exterior facet; ds degrees 2k and k + 2)
 //            --time <reps> --cg-sample <iters> --full-first (the first timed step runs CG to convergence)
 #include "femd/mesh/structured.hpp"
 #include "femd/fe/lagrange_space_2d.hpp"
@@ -103,6 +106,8 @@ struct Opts {
     int time_reps = 0, cg_sample = 0;
     bool full_first = false;
     bool pc = false;                 // also ILU(0)- and SSOR-preconditioned CG
+    bool free_bc = false;            // LagrangeSpace2D(m, k, {}, false)
+    double robin = 0.0;              // alpha of alpha u v ds (0: no facet terms)
 };
 
 static std::vector<double> const_coeff(const Cache2D &Q, double v)
@@ -130,6 +135,8 @@ int main(int argc, char **argv)
         else if (a == "--cg-sample") o.cg_sample = std::atoi(next().c_str());
         else if (a == "--full-first") o.full_first = true;
         else if (a == "--pc") o.pc = true;
+        else if (a == "--free") o.free_bc = true;
+        else if (a == "--robin") o.robin = std::atof(next().c_str());
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     const std::string &dir = o.out;
@@ -145,7 +152,7 @@ int main(int argc, char **argv)
     // ---- setup: mesh, space (numbering), caches, pattern, scatter map ----------------------
     double t0 = now();
     Mesh2D mesh = rectangle_mesh(0.0, 0.0, 1.0, 1.0, N, N);
-    LagrangeSpace2D V(mesh, k, {}, true);
+    LagrangeSpace2D V(mesh, k, {}, !o.free_bc);
     double t_space = now() - t0;
     int qa, qf = 0;
     bool rhs_data = false, rhs_field = false, rhs_vec = false;
@@ -199,6 +206,24 @@ int main(int argc, char **argv)
         std::vector<double> qw;
         for (int q = 0; q < rule.size(); ++q) qw.push_back(rule.weight(q));
         dump(dir, "quad_xi_a", qx); dump(dir, "quad_eta_a", qy); dump(dir, "quad_w_a", qw);
+        if (o.robin != 0.0)
+        {
+            // the exterior-facet cache of the ds matrix term: entries (cell, local edge, marker),
+            // points, weights, outward normals, and the tabulation per local edge
+            Cache2D Fa(V, 2 * k, {}, true);
+            std::vector<int> fc, fv;
+            for (int e = 0; e < Fa.nent(); ++e) { fc.push_back(Fa.cell(e)); fv.push_back(Fa.variant(e)); }
+            dump(dir, "facet_cell", fc);
+            dump(dir, "facet_local", fv);
+            dump(dir, "facet_marker", Fa.markers());
+            dump(dir, "facet_x", Fa.x()); dump(dir, "facet_y", Fa.y()); dump(dir, "facet_w", Fa.weights());
+            dump(dir, "facet_nx", Fa.normal_x()); dump(dir, "facet_ny", Fa.normal_y());
+            std::vector<double> fr;
+            for (int v = 0; v < 3; ++v)
+                for (int q = 0; q < Fa.nq(); ++q) { const double *R = Fa.ref(v, q); fr.insert(fr.end(), R, R + 3 * V.nloc()); }
+            dump(dir, "facet_ref", fr);
+            std::fprintf(meta, "facet_nq %d\nfacet_nent %d\nrobin %.17g\n", Fa.nq(), Fa.nent(), o.robin);
+        }
     }
 
     // ---- numeric assembly ------------------------------------------------------------------
@@ -250,6 +275,19 @@ int main(int argc, char **argv)
             assemble_vector_2d(Qf, {0}, {fc}, b);
         }
         else if (rhs_vec) b = load<double>(o.bpath, static_cast<std::size_t>(n));
+        if (o.robin != 0.0)
+        {
+            // alpha u v ds and g v ds over every exterior facet (Cache2D on facets)
+            Cache2D Fa(V, 2 * k, {}, true), Fb(V, k + 2, {}, true);
+            std::vector<int> fmap = scatter_map_2d(Fa, Fa, *P, 0, 0);
+            auto al = const_coeff(Fa, o.robin);
+            assemble_matrix_2d(Fa, Fa, {0}, {0}, {al}, K, 0, 0, fmap.data());
+            const std::size_t np = static_cast<std::size_t>(Fb.nent()) * Fb.nq();
+            std::vector<double> g(np);
+            for (std::size_t p = 0; p < np; ++p) g[p] = 1.0 + Fb.x()[p] * Fb.y()[p];
+            if (b.size() != static_cast<std::size_t>(n)) b.assign(static_cast<std::size_t>(n), 0.0);
+            assemble_vector_2d(Fb, {0}, {g}, b);
+        }
     };
 
     CSRMatrix K(P), K2(P);

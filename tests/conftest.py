@@ -26,6 +26,7 @@ def golden(name):
 # the assembled-problem fixtures; those with "_pc_" also hold the ILU(0)/SSOR-preconditioned CG
 # and pin the oracle only (the GPU tests run over GOLDEN_CASES)
 _ALL = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("integrand_"))
-GOLDEN_CASES = [n for n in _ALL if "_pc_" not in n]
+GOLDEN_CASES = [n for n in _ALL if "_pc_" not in n and "_ds_" not in n]
 PC_CASES = [n for n in _ALL if "_pc_" in n]
+DS_CASES = [n for n in _ALL if "_ds_" in n]     # free space with ds (Robin) terms: oracle only
 INTEGRAND_CASES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz") and f.startswith("integrand_"))

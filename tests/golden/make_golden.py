@@ -34,9 +34,14 @@ CASES = {
     "p2_poisson_pc_n16": ("poisson_sin", 16, 2, ["--pc"], None, None),
     "p3_varcoef_pc_n6": ("varcoef_field", 6, 3, ["--pc"], "f", 5),
     "p1_vec_pc_n20": ("poisson_vec", 20, 1, ["--c", "1.7", "--pc"], "b", 6),
+    # no Dirichlet elimination, alpha u v ds and g v ds on every exterior facet (--free --robin)
+    "p1_robin_ds_n6": ("poisson_sin", 6, 1, ["--free", "--robin", "2.5"], None, None),
+    "p2_robin_ds_n5": ("poisson_sin", 5, 2, ["--free", "--robin", "0.7"], None, None),
+    "p3_robin_ds_n4": ("poisson_sin", 4, 3, ["--free", "--robin", "4.0"], None, None),
 }
 
-INT_ARRAYS = ("tris", "cell_dofs", "cell_raw_dofs", "indptr", "indices", "scatter_map")
+INT_ARRAYS = ("tris", "cell_dofs", "cell_raw_dofs", "indptr", "indices", "scatter_map", "facet_cell", "facet_local",
+              "facet_marker")
 
 REF_INTEGRAND = os.path.join(ROOT, "oracle", "_ref", "femd_ref_integrand")
 TWO_PI = 6.283185307179586

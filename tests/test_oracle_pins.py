@@ -9,7 +9,7 @@ when given the reference's matrix.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, INTEGRAND_CASES, PC_CASES, golden
+from conftest import DS_CASES, GOLDEN_CASES, INTEGRAND_CASES, PC_CASES, golden
 
 CASES = GOLDEN_CASES + PC_CASES
 from oracle import oracle as O
@@ -129,6 +129,48 @@ def test_ilu0_ssor_and_preconditioned_cg_bit_exact(name):
         assert np.linalg.norm(x - xc) / np.linalg.norm(xc) < 1e-8
     # the stronger preconditioners take fewer iterations than Jacobi on these systems
     assert int(meta["ilu0_iterations"]) < int(meta["cg_iterations"])
+
+
+@pytest.mark.parametrize("name", DS_CASES)
+def test_facet_ds_assembly_bit_exact(name):
+    """A free space (no Dirichlet elimination) with alpha u v ds added to the stiffness matrix and
+    g v ds (g = 1 + x y) to the load over every exterior facet: the facet list, the facet
+    quadrature cache and the ds assembly against Cache2D(V, degree, {}, true) and
+    assemble_matrix_2d / assemble_vector_2d on it."""
+    z, meta = golden(name)
+    N, k, alpha = int(meta["N"]), int(meta["k"]), float(meta["robin"])
+    nloc = (k + 1) * (k + 2) // 2
+    nq = int(meta["facet_nq"])
+    fref = z["facet_ref"].reshape(3, nq, 3, nloc)
+    P = O.problem("poisson_sin", N, k, free=True, robin=alpha, facet_ref=fref)
+    fcell, flocal, fmarker = P["facets"]
+    assert np.array_equal(fcell, z["facet_cell"]) and np.array_equal(flocal, z["facet_local"])
+    assert np.array_equal(fmarker, z["facet_marker"])
+    F = P["facet_cache"]
+    for key in ("x", "y", "w", "nx", "ny"):
+        assert np.array_equal(F[key], z["facet_" + key]), key
+    assert np.allclose(F["ref"], fref, rtol=0, atol=1e-13)
+    assert np.array_equal(P["dofs"].ravel(), z["cell_dofs"]) and P["dim"] == int(meta["dim"])
+    assert np.array_equal(P["indptr"], z["indptr"]) and np.array_equal(P["indices"], z["indices"])
+    # the matrix with the reference's cell and facet tabulations: the same bits
+    xi, eta, w = P["quad"]
+    x, y, ww, Ji = O.cache_points(P["pts"], P["tris"], xi, eta, w)
+    nnz = int(P["indptr"][-1])
+    cell = O.assemble_matrix(nnz, z["ref_tab_a"].reshape(P["ref"].shape), ww, Ji, [1, 2], [1, 2], [np.ones(ww.size)] * 2,
+                             P["map"])
+    fsmap = O.scatter_map(P["dofs"][fcell], P["indptr"], P["indices"])
+    data = O.assemble_matrix_v(nnz, fref, flocal, F["w"], F["Ji"], [0], [0], [alpha * np.ones(F["w"].size)], fsmap, into=cell)
+    assert np.array_equal(data, z["data"])
+    # own tabulation: equal to rounding
+    big = np.abs(z["data"]).max()
+    assert np.all(np.abs(P["data"] - z["data"]) <= 1e-12 * np.abs(z["data"]) + 1e-15 * big)
+    rhs = z["rhs"]
+    assert np.all(np.abs(P["rhs"] - rhs) <= 1e-12 * np.abs(rhs) + 1e-15 * np.abs(rhs).max())
+    # the Robin problem is SPD: CG on the reference's system gives its iterates, and Cholesky's x
+    x_cg, info = O.cg_jacobi(z["indptr"], z["indices"], z["data"], O.jacobi_inverse(z["indptr"], z["indices"], z["data"]),
+                             rhs, tol=1e-10)
+    assert info["iterations"] == int(meta["cg_iterations"]) and np.array_equal(x_cg, z["x_cg"])
+    assert np.linalg.norm(x_cg - z["x_chol"]) <= 1e-8 * np.linalg.norm(z["x_chol"])
 
 
 @pytest.mark.parametrize("name", INTEGRAND_CASES)
