@@ -63,6 +63,7 @@ SIGNATURES = {
     "femd_cuda_matrix_set_host": (_I, [_P, _P]),
     "femd_cuda_matrix_to_host": (_I, [_P, _P]),
     "femd_cuda_matrix_jacobi": (_I, [_P, _P]),
+    "femd_cuda_matrix_set_inv_diag": (_I, [_P, _P, _P]),
     "femd_cuda_matrix_inv_diag_to_host": (_I, [_P, _P]),
     "femd_cuda_assemble_matrix": (_I, [_P, C.POINTER(femd_mesh2d), C.POINTER(femd_rule), _P, _I, _P, _P,
                                        C.POINTER(femd_coef), _I, _P, _I]),

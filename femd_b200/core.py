@@ -591,8 +591,10 @@ def cg_solve(A: CSRMatrix, M, b, x0, max_iter: int, tol: float, *, mixed: bool =
     if M is not None and M.size != n:
         raise ValueError("krylov: preconditioner and right-hand side differ in size")
     if M is not None and M.K is not A:
-        # the preconditioner of another matrix: copy its inverse diagonal into A's slot
-        A.inv_tensor().copy_(M.K.inv_tensor())
+        # the preconditioner of another matrix: its inverse diagonal becomes A's
+        _, inv = M.K._arrays()
+        A.ctx.enter()
+        check(lib.femd_cuda_matrix_set_inv_diag(A.ctx.h, A.h, C.c_void_p(inv)))
         A._jacobi = True
     A.ctx.enter()
     res = N.femd_cg_result()

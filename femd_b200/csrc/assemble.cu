@@ -909,6 +909,7 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
             set_error("Jacobi: zero diagonal entry in row " + std::to_string(bad));
             return FEMD_EZERODIAG;
         }
+        K->inv_valid = true;
     }
     return FEMD_OK;
 }
@@ -968,6 +969,7 @@ int femd_cuda_assemble_matrix(femd_ctx ctx, const femd_mesh2d *mesh, const femd_
         set_error("Jacobi: zero diagonal entry in row " + std::to_string(bad));
         return FEMD_EZERODIAG;
     }
+    if (want_inv) K->inv_valid = true;
     return FEMD_OK;
 }
 

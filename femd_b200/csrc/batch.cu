@@ -394,7 +394,9 @@ __device__ __forceinline__ bool chunk_spmv(const BProb &P, const V *A, unsigned 
                     q->fail_team = P.team;
                     q->fail_rank = (int)par;
                 }
-                if (S.cid[b ^ 1] >= 0) mbar_wait(&S.mbar[b ^ 1], (par >> (b ^ 1)) & 1u);
+                // a copy that still has not landed may write this block's shared memory after it
+                // exits: recorded apart (3), and the host reports the context as suspect
+                if (S.cid[b ^ 1] >= 0 && !mbar_wait(&S.mbar[b ^ 1], (par >> (b ^ 1)) & 1u)) atomicExch(&q->fail_where, 3);
             }
             return false;
         }
@@ -1430,6 +1432,8 @@ static int add_member(femd_batch_s *B, femd_matrix K, int *id_out)
     FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "batch: the matrices must be square");
     FEMD_CHECK_ARG(K->pattern->nrows >= 1, "batch: empty matrix");
     FEMD_CHECK_ARG(K->pattern->nnz < INT_MAX, "batch: more than 2^31 nonzeros");
+    FEMD_CHECK_ARG(K->inv_valid, "batch: the matrix has no inverse diagonal; call JacobiPreconditioner first "
+                                 "(femd_cuda_matrix_jacobi, an assembly with want_inv, or femd_cuda_matrix_set_inv_diag)");
     int id = -1;
     for (size_t i = 0; i < B->mem.size(); ++i)
         if (!B->mem[i]) { id = (int)i; break; }
@@ -1658,6 +1662,11 @@ static int launch_set(femd_ctx ctx, femd_batch_s *B, std::vector<int> order, int
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (e != cudaSuccess) { set_error(std::string("batch: ") + cudaGetErrorString(e)); return FEMD_ECUDA; }
+    if (B->h_qout->fail_where == 3) {
+        set_error("batch: a staging copy had not landed when its block gave up and exited; the CUDA context may be "
+                  "unusable");
+        return FEMD_ECUDA;
+    }
     return FEMD_OK;
 }
 

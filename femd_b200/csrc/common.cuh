@@ -124,6 +124,10 @@ struct femd_matrix_s : femd::HandleBase {
     femd::DevBuf<double> data, inv;
     femd::DevBuf<float> data32, inv32;   // FP32 copies (mixed precision), built on demand
     bool f32_valid = false;
+    // the inverse diagonal has been written (assembly with want_inv, femd_cuda_matrix_jacobi,
+    // femd_cuda_matrix_set_inv_diag, or the host upload of femd_cuda_cg_solve_host); until then
+    // every preconditioned solve refuses the matrix instead of reading uninitialised memory
+    bool inv_valid = false;
     int spmv_tpr = 0;                    // autotuned threads per row (0: not tuned)
     // the solver workspace of this matrix (vectors, pinned state, captured CUDA graphs), kept
     // between solves so that a solve allocates nothing once it has run once

@@ -869,6 +869,11 @@ static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b_in, double *x_
 
 using namespace femd;
 
+// the error of a preconditioned solve on a matrix whose inverse diagonal was never written
+static const char *const JACOBI_MISSING =
+    "Jacobi: the matrix has no inverse diagonal; call JacobiPreconditioner first (femd_cuda_matrix_jacobi, "
+    "an assembly with want_inv, or femd_cuda_matrix_set_inv_diag)";
+
 static femd_matrix as_matrix(void *h)
 {
     femd_matrix m = static_cast<femd_matrix>(h);
@@ -952,6 +957,23 @@ int femd_cuda_matrix_jacobi(femd_ctx ctx, femd_matrix K)
         set_error("Jacobi: zero diagonal entry in row " + std::to_string(bad));
         return FEMD_EZERODIAG;
     }
+    K->inv_valid = true;
+    return FEMD_OK;
+}
+
+int femd_cuda_matrix_set_inv_diag(femd_ctx ctx, femd_matrix K, const double *inv_dev)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K, "Jacobi: NULL argument");
+    FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "Jacobi: the matrix must be square");
+    const int n = K->pattern->nrows;
+    FEMD_CHECK_ARG(n == 0 || inv_dev, "Jacobi: NULL inverse diagonal");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    if (n && inv_dev != K->inv.p)
+        FEMD_TRY_CUDA(cudaMemcpyAsync(K->inv.p, inv_dev, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    K->f32_valid = false;
+    K->inv_valid = true;
     return FEMD_OK;
 }
 
@@ -1092,6 +1114,7 @@ int femd_cuda_cg_jacobi(femd_ctx ctx, femd_matrix K, int use_jacobi, const doubl
     const int n = K->pattern->nrows;
     FEMD_CHECK_ARG(n == 0 || (b_dev && x_dev), "cg: NULL vector");
     FEMD_CHECK_ARG(max_iter >= 0, "cg: max_iter must be >= 0");
+    FEMD_CHECK_ARG(!use_jacobi || K->inv_valid, JACOBI_MISSING);
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
     *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
     if (n == 0) return FEMD_OK;
@@ -1107,6 +1130,7 @@ int femd_cuda_pcg_mixed(femd_ctx ctx, femd_matrix K, const double *b_dev, double
     FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "pcg_mixed: the matrix must be square");
     const int n = K->pattern->nrows;
     FEMD_CHECK_ARG(n == 0 || (b_dev && x_dev), "pcg_mixed: NULL vector");
+    FEMD_CHECK_ARG(K->inv_valid, JACOBI_MISSING);
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
     *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
     if (n == 0) return FEMD_OK;
@@ -1134,6 +1158,7 @@ int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host, const i
     if (!st) {
         if (nnz) e = cudaMemcpyAsync(K->data.p, data_host, (size_t)nnz * sizeof(double), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess && inv_host) e = cudaMemcpyAsync(K->inv.p, inv_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (inv_host) K->inv_valid = true;
         if (e == cudaSuccess) e = cudaMemcpyAsync(b.p, b_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) {
             if (x0_host) e = cudaMemcpyAsync(x.p, x0_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s);
@@ -1176,11 +1201,35 @@ static constexpr size_t NOALLOC_DOUBLES = 3 * (size_t)NOALLOC_MAX_ROWS + NOALLOC
 static __device__ __align__(256) double g_cg_scratch[NOALLOC_DOUBLES];
 
 static constexpr int NOALLOC_MAX_DEVICES = 64;
+// per device: the CUDA context the address was looked up in, and the address
+static void *g_cg_scratch_ctx[NOALLOC_MAX_DEVICES] = {};
 static double *g_cg_scratch_addr[NOALLOC_MAX_DEVICES] = {};
 static std::mutex g_cg_scratch_lock;
 
+// The driver's cuCtxGetCurrent, reached through the runtime (the library links no libcuda): the
+// key that tells a cached address from one of a context that has since been destroyed and made
+// again (after cudaDeviceReset the array lives at a new address in the new context).
+typedef int (*CtxGetCurrentFn)(void **);
+static CtxGetCurrentFn ctx_get_current()
+{
+    static CtxGetCurrentFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
 // The device address of g_cg_scratch on the current device (host code cannot use the symbol
-// itself: on the host it names a stand-in, not device memory).  Looked up once per device.
+// itself: on the host it names a stand-in, not device memory).  Looked up once per device and
+// CUDA context; the caller has made the device current.
 static int noalloc_scratch(int device, double **out)
 {
     if (device < 0 || device >= NOALLOC_MAX_DEVICES) {
@@ -1188,7 +1237,13 @@ static int noalloc_scratch(int device, double **out)
         return FEMD_EINVAL;
     }
     std::lock_guard<std::mutex> g(g_cg_scratch_lock);
-    if (!g_cg_scratch_addr[device]) {
+    void *cur = nullptr;
+    const CtxGetCurrentFn get = ctx_get_current();
+    if (!get || get(&cur) != 0 || !cur) {
+        set_error("cg_jacobi_noalloc: no current CUDA context on the device");
+        return FEMD_ECUDA;
+    }
+    if (!g_cg_scratch_addr[device] || g_cg_scratch_ctx[device] != cur) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_cg_scratch);
         if (e != cudaSuccess || !p) {
@@ -1196,6 +1251,7 @@ static int noalloc_scratch(int device, double **out)
             return FEMD_ECUDA;
         }
         g_cg_scratch_addr[device] = static_cast<double *>(p);
+        g_cg_scratch_ctx[device] = cur;
     }
     *out = g_cg_scratch_addr[device];
     return FEMD_OK;
@@ -1216,7 +1272,11 @@ int femd_cuda_cg_jacobi_noalloc(femd_ctx ctx, femd_matrix K, int use_jacobi, con
     FEMD_CHECK_ARG(n <= NOALLOC_MAX_ROWS, "cg_jacobi_noalloc: " + std::to_string(n) + " rows exceed the fixed scratch of " +
                                               std::to_string(NOALLOC_MAX_ROWS) + " rows; use femd_cuda_cg_jacobi");
     FEMD_CHECK_ARG(n == 0 || (b_dev && x_dev), "cg_jacobi_noalloc: NULL vector");
+    // the solve works on x in place and reads b every chunk: the two must not share memory
+    FEMD_CHECK_ARG(n == 0 || b_dev + n <= x_dev || x_dev + n <= b_dev,
+                   "cg_jacobi_noalloc: b and x overlap; pass separate vectors");
     FEMD_CHECK_ARG(max_iter >= 0, "cg_jacobi_noalloc: max_iter must be >= 0");
+    FEMD_CHECK_ARG(!use_jacobi || K->inv_valid, JACOBI_MISSING);
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
     *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
     if (n == 0) return FEMD_OK;

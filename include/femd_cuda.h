@@ -115,8 +115,17 @@ FEMD_API int femd_cuda_matrix_arrays(femd_matrix K, double **data_dev, double **
 FEMD_API int femd_cuda_matrix_set_host(femd_matrix K, const double *data_host);
 FEMD_API int femd_cuda_matrix_to_host(femd_matrix K, double *data_host);
 /* inv_diag = 1 / a_ii; FEMD_EZERODIAG with "Jacobi: zero diagonal entry in row i"
- * (precond.hpp:68-78) when some a_ii is 0 or missing. */
+ * (precond.hpp:68-78) when some a_ii is 0 or missing.
+ * A new matrix has no inverse diagonal: every preconditioned solve (femd_cuda_cg_jacobi with
+ * use_jacobi, femd_cuda_pcg_mixed, femd_cuda_cg_jacobi_noalloc with use_jacobi, femd_cuda_batch_add)
+ * returns FEMD_EINVAL until this call, an assembly with want_inv, or femd_cuda_matrix_set_inv_diag
+ * has written it.  Changing the values later does not refresh it (the reference's
+ * JacobiPreconditioner also keeps the diagonal of the matrix it was made from). */
 FEMD_API int femd_cuda_matrix_jacobi(femd_ctx ctx, femd_matrix K);
+/* Give K the inverse diagonal inv_dev (nrows device values, copied on the context's stream): the
+ * preconditioner of another matrix of the same size, as cg_solve(A, M, ...) accepts an M built from
+ * another matrix (python/src/femd_bindings.cpp:799-833).  No zero check. */
+FEMD_API int femd_cuda_matrix_set_inv_diag(femd_ctx ctx, femd_matrix K, const double *inv_dev);
 /* Copy of the inverse diagonal to the host (nrows); synchronizes. */
 FEMD_API int femd_cuda_matrix_inv_diag_to_host(femd_matrix K, double *inv_host);
 
@@ -237,9 +246,11 @@ FEMD_API int femd_cuda_pcg_mixed(femd_ctx ctx, femd_matrix K, const double *b_de
  * b and x as before; the solver's work vectors, reduction partials and state live in one fixed
  * static device array (about 25 MB, held by every GPU that loads the library until the process
  * exits) sized for at most 1,048,576 rows -- larger systems are rejected with FEMD_EINVAL.
- * The first call on a device looks up that array's device address; make it before any stream
+ * The first call on a device (and the first after the device's CUDA context was made again, e.g.
+ * after cudaDeviceReset) looks up that array's device address; make it before any stream
  * capture.  Every call shares the array: calls that overlap on the GPU (any stream or context
- * of the same device) race and must be serialized.  Same kernels and iterates as
+ * of the same device) race and must be serialized.  The solve updates x in place and reads b
+ * throughout, so b and x must not overlap (FEMD_EINVAL).  Same kernels and iterates as
  * femd_cuda_cg_jacobi; res->seconds is not measured (0). */
 FEMD_API int femd_cuda_cg_jacobi_noalloc(femd_ctx ctx, femd_matrix K, int use_jacobi, const double *b_dev, double *x_dev,
                                          int max_iter, double tol, femd_cg_result *res);
@@ -327,7 +338,8 @@ FEMD_API int femd_cuda_batch_debug(femd_batch B, int ghost_member, long long spi
 /* Counters of the last launch (cycles_out: 7 entries).  Cycles summed over the blocks (thread 0 of
  * each): [0] in the kernel, [1] waiting at team barriers, [2] waiting at the SpMV chunk barriers
  * -- their ratios show how much of a launch is synchronisation.  When a bounded wait gave up
- * (FEMD_ETIMEOUT): [3] which (1 a team barrier, 2 a staging copy), [4] the barrier phase or the
+ * (FEMD_ETIMEOUT): [3] which (1 a team barrier, 2 a staging copy, 3 a staging copy that had still
+ * not landed when its block exited -- the launch then returns FEMD_ECUDA), [4] the barrier phase or the
  * chunk, [5] the team size, [6] the barrier count seen (team) or the staging parity bits.  No
  * reference counterpart. */
 FEMD_API int femd_cuda_batch_profile(femd_batch B, long long *cycles_out);

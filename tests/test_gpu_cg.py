@@ -126,3 +126,38 @@ def test_assembled_solve_end_to_end(fb):
     assert abs(its - 228) <= 7
     xc = z["x_chol"]
     assert np.linalg.norm(x.cpu().numpy() - xc) / np.linalg.norm(xc) <= 1e-8
+
+
+def test_preconditioned_solves_refuse_a_matrix_without_inverse_diagonal(fb):
+    """A matrix whose inverse diagonal was never written (no JacobiPreconditioner, no assembly
+    with want_inv): the C ABI's preconditioned solves return FEMD_EINVAL instead of reading
+    uninitialised memory; the unpreconditioned solve runs.  femd_cuda_matrix_set_inv_diag gives
+    it the preconditioner of another matrix, as cg_solve(A, M) with M of another matrix does."""
+    import ctypes as C
+
+    import torch
+    z, _ = golden("p2_varcoef_n16")
+    K = _from_golden(fb, z)
+    n = K.nrows
+    b = torch.as_tensor(z["rhs"]).cuda()
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    res = fb._native.femd_cg_result()
+    args = (C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 1000, 1e-10, C.byref(res))
+    torch.cuda.synchronize()
+    for fn in (fb.lib.femd_cuda_cg_jacobi, fb.lib.femd_cuda_cg_jacobi_noalloc):
+        assert fn(K.ctx.h, K.h, 1, *args) == 1
+        assert b"call JacobiPreconditioner first" in fb.lib.femd_cuda_last_error()
+    assert fb.lib.femd_cuda_pcg_mixed(K.ctx.h, K.h, *args) == 1
+    bh = C.c_void_p()
+    assert fb.lib.femd_cuda_batch_create(K.ctx.h, 0, None, 0, C.byref(bh)) == 0
+    mid = C.c_int()
+    assert fb.lib.femd_cuda_batch_add(bh, K.h, C.byref(mid)) == 1
+    fb.lib.femd_cuda_release(bh)
+    assert fb.lib.femd_cuda_cg_jacobi(K.ctx.h, K.h, 0, *args) == 0 and res.converged
+    # the preconditioner of another matrix with the same values
+    K2 = _from_golden(fb, z)
+    M2 = fb.JacobiPreconditioner(K2)
+    xg, conv, its, r, brk = fb.cg_solve(K, M2, z["rhs"], None, 1000, 1e-10)
+    assert conv
+    x2, conv2, its2, *_ = fb.cg_solve(K2, M2, z["rhs"], None, 1000, 1e-10)
+    assert its == its2 and torch.equal(xg, x2)

@@ -16,6 +16,7 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(ROOT, "oracle", "_ref", "femd_ref_omp")
 N, K = 512, 2
+ERR_CONTRACT = 1e-8       # relative error of every solution against the FP64 Cholesky oracle
 
 
 @pytest.fixture(scope="module")
@@ -73,10 +74,12 @@ def test_config3_against_cholesky(case, tol):
     for k, (err, its, outer, ms) in out.items():
         print(f"config 3, tol {tol:g}, {k}: relative error vs FP64 Cholesky {err:.2e}, {its} iterations, "
               f"{outer} reliable updates, {ms:.1f} ms")
-    # the error of a solve to relative residual tol is about kappa tol; FP32 inner iteration with
-    # FP64 reliable updates reaches the same error as the FP64 solve
+    # the contract of the mixed-precision path: every result within 1e-8 relative of the FP64
+    # Cholesky oracle (the error of a solve to relative residual tol is about kappa tol, and at
+    # tol 1e-10 it is 1e-9 here); FP32 inner iteration with FP64 reliable updates reaches the
+    # accuracy of the FP64 solve
     for err, *_ in out.values():
-        assert err <= 2e4 * tol
+        assert err <= ERR_CONTRACT
     assert out["mixed"][0] <= 10 * out["fp64"][0] + 1e-13
 
 

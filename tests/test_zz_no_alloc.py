@@ -19,12 +19,13 @@ from conftest import golden
 pytestmark = pytest.mark.gpu
 
 
-def _solve(fb, fn, K, b, n, tol=1e-10):
+def _solve(fb, fn, K, b, n, tol=1e-10, jac=1, max_iter=None):
     import torch
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     res = fb._native.femd_cg_result()
     torch.cuda.synchronize()
-    st = fn(K.ctx.h, K.h, 1, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), max(1000, 10 * n), tol, C.byref(res))
+    mi = max(1000, 10 * n) if max_iter is None else max_iter
+    st = fn(K.ctx.h, K.h, jac, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), mi, tol, C.byref(res))
     assert st == 0, fb.lib.femd_cuda_last_error()
     return x.cpu().numpy(), res
 
@@ -47,6 +48,47 @@ def test_noalloc_matches_allocating_cg_twice(name):
         assert r.iterations == r_ref.iterations
         assert abs(r.residual - r_ref.residual) <= 1e-12 * r_ref.residual
         assert np.linalg.norm(x - x_ref) <= 1e-12 * np.linalg.norm(x_ref)
+
+
+@pytest.mark.parametrize("jac", [0, 1])
+@pytest.mark.parametrize("max_iter", [5, 17, None])
+def test_noalloc_same_bits_as_allocating_cg(jac, max_iter):
+    """Both branches (Jacobi or no preconditioner) and runs stopped by max_iter: the same
+    iterations, residual, converged flag and solution bits as femd_cuda_cg_jacobi, whose loop
+    runs in captured chunks of another length."""
+    import torch
+
+    import femd_b200 as fb
+    z, _ = golden("p2_varcoef_n16")
+    n = z["indptr"].size - 1
+    K = fb.CSRMatrix.from_arrays(n, n, z["indptr"], z["indices"], z["data"])
+    fb.JacobiPreconditioner(K)
+    b = torch.as_tensor(z["rhs"]).cuda()
+    x_ref, r_ref = _solve(fb, fb.lib.femd_cuda_cg_jacobi, K, b, n, jac=jac, max_iter=max_iter)
+    for _ in range(2):
+        x, r = _solve(fb, fb.lib.femd_cuda_cg_jacobi_noalloc, K, b, n, jac=jac, max_iter=max_iter)
+        assert (r.iterations, r.converged, r.breakdown) == (r_ref.iterations, r_ref.converged, r_ref.breakdown)
+        assert r.residual == r_ref.residual
+        assert np.array_equal(x, x_ref)
+    if max_iter is not None:
+        assert r.iterations == max_iter and not r.converged
+
+
+def test_noalloc_rejects_overlapping_b_and_x():
+    """The solve updates x in place while it reads b: one vector passed as both is refused."""
+    import torch
+
+    import femd_b200 as fb
+    z, _ = golden("p2_varcoef_n16")
+    n = z["indptr"].size - 1
+    K = fb.CSRMatrix.from_arrays(n, n, z["indptr"], z["indices"], z["data"])
+    fb.JacobiPreconditioner(K)
+    v = torch.as_tensor(z["rhs"]).cuda()
+    res = fb._native.femd_cg_result()
+    st = fb.lib.femd_cuda_cg_jacobi_noalloc(K.ctx.h, K.h, 1, C.c_void_p(v.data_ptr()), C.c_void_p(v.data_ptr()), 100,
+                                            1e-10, C.byref(res))
+    assert st == 1
+    assert b"overlap" in fb.lib.femd_cuda_last_error()
 
 
 def test_noalloc_rejects_systems_beyond_its_scratch():
