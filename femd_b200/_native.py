@@ -31,6 +31,11 @@ class femd_rule(C.Structure):
                 ("eta_host", C.c_void_p), ("w_host", C.c_void_p)]
 
 
+class femd_integrand(C.Structure):
+    _fields_ = [("code_host", C.c_void_p), ("ncode", C.c_int), ("nreg", C.c_int), ("nconst", C.c_int),
+                ("ninput", C.c_int)]
+
+
 class femd_cg_result(C.Structure):
     _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("residual", C.c_double), ("breakdown", C.c_int),
                 ("status", C.c_int), ("outer", C.c_int), ("seconds", C.c_double)]
@@ -69,6 +74,10 @@ SIGNATURES = {
                                        C.POINTER(femd_coef), _I, _P, _I]),
     "femd_cuda_assemble_vector": (_I, [_P, C.POINTER(femd_mesh2d), C.POINTER(femd_rule), _P, _I, _P,
                                        C.POINTER(femd_coef), _I, _P]),
+    "femd_cuda_integrand_eval": (_I, [_P, C.POINTER(femd_integrand), _P, _P, C.c_longlong, _P, _P, _P, _P, _P]),
+    "femd_cuda_integrand_eval_cells": (_I, [_P, C.POINTER(femd_integrand), _P, _P, C.POINTER(femd_mesh2d),
+                                            C.POINTER(femd_rule), _P]),
+    "femd_cuda_eval_field": (_I, [_P, C.POINTER(femd_mesh2d), C.POINTER(femd_rule), _P, _P, _I, _P, _P]),
     "femd_cuda_spmv": (_I, [_P, _P, _P, _P]),
     "femd_cuda_spmv_autotune": (_I, [_P, _P, _I, _PI, C.POINTER(C.c_double)]),
     "femd_cuda_spmv_set_tpr": (_I, [_P, _I]),
@@ -76,6 +85,7 @@ SIGNATURES = {
     "femd_cuda_combine": (_I, [_P, _D, _P, _D, _P, _P]),
     "femd_cuda_cg_jacobi": (_I, [_P, _P, _I, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_cg_solve_host": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
+    "femd_cuda_kernel_time": (_I, [_P, _P, _I, _I, C.POINTER(C.c_double)]),
     "femd_cuda_pcg_mixed": (_I, [_P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_cg_jacobi_noalloc": (_I, [_P, _P, _I, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_create": (_I, [_P, _I, _P, _I, C.POINTER(_P)]),

@@ -44,6 +44,7 @@ class Batch:
         self.mats = mats
         self.last_status = N.FEMD_OK
         self._armed = {}                                    # id -> (b, x) kept alive while armed
+        self._ls_shape = dict(nnz_per_entry=16384, chunk=8, spmv="row groups")
 
     def __del__(self):
         try:
@@ -69,6 +70,17 @@ class Batch:
         value).  windows: SpMV by windows of whole rows (True) or by row groups (False)."""
         w = -1 if windows is None else int(bool(windows))
         check(lib.femd_cuda_batch_lockstep_configure(self.h, int(nnz_per_entry), int(chunk), w))
+        if nnz_per_entry:
+            self._ls_shape["nnz_per_entry"] = int(nnz_per_entry)
+        if chunk:
+            self._ls_shape["chunk"] = int(chunk)
+        if windows is not None:
+            self._ls_shape["spmv"] = "windows" if windows else "row groups"
+
+    def lockstep_params(self):
+        """The lockstep engine's shape as configured (nonzeros per table entry, iterations per
+        chunk, SpMV form)."""
+        return dict(self._ls_shape)
 
     def params(self):
         b, n, t, g = C.c_int(), C.c_int(), C.c_int(), C.c_int()

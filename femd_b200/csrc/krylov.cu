@@ -14,6 +14,7 @@
 //
 // HBM bytes per FP64 iteration (n rows, nnz entries): SpMV 12 nnz + 4 (n+1) + 8 n (p) + 8 n (Ap);
 // update 40 n read + 16 n written; direction 24 n read + 8 n written.
+#include <climits>
 #include <cmath>
 #include <memory>
 #include <mutex>
@@ -1135,6 +1136,61 @@ int femd_cuda_pcg_mixed(femd_ctx ctx, femd_matrix K, const double *b_dev, double
     *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
     if (n == 0) return FEMD_OK;
     return mixed_run(ctx, K, b_dev, x_dev, max_iter, tol, res);
+}
+
+int femd_cuda_kernel_time(femd_ctx ctx, femd_matrix K, int kernel, int reps, double *us_out)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K && us_out && reps >= 1, "kernel_time: bad arguments");
+    FEMD_CHECK_ARG(kernel >= 0 && kernel <= 2, "kernel_time: kernel is 0 (SpMV + p.Ap), 1 (fused update) or 2 (direction)");
+    FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "kernel_time: the matrix must be square");
+    FEMD_CHECK_ARG(K->inv_valid, JACOBI_MISSING);
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    const int n = K->pattern->nrows;
+    *us_out = 0.0;
+    if (n == 0) return FEMD_OK;
+    SolverWS *Wp = nullptr;
+    FEMD_TRY(get_ws(ctx, K, &Wp));
+    SolverWS &W = *Wp;
+    cudaStream_t s = ctx->stream;
+    femd_pattern P = K->pattern;
+    // a state that never stops the loop: max_iter huge, r = p = D^-1 (so ||r||, r.z and p.Ap stay
+    // positive for an SPD matrix), alpha and beta 0 (every launch streams the same bytes and leaves
+    // the vectors as they are)
+    CGState<double> S{};
+    S.rz = 1.0;
+    S.max_iter = INT_MAX;
+    *W.st_host = S;
+    const unsigned gn = grid_for((size_t)n, 256, 1u << 20);
+    k_combine<<<gn, 256, 0, counted(s)>>>(1.0, K->inv.p, 0.0, K->inv.p, W.r.p, n);
+    k_combine<<<gn, 256, 0, counted(s)>>>(1.0, K->inv.p, 0.0, K->inv.p, W.p.p, n);
+    FEMD_TRY_CUDA(cudaMemsetAsync(W.wx.p, 0, (size_t)n * sizeof(double), s));
+    auto one = [&]() {
+        if (kernel == 0)
+            launch_spmv<double, double, true>(W.shape, W.gs, s, P->indptr.p, P->indices.p, K->data.p, W.p.p, W.Ap.p, n, W.part.p,
+                                              W.st.p);
+        else if (kernel == 1)
+            k_cg_update<double, true><<<W.gr, RED_BLOCK, 0, counted(s)>>>(W.wx.p, W.r.p, W.p.p, W.Ap.p, K->inv.p, n, W.part.p,
+                                                                          W.st.p, 0);
+        else
+            k_cg_direction<double, true><<<W.gr, RED_BLOCK, 0, counted(s)>>>(W.p.p, W.r.p, K->inv.p, n, W.st.p);
+    };
+    for (int w = 0; w < 3; ++w) {
+        FEMD_TRY_CUDA(cudaMemcpyAsync(W.st.p, W.st_host, sizeof(CGState<double>), cudaMemcpyHostToDevice, s));
+        one();
+    }
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.st.p, W.st_host, sizeof(CGState<double>), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY_CUDA(cudaEventRecord(W.e0, s));
+    for (int r = 0; r < reps; ++r) one();
+    FEMD_TRY_CUDA(cudaEventRecord(W.e1, s));
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY_CUDA(cudaEventSynchronize(W.e1));
+    float ms = 0.f;
+    FEMD_TRY_CUDA(cudaEventElapsedTime(&ms, W.e0, W.e1));
+    *us_out = (double)ms * 1e3 / reps;
+    return FEMD_OK;
 }
 
 int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host, const int *indices_host, const double *data_host,

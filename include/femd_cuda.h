@@ -187,6 +187,43 @@ FEMD_API int femd_cuda_assemble_vector(femd_ctx ctx, const femd_mesh2d *mesh, co
                               int nterms, const int *a, const femd_coef *coef, int mode, double *f_dev);
 
 /* ======================================================================================
+ * Coefficients of a compiled form: the Integrand register program and fields at the points.
+ * Replaces Integrand::evaluate (include/femd/forms/integrand.hpp:85-109, the program run of
+ * :300-342, checks of :47-66, reached through FormAssembler2D::coefficients,
+ * include/femd/forms/assembler_2d.hpp:393-410) and Cache2D::eval_multi
+ * (include/femd/fe/cache_2d.hpp:245-288, FormAssembler2D::evaluate_fields).  A program is the
+ * reference's format -- what python/femd/forms.py:1822-1938 (_Program) emits: 4 integers per
+ * instruction (op, out register, a, b) with the opcodes of integrand.hpp:33-45 (CONST 0, X 1,
+ * Y 2, NX 3, NY 4, INPUT 5, ADD 6, MUL 7, POW 8, SIN 9 ... SIGN 19); the result is the last
+ * instruction's register.  Errors carry the reference's messages (FEMD_EINVAL).  Sums and
+ * products are exact IEEE operations as in the reference; the transcendental functions are
+ * CUDA's (within a few ulp of the host C library's).  Limits of this evaluator: 160 registers,
+ * 2048 instructions, 1024 constants, 16 inputs.
+ * ====================================================================================== */
+typedef struct {
+    const int *code_host;   /* ncode = 4 x instructions */
+    int ncode, nreg, nconst, ninput;
+} femd_integrand;
+
+/* out_dev[q] (npts values) = the program at given points: inputs_dev[i] are ninput device arrays
+ * of npts values, consts_host nconst values, xs/ys and nx/ny device arrays (NULL when the program
+ * does not read them).  Synchronizes. */
+FEMD_API int femd_cuda_integrand_eval(femd_ctx ctx, const femd_integrand *prog, const double *consts_host,
+                                      const double *const *inputs_dev, long long npts, const double *xs_dev,
+                                      const double *ys_dev, const double *nx_dev, const double *ny_dev, double *out_dev);
+/* The same at the points of a cell rule, out_dev[e nq + q] (ncells x nq): x and y formed from the
+ * mesh as the reference's cell cache does; a program that reads the normal is refused on cells
+ * (FormAssembler2D::add_term).  Synchronizes. */
+FEMD_API int femd_cuda_integrand_eval_cells(femd_ctx ctx, const femd_integrand *prog, const double *consts_host,
+                                            const double *const *inputs_dev, const femd_mesh2d *mesh, const femd_rule *rule,
+                                            double *out_dev);
+/* A P_k field at the points of a cell rule (Cache2D::eval_multi): out_dev[i np + e nq + q] for
+ * codes[i] in {0 value, 1 d/dx, 2 d/dy} (1 to 3 codes, np = ncells nq); cell_dofs_dev the
+ * ncells x nloc dof map of the field's coefficients (-1: the node reads 0).  Synchronizes. */
+FEMD_API int femd_cuda_eval_field(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, const int *cell_dofs_dev,
+                                  const double *field_dev, int ncodes, const int *codes, double *out_dev);
+
+/* ======================================================================================
  * Sparse kernels on a matrix.
  * ====================================================================================== */
 /* y = K x: CSRMatrix::apply (include/femd/sparse/csr.hpp:203-215). */
@@ -231,6 +268,13 @@ FEMD_API int femd_cuda_cg_jacobi(femd_ctx ctx, femd_matrix K, int use_jacobi, co
 FEMD_API int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host, const int *indices_host,
                             const double *data_host, const double *inv_host, const double *b_host, const double *x0_host,
                             double *x_host, int max_iter, double tol, femd_cg_result *res);
+
+/* Device time of one launch of a kernel of the FP64 Jacobi-PCG loop on K (CUDA events on the
+ * context's stream, averaged over reps back-to-back launches after a warm-up): kernel 0 the SpMV
+ * with the fused p.Ap (K5), 1 the fused update x += a p, r -= a Ap, ||r||^2, r.D^-1 r (K6), 2 the
+ * direction update p = D^-1 r + b p.  Runs on K's solver workspace with a = b = 0 (the same bytes
+ * as a real iteration).  Instrumentation with no reference counterpart.  Synchronizes. */
+FEMD_API int femd_cuda_kernel_time(femd_ctx ctx, femd_matrix K, int kernel, int reps, double *us_out);
 
 /* Mixed precision: inner Jacobi-PCG on an FP32 copy of K with FP32 vectors and FP32
  * accumulation; the residual r = b - A x is recomputed on the FP64 matrix and the solution
