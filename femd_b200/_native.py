@@ -36,6 +36,11 @@ class femd_integrand(C.Structure):
                 ("ninput", C.c_int)]
 
 
+class femd_facet_rule(C.Structure):
+    _fields_ = [("k", C.c_int), ("nloc", C.c_int), ("nq", C.c_int), ("xi_host", C.c_void_p), ("eta_host", C.c_void_p),
+                ("gw_host", C.c_void_p), ("ref_host", C.c_void_p)]
+
+
 class femd_cg_result(C.Structure):
     _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("residual", C.c_double), ("breakdown", C.c_int),
                 ("status", C.c_int), ("outer", C.c_int), ("seconds", C.c_double)]
@@ -78,6 +83,13 @@ SIGNATURES = {
     "femd_cuda_integrand_eval_cells": (_I, [_P, C.POINTER(femd_integrand), _P, _P, C.POINTER(femd_mesh2d),
                                             C.POINTER(femd_rule), _P]),
     "femd_cuda_eval_field": (_I, [_P, C.POINTER(femd_mesh2d), C.POINTER(femd_rule), _P, _P, _I, _P, _P]),
+    "femd_cuda_facets_create": (_I, [_P, _P, _I, _P, _P, C.POINTER(_P)]),
+    "femd_cuda_facet_points": (_I, [_P, _P, C.POINTER(femd_mesh2d), C.POINTER(femd_facet_rule), _P, _P, _P, _P, _P]),
+    "femd_cuda_assemble_facet_matrix": (_I, [_P, _P, C.POINTER(femd_mesh2d), C.POINTER(femd_facet_rule), _I, _P, _P,
+                                             C.POINTER(femd_coef), _P]),
+    "femd_cuda_assemble_facet_vector": (_I, [_P, _P, C.POINTER(femd_mesh2d), C.POINTER(femd_facet_rule), _I, _P,
+                                             C.POINTER(femd_coef), _P]),
+    "femd_cuda_prolongate": (_I, [_P, _I, _P, _P, _P]),
     "femd_cuda_spmv": (_I, [_P, _P, _P, _P]),
     "femd_cuda_spmv_autotune": (_I, [_P, _P, _I, _PI, C.POINTER(C.c_double)]),
     "femd_cuda_spmv_set_tpr": (_I, [_P, _I]),
@@ -91,9 +103,10 @@ SIGNATURES = {
     "femd_cuda_batch_create": (_I, [_P, _I, _P, _I, C.POINTER(_P)]),
     "femd_cuda_batch_solve": (_I, [_P, _P, _P, _P, _I, _D, _I, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_solve_lockstep": (_I, [_P, _P, _P, _P, _I, _D, _I, C.POINTER(femd_cg_result)]),
-    "femd_cuda_batch_lockstep_configure": (_I, [_P, _I, _I, _I]),
+    "femd_cuda_batch_lockstep_configure": (_I, [_P, _I, _I, _I, _I]),
     "femd_cuda_batch_step_lockstep": (_I, [_P, _P, _I, _PI, _PI, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_abort": (_I, [_P]),
+    "femd_cuda_batch_lockstep_stats": (_I, [_P, C.POINTER(C.c_longlong)]),
     "femd_cuda_batch_info": (_I, [_P, _PI, _PI, _PI, _PI]),
     "femd_cuda_batch_debug": (_I, [_P, _I, C.c_longlong]),
     "femd_cuda_batch_profile": (_I, [_P, C.POINTER(C.c_longlong)]),
@@ -109,6 +122,11 @@ SIGNATURES = {
     "femd_host_lagrange_numbering": (_I, [_I, _I, _P, _I, _I, _P, _PI, _PI]),
     "femd_host_triangle_quadrature": (_I, [_I, _P, _P, _P]),
     "femd_host_tabulate": (_I, [_I, _I, _P, _P, _P]),
+    "femd_host_rcm_order": (_I, [_I, _P, _P, _P]),
+    "femd_host_lagrange_raw": (_I, [_I, _I, _P, _I, _P, _PI]),
+    "femd_host_lagrange_nodes": (_I, [_I, _P, _P]),
+    "femd_host_exterior_facets": (_I, [_I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _P, _P]),
+    "femd_host_facet_rule": (_I, [_I, _I, _P, _P, _P, _P]),
 }
 
 

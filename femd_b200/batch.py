@@ -44,7 +44,7 @@ class Batch:
         self.mats = mats
         self.last_status = N.FEMD_OK
         self._armed = {}                                    # id -> (b, x) kept alive while armed
-        self._ls_shape = dict(nnz_per_entry=16384, chunk=8, spmv="row groups")
+        self._ls_shape = dict(nnz_per_entry=16384, chunk=8, spmv="row groups", compact=True)
 
     def __del__(self):
         try:
@@ -65,17 +65,29 @@ class Batch:
         """Set the launch shape (femd_cuda_batch_configure)."""
         check(lib.femd_cuda_batch_configure(self.h, int(block), int(nnz_per_block), int(nnz_per_thread)))
 
-    def configure_lockstep(self, nnz_per_entry=0, chunk=0, windows=None):
+    def configure_lockstep(self, nnz_per_entry=0, chunk=0, windows=None, compact=None):
         """Shape of the lockstep engine (femd_cuda_batch_lockstep_configure; 0 / None keep a
-        value).  windows: SpMV by windows of whole rows (True) or by row groups (False)."""
+        value).  windows: SpMV by windows of whole rows (True) or by row groups (False); compact:
+        in mixed precision, the reordered layout with 16-bit column offsets and the direction
+        read from shared memory (True, the default) or the plain layout (False)."""
         w = -1 if windows is None else int(bool(windows))
-        check(lib.femd_cuda_batch_lockstep_configure(self.h, int(nnz_per_entry), int(chunk), w))
+        cp = -1 if compact is None else int(bool(compact))
+        check(lib.femd_cuda_batch_lockstep_configure(self.h, int(nnz_per_entry), int(chunk), w, cp))
         if nnz_per_entry:
             self._ls_shape["nnz_per_entry"] = int(nnz_per_entry)
         if chunk:
             self._ls_shape["chunk"] = int(chunk)
         if windows is not None:
             self._ls_shape["spmv"] = "windows" if windows else "row groups"
+        if compact is not None:
+            self._ls_shape["compact"] = bool(compact)
+
+    def lockstep_stats(self):
+        """The last lockstep solve's layout (femd_cuda_batch_lockstep_stats): members in the compact
+        and in the plain layout, the widest shared-memory window, the table entries."""
+        out = (C.c_longlong * 4)()
+        check(lib.femd_cuda_batch_lockstep_stats(self.h, out))
+        return dict(compact=out[0], plain=out[1], widest_window=out[2], entries=out[3])
 
     def lockstep_params(self):
         """The lockstep engine's shape as configured (nonzeros per table entry, iterations per

@@ -77,6 +77,11 @@ struct BProb {
     unsigned long long *claim;   // chunk claims of the SpMV passes
     unsigned *bar;
     BState *st;
+    // lockstep engine, compact layout (mixed precision; null otherwise): the member's FP32 matrix
+    // and its vectors are in the pattern's reverse Cuthill-McKee order; iperm maps an original row
+    // to its reordered one, cptr / coff are the reordered rows' pointers and 16-bit column offsets
+    const int *iperm, *cptr;
+    const short *coff;
 };
 
 struct BQueue {
@@ -759,6 +764,17 @@ __global__ void k_batch_f32(const double *__restrict__ a, float *__restrict__ a3
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv32[i] = (float)inv[i];
 }
 
+// the same for the compact layout: value q of the original CSR goes to position dst[q] of the
+// reordered one, the inverse diagonal of original row i to reordered row iperm[i]
+__global__ void k_ls_f32_perm(const double *__restrict__ a, const int *__restrict__ dst, float *__restrict__ a32,
+                              long long nnz, const double *__restrict__ inv, const int *__restrict__ iperm,
+                              float *__restrict__ inv32, int n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += stride) a32[dst[q]] = (float)a[q];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv32[iperm[i]] = (float)inv[i];
+}
+
 // chunk tables of one matrix: chunk k starts at the first row whose first nonzero is at or after
 // k * cp (cp = chunk capacity - longest row), so no chunk holds more than the capacity
 __global__ void k_chunk_table(const int *__restrict__ indptr, int n, int nnz, int cp, int nch, int *crow, int *cq)
@@ -876,6 +892,58 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
 #pragma unroll
         for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
         if (lane == 0 && i < r1) out(i, s, pv);
+        i = inext;
+        lo = lo_n;
+        hi = hi_n;
+    }
+}
+
+// y = A p on reordered rows [r0, r1) of the compact layout, the direction p staged in shared
+// memory over the entry's column window [c0, ...): TPR lanes per row, U value / offset loads in
+// flight per lane, the products read p from shared memory (no gathers from global memory).  Each
+// lane adds its entries in increasing position and the row's lanes combine by a fixed shuffle tree.
+template <int TPR>
+__device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restrict__ A, const float *win, int c0, int r0,
+                                          int r1, float *__restrict__ Ap, double &dot)
+{
+    constexpr int U = 4, GPW = 32 / TPR, STEP = (LS_BB / 32) * GPW;
+    const int lane = threadIdx.x % TPR;
+    const int sub = (int)(threadIdx.x & 31) / TPR;
+    int i0 = r0 + (int)(threadIdx.x >> 5) * GPW;
+    int i = i0 + sub;
+    int lo = 0, hi = 0;
+    if (i < r1) {
+        lo = P.cptr[i];
+        hi = P.cptr[i + 1];
+    }
+    for (; i0 < r1; i0 += STEP) {
+        const int inext = i + STEP;
+        int lo_n = 0, hi_n = 0;
+        if (inext < r1) {
+            lo_n = P.cptr[inext];
+            hi_n = P.cptr[inext + 1];
+        }
+        const float *wrow = win + (i - c0);
+        float s = 0.0f;
+        for (int base = lo + lane; base < hi; base += U * TPR) {
+            short o[U];
+            float v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int q = base + u * TPR;
+                o[u] = q < hi ? __ldcs(&P.coff[q]) : (short)0;
+                v[u] = q < hi ? __ldcs(&A[q]) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (base + u * TPR < hi) s += v[u] * wrow[o[u]];
+        }
+#pragma unroll
+        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
+        if (lane == 0 && i < r1) {
+            Ap[i] = s;
+            dot += (double)wrow[0] * (double)s;
+        }
         i = inext;
         lo = lo_n;
         hi = hi_n;
@@ -1009,6 +1077,7 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ 
                                                    LState *st, double *part, int *active, int *ru_count)
 {
     using F = typename std::conditional<MIXED, float, double>::type;
+    extern __shared__ float ls_win[];
     if (MIXED && blockIdx.x == 0 && threadIdx.x == 0) *ru_count = 0;
     const int e = blockIdx.x;
     const LBlock L = blks[e];
@@ -1025,13 +1094,32 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ 
     const F *pold = (it & 1) ? pa : pb;
     F *pnew = (it & 1) ? pb : pa;
     double dot = 0.0;
-    ls_spmv_entry<F, F>(
-        P, A, L, [&](int j) { return pdir(z, pold, beta, j); }, [&](int i) { return pdir(z, pold, beta, i); },
-        [&](int i, F s, F pi) {
-            pnew[i] = pi;
-            Ap[i] = s;
-            dot += (double)pi * (double)s;
-        });
+    if (MIXED && P.coff) {
+        // compact layout: p over the entry's column window [w0, w1) into shared memory (the
+        // owner's values to pnew), then the rows read it there
+        const int c0 = L.w0, c1 = L.w1;
+        for (int w = c0 + (int)threadIdx.x; w < c1; w += LS_BB) {
+            const float pw = pdir((const float *)z, (const float *)pold, (float)beta, w);
+            ls_win[w - c0] = pw;
+            if (w >= L.r0 && w < L.r1) ((float *)pnew)[w] = pw;
+        }
+        __syncthreads();
+        switch (P.tpr) {
+        case 2: ls_rows_c<2>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        case 4: ls_rows_c<4>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        case 8: ls_rows_c<8>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        case 16: ls_rows_c<16>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        default: ls_rows_c<32>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        }
+    } else {
+        ls_spmv_entry<F, F>(
+            P, A, L, [&](int j) { return pdir(z, pold, beta, j); }, [&](int i) { return pdir(z, pold, beta, i); },
+            [&](int i, F s, F pi) {
+                pnew[i] = pi;
+                Ap[i] = s;
+                dot += (double)pi * (double)s;
+            });
+    }
     const double v[1] = {dot};
     double tot[1];
     if (ls_member_sum<1>(v, part, NE, e, L, &S.t1, tot) && threadIdx.x == 0) {
@@ -1118,8 +1206,9 @@ __global__ void __launch_bounds__(LS_BB) k_ls_flush(const BProb *__restrict__ pr
         const BProb P = probs[L.m];
         if (ALL && !st[L.m].breakdown) continue;
         for (int i = L.r0 + (int)threadIdx.x; i < L.r1; i += LS_BB) {
-            P.x[i] += (double)P.d32[i];
-            P.d32[i] = 0.0f;
+            const int ii = P.iperm ? P.iperm[i] : i;
+            P.x[i] += (double)P.d32[ii];
+            P.d32[ii] = 0.0f;
         }
     }
 }
@@ -1149,12 +1238,13 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_resid(const BProb *__restrict__
             [&](int i) { return make_double2(P.b[i], MODE == 2 ? 0.0 : P.inv64[i]); },
             [&](int i, double s, double2 own) {
                 const double bi = own.x, ri = bi - s;
+                const int ii = MIXED && P.iperm ? P.iperm[i] : i;   // the row in the member's vector order
                 v[0] += ri * ri;
                 if (MODE != 2) {
                     if (MIXED) {
                         const float rf = (float)ri, zf = (float)own.y * rf;
-                        P.r32[i] = rf;
-                        P.z32[i] = zf;
+                        P.r32[ii] = rf;
+                        P.z32[ii] = zf;
                         v[1] += (double)rf * (double)zf;
                     } else {
                         const double zi = own.y * ri;
@@ -1165,8 +1255,8 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_resid(const BProb *__restrict__
                 }
                 if (MODE == 0) {
                     v[2] += bi * bi;
-                    pb[i] = F(0);
-                    if (MIXED) P.d32[i] = 0.0f;
+                    pb[ii] = F(0);
+                    if (MIXED) P.d32[ii] = 0.0f;
                 }
             });
         double tot[3];
@@ -1252,6 +1342,7 @@ struct Member {
     double tol = 0.0;
     int max_iter = 0;
     bool need_f32 = false;                      // armed: the FP32 copies are made before its first mixed launch
+    bool f32_compact = false;                   // the FP32 copy is in the compact (reordered) layout
     bool force_fp64 = false;                    // its FP32 recurrence stagnated: FP64 for the rest of the solve
     int prior_its = 0, prior_rus = 0;           // iterations and reliable updates before the switch
     DevBuf<int> ls_tab;                         // lockstep SpMV windows: first rows (nw + 1), scratch
@@ -1291,6 +1382,8 @@ struct femd_batch_s : femd::HandleBase {
     // the lockstep engine: nonzeros per table entry, iterations enqueued between state reads
     int ls_nnz = 16384, ls_chunk = 8;
     bool ls_windows = false;                    // SpMV by windows (else by row groups)
+    bool ls_compact = true;                     // mixed precision: the compact layout where it applies
+    long long ls_stats[4] = {0, 0, 0, 0};       // last lockstep solve: compact members, plain members, widest window, entries
     int *abort_dev = nullptr;
     femd_batch_s() : HandleBase(femd::KIND_BATCH) {}
     void drop_graphs()
@@ -1587,12 +1680,13 @@ static int launch_set(femd_ctx ctx, femd_batch_s *B, std::vector<int> order, int
     if (mx) {
         for (int id : order) {
             Member &M = *B->mem[id];
-            if (!M.need_f32) continue;
+            if (!M.need_f32 && !M.f32_compact) continue;
             const BProb P = describe(B, id, true);
             k_batch_f32<<<grid_for((size_t)M.nnz, 256, 4 * (unsigned)B->ctx->sm_count), 256, 0, counted(s)>>>(
                 M.K->data.p, P.A32, M.nnz, M.K->inv.p, P.inv32, M.n);
             FEMD_TRY_CUDA(cudaGetLastError());
             M.need_f32 = false;
+            M.f32_compact = false;
         }
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -1801,6 +1895,77 @@ static int ls_windows_of(femd_batch_s *B, Member &M)
     return FEMD_OK;
 }
 
+// ---- the compact layout (lockstep engine, mixed precision) -------------------------------------
+
+// a reverse Cuthill-McKee order of a square host CSR pattern, order[new] = old (setup_host.cpp)
+namespace femd {
+void rcm_order(int n, const std::vector<int> &ip, const std::vector<int> &ix, std::vector<int> &order);
+}
+
+static constexpr int CL_TILE = 32;          // rows per tile of the column-window bounds
+static constexpr int CL_WIN_MAX = 12288;    // largest column window of an entry (FP32: 48 KB of shared memory)
+
+// Build the pattern's compact layout once (cl_state 1), or mark it unsuitable (-1).
+static int build_compact(femd_ctx ctx, femd_pattern P)
+{
+    if (P->cl_state != 0) return FEMD_OK;
+    cudaStream_t s = ctx->stream;
+    const int n = P->nrows;
+    const long long nnz = P->nnz;
+    std::vector<int> ip((size_t)n + 1), ix((size_t)std::max<long long>(nnz, 1));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(ip.data(), P->indptr.p, ((size_t)n + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (nnz) FEMD_TRY_CUDA(cudaMemcpyAsync(ix.data(), P->indices.p, (size_t)nnz * sizeof(int), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> order;
+    rcm_order(n, ip, ix, order);
+    std::vector<int> iperm((size_t)n), cptr((size_t)n + 1, 0), dst((size_t)std::max<long long>(nnz, 1));
+    std::vector<short> off((size_t)std::max<long long>(nnz, 1));
+    for (int k = 0; k < n; ++k) iperm[order[k]] = k;
+    for (int k = 0; k < n; ++k) cptr[k + 1] = cptr[k] + (ip[order[k] + 1] - ip[order[k]]);
+    const int ntile = (n + CL_TILE - 1) / CL_TILE;
+    std::vector<int> tlo((size_t)ntile, INT_MAX), thi((size_t)ntile, INT_MIN);
+    std::vector<std::pair<int, int>> row;
+    int bw = 0;
+    for (int k = 0; k < n; ++k) {
+        const int i = order[k];
+        row.clear();
+        for (int q = ip[i]; q < ip[i + 1]; ++q) row.emplace_back(iperm[ix[q]], q);
+        std::sort(row.begin(), row.end());
+        int pos = cptr[k];
+        int &lo = tlo[k / CL_TILE], &hi = thi[k / CL_TILE];
+        lo = std::min(lo, k);
+        hi = std::max(hi, k);
+        for (const auto &e : row) {
+            const int d = e.first - k;
+            bw = std::max(bw, std::abs(d));
+            off[pos] = (short)std::max(-32768, std::min(32767, d));
+            dst[e.second] = pos++;
+            lo = std::min(lo, e.first);
+            hi = std::max(hi, e.first);
+        }
+    }
+    P->cl_bw = bw;
+    if (bw > 32767) {
+        P->cl_state = -1;
+        return FEMD_OK;
+    }
+    int st;
+    if ((st = P->cl_iperm.alloc((size_t)n)) || (st = P->cl_indptr.alloc((size_t)n + 1)) ||
+        (st = P->cl_dst.alloc((size_t)std::max<long long>(nnz, 1))) || (st = P->cl_off.alloc((size_t)std::max<long long>(nnz, 1))))
+        return st;
+    FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_iperm.p, iperm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_indptr.p, cptr.data(), ((size_t)n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (nnz) {
+        FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_dst.p, dst.data(), (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
+        FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_off.p, off.data(), (size_t)nnz * sizeof(short), cudaMemcpyHostToDevice, s));
+    }
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // the host vectors are released on return
+    P->cl_tile_lo.swap(tlo);
+    P->cl_tile_hi.swap(thi);
+    P->cl_state = 1;
+    return FEMD_OK;
+}
+
 namespace {
 struct PinnedBuf {
     void *p = nullptr;
@@ -1826,15 +1991,56 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     std::vector<std::vector<std::array<int, 4>>> ents(nm);   // per member: r0, r1, w0, w1 of its entries
     std::vector<int> nent(nm);
     int NEfull = 0, max_it = 1;
+    int maxwin = 0;                                     // the widest column window of a compact entry
     for (int k = 0; k < nm; ++k) {
         Member &M = *B->mem[ids[k]];
         desc[k] = describe(B, ids[k], mx);
         desc[k].tpr = ls_tpr(M);
         desc[k].wrow = nullptr;
+        desc[k].iperm = desc[k].cptr = nullptr;
+        desc[k].coff = nullptr;
         if (B->ls_windows && (st = ls_windows_of(B, M))) return st;
         auto &E = ents[k];
         E.clear();
-        if (B->ls_windows && !M.ls_wrow.empty()) {
+        bool compact = false;
+        if (mx && B->ls_compact && !B->ls_windows) {
+            femd_pattern P = M.K->pattern;
+            if ((st = build_compact(ctx, P))) return st;
+            if (P->cl_state == 1) {
+                // rows per entry: a multiple of the tile near nnz_per_entry nonzeros, halved while
+                // some entry's column window is wider than the shared-memory window
+                int R = std::max(CL_TILE, ls_rows_per_entry(B, M) / CL_TILE * CL_TILE);
+                while (!compact) {
+                    E.clear();
+                    int wmax = 0;
+                    for (int r = 0; r < M.n; r += R) {
+                        const int r1 = std::min(M.n, r + R);
+                        int lo = INT_MAX, hi = INT_MIN;
+                        for (int t = r / CL_TILE; t <= (r1 - 1) / CL_TILE; ++t) {
+                            lo = std::min(lo, P->cl_tile_lo[t]);
+                            hi = std::max(hi, P->cl_tile_hi[t]);
+                        }
+                        E.push_back({r, r1, lo, hi + 1});
+                        wmax = std::max(wmax, hi + 1 - lo);
+                    }
+                    if (wmax <= CL_WIN_MAX) {
+                        compact = true;
+                        maxwin = std::max(maxwin, wmax);
+                    } else if (R > CL_TILE) {
+                        R = std::max(CL_TILE, R / 2 / CL_TILE * CL_TILE);
+                    } else {
+                        break;
+                    }
+                }
+                if (!compact) E.clear();
+            }
+        }
+        if (compact) {
+            femd_pattern P = M.K->pattern;
+            desc[k].iperm = P->cl_iperm.p;
+            desc[k].cptr = P->cl_indptr.p;
+            desc[k].coff = P->cl_off.p;
+        } else if (B->ls_windows && !M.ls_wrow.empty()) {
             desc[k].wrow = M.ls_tab.p;
             const int nw = (int)M.ls_wrow.size() - 1;
             const int G = std::max(1, B->ls_nnz / LS_W);
@@ -1850,12 +2056,25 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
         FEMD_CHECK_ARG((long long)NEfull + nent[k] < INT_MAX / 4, "batch: too many table entries");
         NEfull += nent[k];
         max_it = std::max(max_it, M.max_iter);
-        if (mx && M.need_f32) {
-            k_batch_f32<<<grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count), 256, 0, counted(s)>>>(
-                M.K->data.p, desc[k].A32, M.nnz, M.K->inv.p, desc[k].inv32, M.n);
+        if (mx && (M.need_f32 || M.f32_compact != compact)) {
+            const unsigned g = grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count);
+            if (compact)
+                k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, M.K->pattern->cl_dst.p, desc[k].A32, M.nnz, M.K->inv.p,
+                                                         M.K->pattern->cl_iperm.p, desc[k].inv32, M.n);
+            else
+                k_batch_f32<<<g, 256, 0, counted(s)>>>(M.K->data.p, desc[k].A32, M.nnz, M.K->inv.p, desc[k].inv32, M.n);
             FEMD_TRY_CUDA(cudaGetLastError());
             M.need_f32 = false;
+            M.f32_compact = compact;
         }
+    }
+    {
+        long long nc = 0;
+        for (int k = 0; k < nm; ++k) nc += desc[k].coff != nullptr;
+        B->ls_stats[0] = nc;
+        B->ls_stats[1] = nm - nc;
+        B->ls_stats[2] = maxwin;
+        B->ls_stats[3] = NEfull;
     }
     DevBuf<BProb> d_desc;
     DevBuf<LState> d_state;
@@ -1918,13 +2137,16 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     else
         k_ls_resid<false, 0><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
     FEMD_TRY_CUDA(cudaGetLastError());
+    const size_t win_b = (size_t)maxwin * sizeof(float);   // the SpMV's shared-memory window
+    if (mx) FEMD_TRY_CUDA(cudaFuncSetAttribute(k_ls_spmv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)(CL_WIN_MAX * sizeof(float))));
     const int C = std::max(1, B->ls_chunk);
     const long long max_chunks = (long long)max_it / C + 4;
     int aborted = 0;
     for (long long j = 0; j <= max_chunks; ++j) {
         for (int c = 0; c < C; ++c) {
             if (mx) {
-                k_ls_spmv<true><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count);
+                k_ls_spmv<true><<<NE, LS_BB, win_b, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count);
                 k_ls_update<true><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
                 k_ls_flush<false><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, ru_list, ru_count);
                 k_ls_resid<true, 1><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active,
@@ -2204,15 +2426,17 @@ int femd_cuda_batch_solve_lockstep(femd_ctx ctx, femd_batch handle, const double
     return st;
 }
 
-int femd_cuda_batch_lockstep_configure(femd_batch handle, int nnz_per_entry, int chunk, int windows)
+int femd_cuda_batch_lockstep_configure(femd_batch handle, int nnz_per_entry, int chunk, int windows, int compact)
 {
     clear_error();
     femd_batch_s *B = as_batch(handle);
     FEMD_CHECK_ARG(B, "batch_lockstep_configure: bad handle");
-    FEMD_CHECK_ARG(nnz_per_entry >= 0 && chunk >= 0 && windows >= -1 && windows <= 1, "batch_lockstep_configure: bad argument");
+    FEMD_CHECK_ARG(nnz_per_entry >= 0 && chunk >= 0 && windows >= -1 && windows <= 1 && compact >= -1 && compact <= 1,
+                   "batch_lockstep_configure: bad argument");
     if (nnz_per_entry) B->ls_nnz = nnz_per_entry;
     if (chunk) B->ls_chunk = chunk;
     if (windows >= 0) B->ls_windows = windows != 0;
+    if (compact >= 0) B->ls_compact = compact != 0;
     return FEMD_OK;
 }
 
@@ -2273,6 +2497,15 @@ int femd_cuda_batch_tune(femd_ctx ctx, femd_batch handle, const double *const *b
     if ((st = femd_cuda_batch_configure(handle, cb, cn, ct))) return st;
     if (best_out) { best_out[0] = cb; best_out[1] = cn; best_out[2] = ct; }
     if (seconds_out) *seconds_out = tbest;
+    return FEMD_OK;
+}
+
+int femd_cuda_batch_lockstep_stats(femd_batch handle, long long *out)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(B && out, "batch_lockstep_stats: bad arguments");
+    for (int k = 0; k < 4; ++k) out[k] = B->ls_stats[k];
     return FEMD_OK;
 }
 

@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/femd_cuda.h"
 
@@ -38,7 +39,7 @@ void clear_error();
 
 // ---- handles ------------------------------------------------------------------------------
 enum HandleKind : uint32_t { KIND_PATTERN = 0x50415454u, KIND_MATRIX = 0x4d415452u, KIND_SOLVER = 0x534f4c56u,
-                             KIND_BATCH = 0x42415443u };
+                             KIND_BATCH = 0x42415443u, KIND_FACETS = 0x46414354u };
 
 struct HandleBase {
     uint32_t kind;
@@ -114,6 +115,15 @@ struct femd_pattern_s : femd::HandleBase {
     // columns (uint8, 255 = constrained): the scatter map in the rows' own order, a quarter of
     // its size (built on the first FAST assembly when every row is shorter than 255)
     femd::DevBuf<unsigned char> pair_off;
+    // the batched engine's compact layout of the pattern, built on first use: a reverse
+    // Cuthill-McKee order (iperm: original row -> reordered row), the reordered rows' pointers,
+    // every entry's column as a 16-bit offset from its (reordered) row, and for every original
+    // entry its position in the reordered layout; per tile of 32 reordered rows the smallest and
+    // largest column.  cl_state: 0 not built, 1 built, -1 unsuitable (a column offset over 32767)
+    int cl_state = 0, cl_bw = 0;
+    femd::DevBuf<int> cl_iperm, cl_indptr, cl_dst;
+    femd::DevBuf<short> cl_off;
+    std::vector<int> cl_tile_lo, cl_tile_hi;
     femd_pattern_s() : HandleBase(femd::KIND_PATTERN) {}
     ~femd_pattern_s() override { femd::ctx_release(ctx); }
 };

@@ -204,7 +204,8 @@ void femd_cuda_release(void *handle)
 {
     if (!handle) return;
     HandleBase *h = static_cast<HandleBase *>(handle);
-    if (h->kind == KIND_PATTERN || h->kind == KIND_MATRIX || h->kind == KIND_SOLVER || h->kind == KIND_BATCH) {
+    if (h->kind == KIND_PATTERN || h->kind == KIND_MATRIX || h->kind == KIND_SOLVER || h->kind == KIND_BATCH ||
+        h->kind == KIND_FACETS) {
         h->kind = 0;
         delete h;
     }

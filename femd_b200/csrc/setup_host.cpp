@@ -12,7 +12,84 @@
 namespace femd {
 void set_error(const std::string &msg);
 void clear_error();
+
+// A reverse Cuthill-McKee order of a square pattern (host CSR): order[new] = old.  Per connected
+// component: a pseudo-peripheral start (repeated breadth-first sweeps from the lowest-degree node
+// of the last level while the depth grows; George and Liu's heuristic), then the Cuthill-McKee
+// breadth-first numbering with each node's unnumbered neighbours taken in increasing degree
+// (ties by index); the whole sequence reversed.  Deterministic.
+void rcm_order(int n, const std::vector<int> &ip, const std::vector<int> &ix, std::vector<int> &order)
+{
+    std::vector<int> deg(n), mark(n, -1), num(n, 0), queue;
+    for (int i = 0; i < n; ++i) deg[i] = ip[i + 1] - ip[i];
+    order.clear();
+    order.reserve(n);
+    queue.reserve(n);
+    int stamp = 0;
+    // breadth-first levels from s over the nodes not yet numbered; the depth, and the
+    // lowest-degree node of the last level
+    auto sweep = [&](int s, int &depth, int &far) {
+        ++stamp;
+        queue.clear();
+        queue.push_back(s);
+        mark[s] = stamp;
+        size_t head = 0, level_start = 0;
+        depth = 0;
+        while (true) {
+            const size_t level_end = queue.size();
+            for (; head < level_end; ++head) {
+                const int u = queue[head];
+                for (int q = ip[u]; q < ip[u + 1]; ++q) {
+                    const int v = ix[q];
+                    if (!num[v] && mark[v] != stamp) {
+                        mark[v] = stamp;
+                        queue.push_back(v);
+                    }
+                }
+            }
+            if (queue.size() == level_end) {
+                far = queue[level_start];
+                for (size_t k = level_start; k < level_end; ++k)
+                    if (deg[queue[k]] < deg[far] || (deg[queue[k]] == deg[far] && queue[k] < far)) far = queue[k];
+                return;
+            }
+            level_start = level_end;
+            ++depth;
+        }
+    };
+    std::vector<int> nb;
+    for (int seed = 0; seed < n; ++seed) {
+        if (num[seed]) continue;
+        int r = seed, depth = 0, far = seed;
+        sweep(r, depth, far);
+        for (int t = 0; t < 8; ++t) {
+            int d2 = 0, f2 = far;
+            sweep(far, d2, f2);
+            if (d2 <= depth) break;
+            r = far;
+            depth = d2;
+            far = f2;
+        }
+        // Cuthill-McKee from r
+        const size_t first = order.size();
+        order.push_back(r);
+        num[r] = 1;
+        for (size_t h = first; h < order.size(); ++h) {
+            const int u = order[h];
+            nb.clear();
+            for (int q = ip[u]; q < ip[u + 1]; ++q)
+                if (!num[ix[q]]) {
+                    num[ix[q]] = 1;
+                    nb.push_back(ix[q]);
+                }
+            std::sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+            order.insert(order.end(), nb.begin(), nb.end());
+        }
+    }
+    std::reverse(order.begin(), order.end());
 }
+
+}  // namespace femd
 
 using femd::set_error;
 
@@ -53,12 +130,16 @@ int femd_host_rectangle_mesh(double x0, double y0, double x1, double y1, int nx,
 // (i+1)%3 to (i+2)%3.  Here the first appearance is found by sorting the (edge key, c 3 + i)
 // pairs: within a key the smallest c 3 + i comes first, and the edges are ranked by it.
 // An edge met once is exterior; with all_exterior its vertices and nodes are fixed.
-int femd_host_lagrange_numbering(int nverts, int ncells, const int *tris, int k, int all_exterior, int *cell_dofs,
-                                 int *dim, int *raw_dim)
+}  // extern "C"
+
+// The numbering of femd_host_lagrange_numbering; cell_raw (optional) receives the raw numbering
+// (before the elimination of Dirichlet nodes), cell_dofs (optional) the adapted one.
+static int lagrange_numbering(int nverts, int ncells, const int *tris, int k, int all_exterior, int *cell_dofs,
+                              int *cell_raw, int *dim, int *raw_dim)
 {
     femd::clear_error();
     if (k < 1 || k > 20) { set_error("LagrangeSpace2D: degree must be in 1..20"); return FEMD_EINVAL; }
-    if (nverts < 3 || ncells < 1 || !tris || !cell_dofs || !dim) { set_error("lagrange_numbering: bad arguments"); return FEMD_EINVAL; }
+    if (nverts < 3 || ncells < 1 || !tris || (!cell_dofs && !cell_raw)) { set_error("lagrange_numbering: bad arguments"); return FEMD_EINVAL; }
     const int nloc = (k + 1) * (k + 2) / 2, de = k - 1, nint = (k - 1) * (k - 2) / 2;
     const size_t nh = (size_t)ncells * 3;
     struct Half { uint64_t key; int val; };
@@ -117,10 +198,29 @@ int femd_host_lagrange_numbering(int nverts, int ncells, const int *tris, int k,
     std::vector<int> r2a((size_t)rd);
     int n = 0;
     for (long long r = 0; r < rd; ++r) r2a[r] = fixed[r] ? -1 : n++;
-    for (size_t q = 0; q < raw.size(); ++q) cell_dofs[q] = r2a[raw[q]];
-    *dim = n;
+    if (cell_dofs)
+        for (size_t q = 0; q < raw.size(); ++q) cell_dofs[q] = r2a[raw[q]];
+    if (cell_raw) std::copy(raw.begin(), raw.end(), cell_raw);
+    if (dim) *dim = n;
     if (raw_dim) *raw_dim = (int)rd;
     return FEMD_OK;
+}
+
+extern "C" {
+
+int femd_host_lagrange_numbering(int nverts, int ncells, const int *tris, int k, int all_exterior, int *cell_dofs,
+                                 int *dim, int *raw_dim)
+{
+    if (!cell_dofs || !dim) { femd::clear_error(); set_error("lagrange_numbering: bad arguments"); return FEMD_EINVAL; }
+    return lagrange_numbering(nverts, ncells, tris, k, all_exterior, cell_dofs, nullptr, dim, raw_dim);
+}
+
+// The raw numbering of the same space (every node, none eliminated), ncells x nloc: vertices
+// first, then edge nodes from the smaller vertex to the larger, then cell interiors
+// (include/femd/fe/space_2d.hpp:448-470).
+int femd_host_lagrange_raw(int nverts, int ncells, const int *tris, int k, int *cell_raw, int *raw_dim)
+{
+    return lagrange_numbering(nverts, ncells, tris, k, 0, nullptr, cell_raw, nullptr, raw_dim);
 }
 
 // Gauss-Legendre on [-1, 1]: closed forms for 1..5 points, Newton on P_n from Chebyshev-spaced
@@ -255,6 +355,118 @@ int femd_host_tabulate(int k, int nq, const double *xi, const double *eta, doubl
         }
     }
     return nloc;
+}
+
+// The reverse Cuthill-McKee order of a square CSR pattern (femd::rcm_order), order[new] = old: the
+// order of the lockstep engine's compact layout.
+int femd_host_rcm_order(int n, const int *indptr, const int *indices, int *order)
+{
+    femd::clear_error();
+    if (n < 0 || !indptr || !order || (n > 0 && indptr[n] > 0 && !indices)) { set_error("rcm_order: bad arguments"); return FEMD_EINVAL; }
+    for (int i = 0; i < n; ++i)
+        if (indptr[i + 1] < indptr[i]) { set_error("rcm_order: indptr is not increasing"); return FEMD_EINVAL; }
+    const long long nnz = n ? indptr[n] : 0;
+    for (long long q = 0; q < nnz; ++q)
+        if (indices[q] < 0 || indices[q] >= n) { set_error("rcm_order: column out of range"); return FEMD_EINVAL; }
+    std::vector<int> ip(indptr, indptr + n + 1), ix(indices, indices + nnz), out;
+    femd::rcm_order(n, ip, ix, out);
+    std::copy(out.begin(), out.end(), order);
+    return FEMD_OK;
+}
+
+// The reference coordinates of the nloc local nodes of equispaced P_k (the lattice of
+// femd_host_tabulate: the three vertices, k - 1 nodes per edge, then the interior): xi, eta.
+int femd_host_lagrange_nodes(int k, double *xi, double *eta)
+{
+    femd::clear_error();
+    if (k < 1 || k > 20 || !xi || !eta) { set_error("lagrange_nodes: bad arguments"); return -FEMD_EINVAL; }
+    int l = 0;
+    const int V[3][2] = {{0, 0}, {k, 0}, {0, k}};
+    for (auto &v : V) { xi[l] = (double)v[0] / k; eta[l] = (double)v[1] / k; ++l; }
+    for (int e = 0; e < 3; ++e)
+        for (int j = 1; j < k; ++j) {
+            int a[3] = {0, 0, 0};
+            a[(e + 1) % 3] = k - j;
+            a[(e + 2) % 3] = j;
+            xi[l] = (double)a[1] / k;
+            eta[l] = (double)a[2] / k;
+            ++l;
+        }
+    for (int j = 1; j < k; ++j)
+        for (int i = 1; i + j < k; ++i) { xi[l] = (double)i / k; eta[l] = (double)j / k; ++l; }
+    return l;
+}
+
+// The exterior facets of a rectangle mesh in (cell, local edge) order -- an edge (local edge i
+// joins vertices (i + 1) % 3 and (i + 2) % 3) held by one cell only -- with the marker of its side
+// of [x0, x1] x [y0, y1]: markers[0..3] for bottom, right, top, left, 0 for none
+// (include/femd/fe/space_2d.hpp:430-446 facets, mesh/structured.hpp:26-31 side markers).  cell,
+// local, marker: room for 3 ncells entries.  Returns the number of facets, or -FEMD_E*.
+int femd_host_exterior_facets(int nverts, int ncells, const int *tris, const double *points, double x0, double y0,
+                              double x1, double y1, const int *markers, int *cell, int *local, int *marker)
+{
+    femd::clear_error();
+    if (nverts < 3 || ncells < 1 || !tris || !points || !markers || !cell || !local || !marker) {
+        set_error("exterior_facets: bad arguments");
+        return -FEMD_EINVAL;
+    }
+    const size_t nh = (size_t)ncells * 3;
+    std::vector<uint64_t> keys(nh);
+    for (size_t t = 0; t < nh; ++t) {
+        const size_t c = t / 3;
+        const int i = (int)(t % 3);
+        const int a = tris[3 * c + (i + 1) % 3], b = tris[3 * c + (i + 2) % 3];
+        if (a < 0 || a >= nverts || b < 0 || b >= nverts) { set_error("exterior_facets: vertex index out of range"); return -FEMD_EINVAL; }
+        keys[t] = ((uint64_t)std::min(a, b) << 32) | (uint64_t)std::max(a, b);
+    }
+    std::vector<uint64_t> sorted(keys);
+    std::sort(sorted.begin(), sorted.end());
+    int nf = 0;
+    for (size_t t = 0; t < nh; ++t) {
+        const auto r = std::equal_range(sorted.begin(), sorted.end(), keys[t]);
+        if (r.second - r.first != 1) continue;
+        const size_t c = t / 3;
+        const int i = (int)(t % 3);
+        const int a = tris[3 * c + (i + 1) % 3], b = tris[3 * c + (i + 2) % 3];
+        const double ax = points[2 * a], ay = points[2 * a + 1], bx = points[2 * b], by = points[2 * b + 1];
+        int m = 0;
+        if (ay == y0 && by == y0) m = markers[0];
+        else if (ax == x1 && bx == x1) m = markers[1];
+        else if (ay == y1 && by == y1) m = markers[2];
+        else if (ax == x0 && bx == x0) m = markers[3];
+        cell[nf] = (int)c;
+        local[nf] = i;
+        marker[nf] = m;
+        ++nf;
+    }
+    return nf;
+}
+
+// The rule of a facet cache (include/femd/fe/cache_2d.hpp:126-149): Gauss-Legendre with
+// max(1, (degree + 2) / 2) points, on local edge i (from reference vertex (i + 1) % 3 to (i + 2) % 3)
+// at t = (node + 1) / 2: xi, eta (3 x nq), the Gauss weights gw (nq), and the P_k tabulation per
+// local edge ref (3 x nq x 3 x nloc).  Returns nq (at most 64), or -FEMD_E*.
+int femd_host_facet_rule(int k, int degree, double *xi, double *eta, double *gw, double *ref)
+{
+    femd::clear_error();
+    if (k < 1 || k > 20 || degree < 0 || !xi || !eta || !gw || !ref) { set_error("facet_rule: bad arguments"); return -FEMD_EINVAL; }
+    const int n = std::max(1, (degree + 2) / 2);
+    if (n > 64) { set_error("facet_rule: more than 64 points"); return -FEMD_EINVAL; }
+    double gx[64];
+    gauss_legendre(n, gx, gw);
+    const double vx[3] = {0.0, 1.0, 0.0}, vy[3] = {0.0, 0.0, 1.0};
+    const int nloc = (k + 1) * (k + 2) / 2;
+    for (int i = 0; i < 3; ++i) {
+        const int a = (i + 1) % 3, b = (i + 2) % 3;
+        for (int q = 0; q < n; ++q) {
+            const double t = 0.5 * (gx[q] + 1.0);
+            xi[i * n + q] = (1.0 - t) * vx[a] + t * vx[b];
+            eta[i * n + q] = (1.0 - t) * vy[a] + t * vy[b];
+        }
+        const int st = femd_host_tabulate(k, n, xi + i * n, eta + i * n, ref + (size_t)i * n * 3 * nloc);
+        if (st < 0) return st;
+    }
+    return n;
 }
 
 }  // extern "C"

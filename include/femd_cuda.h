@@ -224,6 +224,47 @@ FEMD_API int femd_cuda_eval_field(femd_ctx ctx, const femd_mesh2d *mesh, const f
                                   const double *field_dev, int ncodes, const int *codes, double *out_dev);
 
 /* ======================================================================================
+ * Facet (ds) terms and the Dirichlet lift.
+ * Replaces the exterior-facet cache Cache2D(V, degree, markers, all)
+ * (include/femd/fe/cache_2d.hpp:126-184) with assemble_matrix_2d / assemble_vector_2d on it
+ * (include/femd/forms/assembly_2d.hpp:173-305), i.e. the ds(marker) terms of a form (Robin and
+ * Neumann data), and the pieces of the Dirichlet lift of fd.solve(a, L, dirichlet=g)
+ * (python/femd/linalg.py:748-755, V.lift at python/femd/spaces2d.py:373-414).  A facet set is a
+ * list of (cell, local edge) -- local edge i joins the cell's vertices (i + 1) % 3 and (i + 2) % 3 --
+ * in the reference's facet order (femd_host_exterior_facets), on a cell pattern.  Assembly adds
+ * into K / f: every touched value gets its facets' element entries in increasing facet order, the
+ * order of the reference (no atomics).
+ * ====================================================================================== */
+typedef struct femd_facets_s *femd_facets;
+
+typedef struct {
+    int k, nloc, nq;
+    const double *xi_host, *eta_host;   /* 3 x nq: the points on local edge 0, 1, 2 (reference coordinates) */
+    const double *gw_host;              /* nq Gauss-Legendre weights on [-1, 1] */
+    const double *ref_host;             /* 3 x nq x 3 x nloc: the tabulation per local edge */
+} femd_facet_rule;
+
+/* A facet set on a cell pattern (copies the list; release with femd_cuda_release). */
+FEMD_API int femd_cuda_facets_create(femd_ctx ctx, femd_pattern p, int nf, const int *fcell_host, const int *flocal_host,
+                                     femd_facets *out);
+/* Per facet point [f nq + q]: x, y, the weight 0.5 gw len, the outward unit normal (any output may
+ * be NULL).  Synchronizes. */
+FEMD_API int femd_cuda_facet_points(femd_ctx ctx, femd_facets F, const femd_mesh2d *mesh, const femd_facet_rule *rule,
+                                    double *x_dev, double *y_dev, double *w_dev, double *nx_dev, double *ny_dev);
+/* K += sum_t integral over the facets of c_t (D^{a_t} phi_i)(D^{b_t} phi_j) ds; coef[t] a constant or
+ * an array at the facet points (FEMD_COEF_POINTS, [f nq + q]).  Synchronizes. */
+FEMD_API int femd_cuda_assemble_facet_matrix(femd_ctx ctx, femd_facets F, const femd_mesh2d *mesh,
+                                             const femd_facet_rule *rule, int nterms, const int *a, const int *b,
+                                             const femd_coef *coef, femd_matrix K);
+/* f += sum_t integral over the facets of c_t (D^{a_t} phi_i) ds.  Synchronizes. */
+FEMD_API int femd_cuda_assemble_facet_vector(femd_ctx ctx, femd_facets F, const femd_mesh2d *mesh,
+                                             const femd_facet_rule *rule, int nterms, const int *a, const femd_coef *coef,
+                                             double *f_dev);
+/* u_raw[raw_of[i]] = x[i] for i < n: a solution on the space's dofs written into the raw numbering
+ * over a lift (the reference's V.prolongate(c) + u_g, python/femd/spaces2d.py:373-385). */
+FEMD_API int femd_cuda_prolongate(femd_ctx ctx, int n, const int *raw_of_dev, const double *x_dev, double *u_raw_dev);
+
+/* ======================================================================================
  * Sparse kernels on a matrix.
  * ====================================================================================== */
 /* y = K x: CSRMatrix::apply (include/femd/sparse/csr.hpp:203-215). */
@@ -337,9 +378,19 @@ FEMD_API int femd_cuda_batch_step_lockstep(femd_ctx ctx, femd_batch B, int mixed
 /* Shape of the lockstep engine: nonzeros per row range of a member (one thread block each;
  * default 16384), iterations enqueued between two reads of the members' states (default 8), the
  * SpMV by windows of whole rows read by coalesced loads (windows = 1) or by row groups of a few
- * lanes per row (0, the default).  0 (-1 for windows) keeps the current value.  No reference
+ * lanes per row (0, the default), and in mixed precision the compact layout (compact = 1, the
+ * default): each member's FP32 matrix and vectors in a reverse Cuthill-McKee order of its
+ * pattern (built once per pattern on the host, kept with the pattern), column indices as 16-bit
+ * offsets from the row (6 bytes per nonzero instead of 8), and the SpMV reading the search
+ * direction from a shared-memory window of each row range instead of gathering it from global
+ * memory; a pattern whose reordered bandwidth exceeds 32767 or whose windows exceed 12288 columns
+ * keeps the plain layout.  0 (-1 for windows and compact) keeps the current value.  No reference
  * counterpart. */
-FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry, int chunk, int windows);
+FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry, int chunk, int windows, int compact);
+/* The last lockstep solve's layout (out: 4 entries): [0] members in the compact layout, [1] members
+ * in the plain layout, [2] the widest shared-memory column window (columns), [3] table entries.
+ * Instrumentation with no reference counterpart. */
+FEMD_API int femd_cuda_batch_lockstep_stats(femd_batch B, long long *out);
 /* Add a member (a square matrix with its Jacobi inverse diagonal); *id_out its id (a free id is
  * reused).  Remove frees its solver vectors; a removed member's solve is dropped. */
 FEMD_API int femd_cuda_batch_add(femd_batch B, femd_matrix K, int *id_out);
@@ -407,8 +458,28 @@ FEMD_API int femd_host_rectangle_mesh(double x0, double y0, double x1, double y1
  * include/femd/fe/space_2d.hpp:390-526).  cell_dofs: ncells x nloc; returns dim via *dim. */
 FEMD_API int femd_host_lagrange_numbering(int nverts, int ncells, const int *tris, int k, int all_exterior, int *cell_dofs,
                                  int *dim, int *raw_dim);
+/* The raw numbering of the same space (no node eliminated; include/femd/fe/space_2d.hpp:448-470):
+ * cell_raw ncells x nloc, *raw_dim the node count. */
+FEMD_API int femd_host_lagrange_raw(int nverts, int ncells, const int *tris, int k, int *cell_raw, int *raw_dim);
+/* The reference coordinates of the nloc local nodes of equispaced P_k (vertices, edge nodes, interior);
+ * returns nloc. */
+FEMD_API int femd_host_lagrange_nodes(int k, double *xi, double *eta);
+/* The exterior facets of a rectangle mesh [x0, x1] x [y0, y1] in (cell, local edge) order with the
+ * marker of their side (markers[0..3]: bottom, right, top, left; 0 elsewhere)
+ * (include/femd/fe/space_2d.hpp:430-446, include/femd/mesh/structured.hpp:26-31).  cell, local,
+ * marker: room for 3 ncells.  Returns the facet count. */
+FEMD_API int femd_host_exterior_facets(int nverts, int ncells, const int *tris, const double *points, double x0, double y0,
+                                       double x1, double y1, const int *markers, int *cell, int *local, int *marker);
+/* The facet rule of Cache2D(V, degree, ..., true) (include/femd/fe/cache_2d.hpp:126-149):
+ * max(1, (degree + 2) / 2) Gauss-Legendre points; xi, eta: 3 x nq, gw: nq, ref: 3 x nq x 3 x nloc.
+ * Returns nq (<= 64). */
+FEMD_API int femd_host_facet_rule(int k, int degree, double *xi, double *eta, double *gw, double *ref);
 /* TriangleQuadrature(degree) (include/femd/quadrature/triangle.hpp:24-58): returns nq (<= 64). */
 FEMD_API int femd_host_triangle_quadrature(int degree, double *xi, double *eta, double *w);
+/* A reverse Cuthill-McKee order of a square CSR pattern: order[new] = old (George and Liu's
+ * pseudo-peripheral start per connected component, neighbours by increasing degree, reversed) --
+ * the order of the batched engine's compact layout.  No reference counterpart. */
+FEMD_API int femd_host_rcm_order(int n, const int *indptr, const int *indices, int *order);
 /* The equispaced P_k basis and its reference derivatives at points: out[q][3][nloc]. */
 FEMD_API int femd_host_tabulate(int k, int nq, const double *xi, const double *eta, double *out);
 
