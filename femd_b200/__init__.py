@@ -4,8 +4,8 @@ The compute runs in libfemd_cuda.so (hand-written CUDA, C ABI in include/femd_cu
 package is the host-side mirror of the reference's interface for that path.  Importing it
 loads the library and fails if it is missing -- there is no CPU fallback.
 """
-from .core import (Cache2D, Coef, Context, CSRMatrix, JacobiPreconditioner, LagrangeSpace2D, Mesh2D,  # noqa: F401
-                   SparsityPattern, assemble_matrix_2d, assemble_vector_2d, cell_pattern, cg_solve, cg_solve_host,
+from .core import (Cache2D, Coef, Context, CSRMatrix, ILU0Preconditioner, JacobiPreconditioner,  # noqa: F401
+                   LagrangeSpace2D, Mesh2D, SSORPreconditioner, SparsityPattern, assemble_matrix_2d, assemble_vector_2d, cell_pattern, cg_solve, cg_solve_host,
                    context, quad_degree, rectangle_mesh, scatter_map_2d)
 from .krylov import KrylovInfo, cg  # noqa: F401
 from ._native import FemdError, lib  # noqa: F401

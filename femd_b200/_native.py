@@ -12,7 +12,9 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfemd_cuda.so")
 
-FEMD_OK, FEMD_EINVAL, FEMD_ENOMEM, FEMD_ECUDA, FEMD_EOUTSIDE, FEMD_EZERODIAG, FEMD_ETIMEOUT, FEMD_EABORT = range(8)
+FEMD_OK, FEMD_EINVAL, FEMD_ENOMEM, FEMD_ECUDA, FEMD_EOUTSIDE, FEMD_EZERODIAG, FEMD_ETIMEOUT, FEMD_EABORT, FEMD_EPIVOT = \
+    range(9)
+PC_ILU0, PC_SSOR = 1, 2
 COEF_CONST, COEF_POINTS, COEF_SINSIN, COEF_SINSIN_HELM, COEF_FIELD = range(5)
 ASM_FAST, ASM_EXACT = 0, 1
 
@@ -98,6 +100,10 @@ SIGNATURES = {
     "femd_cuda_cg_jacobi": (_I, [_P, _P, _I, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_cg_solve_host": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_kernel_time": (_I, [_P, _P, _I, _I, C.POINTER(C.c_double)]),
+    "femd_cuda_precond_create": (_I, [_P, _P, _I, _D, C.POINTER(_P)]),
+    "femd_cuda_precond_info": (_I, [_P, _PI, _PI, _PI, C.POINTER(C.c_double)]),
+    "femd_cuda_precond_apply": (_I, [_P, _P, _P, _P]),
+    "femd_cuda_cg_precond": (_I, [_P, _P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_pcg_mixed": (_I, [_P, _P, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_cg_jacobi_noalloc": (_I, [_P, _P, _I, _P, _P, _I, _D, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_create": (_I, [_P, _I, _P, _I, C.POINTER(_P)]),
@@ -162,7 +168,7 @@ def check(status: int, what: str = ""):
         e = ValueError(msg)
     elif status == FEMD_ENOMEM:
         e = MemoryError(msg)
-    elif status == FEMD_EOUTSIDE:
+    elif status in (FEMD_EOUTSIDE, FEMD_EPIVOT):
         e = RuntimeError(msg)
     else:
         e = FemdError(status, msg)

@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfemd_cuda.so")
-SOURCES = ["core.cu", "pattern.cu", "assemble.cu", "krylov.cu", "batch.cu", "numbering.cu", "forms.cu", "facets.cu", "setup_host.cpp"]
+SOURCES = ["core.cu", "pattern.cu", "assemble.cu", "krylov.cu", "batch.cu", "numbering.cu", "forms.cu", "facets.cu", "precond.cu", "setup_host.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",

@@ -475,6 +475,59 @@ class JacobiPreconditioner:
         return out[:self.size]
 
 
+class _PCBase(_Handle):
+    """A preconditioner of libfemd_cuda (femd_precond) built from a square CSRMatrix."""
+
+    def __init__(self, K: CSRMatrix, kind, omega, name):
+        if K.nrows != K.ncols:
+            raise ValueError(f"{name}: the matrix must be square")
+        h = C.c_void_p()
+        K.ctx.enter()
+        check(lib.femd_cuda_precond_create(K.ctx.h, K.h, int(kind), float(omega), C.byref(h)))
+        super().__init__(h)
+        self.K, self.ctx, self.size = K, K.ctx, K.nrows
+        k, lf, lb, mp = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        check(lib.femd_cuda_precond_info(h, C.byref(k), C.byref(lf), C.byref(lb), C.byref(mp)))
+        self.levels = (lf.value, lb.value)
+        self._min_pivot = mp.value
+
+    def apply(self, r):
+        """z = M^{-1} r for a device or host vector (returns a float64 device tensor)."""
+        torch = _torch()
+        rv = _as_device(r, self.ctx)
+        if rv.numel() != self.size:
+            raise ValueError(f"{self.name}: vector length differs from the matrix")
+        z = torch.empty_like(rv)
+        self.ctx.enter()
+        check(lib.femd_cuda_precond_apply(self.ctx.h, self.h, _ptr(rv), _ptr(z)))
+        self.ctx.leave()
+        return z
+
+
+class ILU0Preconditioner(_PCBase):
+    """Incomplete LU with no fill on the pattern of K, natural ordering (ILU0Preconditioner,
+    include/femd/sparse/precond.hpp:151-213): factors and applications bit-identical to the
+    reference's.  Raises ValueError on a zero diagonal entry and RuntimeError on a zero pivot."""
+
+    def __init__(self, K: CSRMatrix):
+        super().__init__(K, N.PC_ILU0, 1.0, "ILU(0)")
+        self.name = "ilu0"
+
+    def min_pivot(self):
+        """The smallest pivot met (negative: the factorization is indefinite, not for CG)."""
+        return self._min_pivot
+
+
+class SSORPreconditioner(_PCBase):
+    """Symmetric SOR, M = w/(2-w) (D/w + L) (D/w)^{-1} (D/w + U), natural ordering
+    (SSORPreconditioner, include/femd/sparse/precond.hpp:105-149)."""
+
+    def __init__(self, K: CSRMatrix, omega: float = 1.0):
+        super().__init__(K, N.PC_SSOR, omega, "SSOR")
+        self.name = "ssor"
+        self.omega = float(omega)
+
+
 # ---- coefficients and assembly ---------------------------------------------------------------
 class Coef:
     """A term coefficient: Coef.const(v), Coef.sinsin(p0, p1, a, b) = p0 + p1 sin(a x) sin(b y),
@@ -586,10 +639,22 @@ def cg_solve(A: CSRMatrix, M, b, x0, max_iter: int, tol: float, *, mixed: bool =
     x = (torch.zeros(n, dtype=torch.float64, device=bv.device) if x0 is None else _as_device(x0, A.ctx).clone())
     if x.numel() != n:
         raise ValueError("cg: x0 and b differ in length")
-    if M is not None and not isinstance(M, JacobiPreconditioner):
-        raise TypeError("cg_solve: M is None or a JacobiPreconditioner on this path")
+    if M is not None and not isinstance(M, (JacobiPreconditioner, _PCBase)):
+        raise TypeError("cg_solve: M is None, a JacobiPreconditioner, an ILU0Preconditioner or an SSORPreconditioner")
     if M is not None and M.size != n:
         raise ValueError("krylov: preconditioner and right-hand side differ in size")
+    if isinstance(M, _PCBase):
+        # krylov::cg with a general preconditioner (cg.hpp:245-290)
+        if mixed:
+            raise ValueError("pcg_mixed: the mixed-precision solve is Jacobi-preconditioned")
+        if M.K.pattern is not A.pattern:
+            raise ValueError("krylov: the preconditioner was built on another matrix pattern")
+        A.ctx.enter()
+        res = N.femd_cg_result()
+        check(lib.femd_cuda_cg_precond(A.ctx.h, A.h, M.h, _ptr(bv), _ptr(x), int(max_iter), float(tol), C.byref(res)))
+        A.ctx.leave()
+        cg_solve.last = res
+        return x, bool(res.converged), int(res.iterations), float(res.residual), bool(res.breakdown)
     if M is not None and M.K is not A:
         # the preconditioner of another matrix: its inverse diagonal becomes A's
         _, inv = M.K._arrays()

@@ -39,7 +39,8 @@ void clear_error();
 
 // ---- handles ------------------------------------------------------------------------------
 enum HandleKind : uint32_t { KIND_PATTERN = 0x50415454u, KIND_MATRIX = 0x4d415452u, KIND_SOLVER = 0x534f4c56u,
-                             KIND_BATCH = 0x42415443u, KIND_FACETS = 0x46414354u };
+                             KIND_BATCH = 0x42415443u, KIND_FACETS = 0x46414354u,
+                             KIND_PRECOND = 0x50524543u };
 
 struct HandleBase {
     uint32_t kind;
@@ -93,6 +94,11 @@ struct femd_ctx_s {
 namespace femd {
 void ctx_retain(femd_ctx ctx);
 void ctx_release(femd_ctx ctx);
+// the preconditioners of precond.cu: z = M^{-1} r enqueued on s (skipped when *skip is set)
+int precond_enqueue(femd_precond P, const double *r, double *z, const int *skip, cudaStream_t s);
+int precond_rows(femd_precond P);
+femd_ctx precond_ctx(femd_precond P);
+femd_pattern precond_pattern(femd_precond P);
 }  // namespace femd
 
 struct femd_pattern_s : femd::HandleBase {

@@ -205,7 +205,7 @@ void femd_cuda_release(void *handle)
     if (!handle) return;
     HandleBase *h = static_cast<HandleBase *>(handle);
     if (h->kind == KIND_PATTERN || h->kind == KIND_MATRIX || h->kind == KIND_SOLVER || h->kind == KIND_BATCH ||
-        h->kind == KIND_FACETS) {
+        h->kind == KIND_FACETS || h->kind == KIND_PRECOND) {
         h->kind = 0;
         delete h;
     }

@@ -290,6 +290,107 @@ __global__ void __launch_bounds__(RED_BLOCK) k_cg_finish(const double *__restric
     }
 }
 
+// ---- CG with a general preconditioner M (cg.hpp:245-290) -------------------------------------
+// start: r = b - Ax; nb, ||r||; done when b = 0 or ||r|| <= tol ||b|| (then M and the loop are skipped)
+__global__ void __launch_bounds__(RED_BLOCK) k_pc_start(const double *__restrict__ b, const double *__restrict__ Ax,
+                                                        double *__restrict__ r, int n, double *__restrict__ part,
+                                                        CGState<double> *__restrict__ st, double tol)
+{
+    __shared__ double sh[64];
+    double bb = 0.0, rr = 0.0;
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
+        const double bi = b[i], ri = bi - Ax[i];
+        r[i] = ri;
+        bb += bi * bi;
+        rr += ri * ri;
+    }
+    double v[2] = {bb, rr};
+    block_reduce<double, 2>(v, sh);
+    if (threadIdx.x == 0) { part[blockIdx.x] = v[0]; part[gridDim.x + blockIdx.x] = v[1]; }
+    if (!last_block(&st->ticket)) return;
+    double tot[2];
+    reduce_partials<double, 2>(part, gridDim.x, gridDim.x, tot, sh);
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        const double nb = sqrt(tot[0]), rn = sqrt(tot[1]);
+        st->nb = nb;
+        st->tol_nb = tol * nb;
+        st->rn = rn;
+        st->it = 0;
+        st->breakdown = 0;
+        st->done = nb == 0.0 || rn <= tol * nb;                           // cg.hpp:259, 265
+    }
+}
+
+// rz = r.z; FIRST: p = z and the breakdown test of the loop top (cg.hpp:266-271); else
+// beta = rz_new / rz (cg.hpp:283-285), and the loop top's test on the new rz
+template <bool FIRST>
+__global__ void __launch_bounds__(RED_BLOCK) k_pc_rz(const double *__restrict__ r, const double *__restrict__ z,
+                                                     double *__restrict__ p, int n, double *__restrict__ part,
+                                                     CGState<double> *__restrict__ st)
+{
+    __shared__ double sh[32];
+    if (st->done) return;
+    double rz = 0.0;
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
+        rz += r[i] * z[i];
+        if (FIRST) p[i] = z[i];
+    }
+    double v[1] = {rz};
+    block_reduce<double, 1>(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    if (!last_block(&st->ticket)) return;
+    double tot[1];
+    reduce_partials<double, 1>(part, gridDim.x, 0, tot, sh);
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        const double rzn = tot[0];
+        if (!FIRST) st->beta = rzn / st->rz;
+        st->rz = rzn;
+        if (!(rzn > 0.0)) { st->breakdown = 1; st->done = 1; }
+    }
+}
+
+// x += a p; r -= a Ap; ||r||; the stopping test (cg.hpp:278-281)
+__global__ void __launch_bounds__(RED_BLOCK) k_pc_update(double *__restrict__ x, double *__restrict__ r,
+                                                         const double *__restrict__ p, const double *__restrict__ Ap, int n,
+                                                         double *__restrict__ part, CGState<double> *__restrict__ st)
+{
+    __shared__ double sh[32];
+    if (st->done) return;
+    const double a = st->alpha;
+    double rr = 0.0;
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) {
+        const double ri = r[i] - a * Ap[i];
+        r[i] = ri;
+        x[i] = x[i] + a * p[i];
+        rr += ri * ri;
+    }
+    double v[1] = {rr};
+    block_reduce<double, 1>(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    if (!last_block(&st->ticket)) return;
+    double tot[1];
+    reduce_partials<double, 1>(part, gridDim.x, 0, tot, sh);
+    if (threadIdx.x == 0) {
+        st->ticket = 0;
+        st->rr = tot[0];
+        st->it += 1;
+        const double rn = sqrt(tot[0]);
+        st->rn = rn;
+        if (rn <= st->tol_nb || st->it >= st->max_iter) st->done = 1;
+    }
+}
+
+// p = z + beta p (cg.hpp:286-288)
+__global__ void __launch_bounds__(RED_BLOCK) k_pc_direction(double *__restrict__ p, const double *__restrict__ z, int n,
+                                                            const CGState<double> *__restrict__ st)
+{
+    if (st->done) return;
+    const double b = st->beta;
+    for (int i = blockIdx.x * RED_BLOCK + threadIdx.x; i < n; i += gridDim.x * RED_BLOCK) p[i] = z[i] + b * p[i];
+}
+
 // ---- mixed precision kernels -----------------------------------------------------------------
 // x64 += d32; d32 = 0 (reliable update of the solution), when st32->want_ru
 __global__ void k_mixed_flush(double *__restrict__ x, float *__restrict__ d, int n, const CGState<float> *__restrict__ st)
@@ -527,10 +628,18 @@ struct SolverWS {
     cudaGraphExec_t xm = nullptr;
     size_t nodesm = 0;
     int chm = 0;
+    // CG with a general preconditioner: z, and the graph of a chunk for the preconditioner it was
+    // captured with
+    DevBuf<double> z;
+    cudaGraphExec_t xpc = nullptr;
+    size_t nodespc = 0;
+    femd_precond pc_for = nullptr;
+    int chpc = 0;
     ~SolverWS()
     {
         for (auto &g : x64) if (g) cudaGraphExecDestroy(g);
         if (xm) cudaGraphExecDestroy(xm);
+        if (xpc) cudaGraphExecDestroy(xpc);
         for (cudaEvent_t e : {e0, e1, ev[0], ev[1]}) if (e) cudaEventDestroy(e);
         if (st_host) cudaFreeHost(st_host);
         if (maxit_host) cudaFreeHost(maxit_host);
@@ -866,6 +975,108 @@ static int mixed_run(femd_ctx ctx, femd_matrix K, const double *b_in, double *x_
     return status;
 }
 
+// CG preconditioned by P (cg.hpp:245-290) on the matrix's workspace: the loop in captured chunks
+// of CH iterations (SpMV with p.Ap, update, M, r.z, direction), polled between chunks.
+static int pc_run(femd_ctx ctx, femd_matrix K, femd_precond P, const double *b, double *x, int max_iter, double tol,
+                  femd_cg_result *res)
+{
+    femd_pattern Q = K->pattern;
+    const int n = Q->nrows;
+    cudaStream_t s = ctx->stream;
+    SolverWS *Wp = nullptr;
+    FEMD_TRY(get_ws(ctx, K, &Wp));
+    SolverWS &W = *Wp;
+    if (!W.z.p) FEMD_TRY(W.z.alloc((size_t)n + 1));
+    const unsigned gs = W.gs, gr = W.gr;
+    const int *done = &W.st.p->done;
+    if (W.pc_for != P) {
+        if (W.xpc) cudaGraphExecDestroy(W.xpc);
+        W.xpc = nullptr;
+        W.pc_for = P;
+        W.chpc = n > (1 << 18) ? 2 : 8;
+        cudaGraph_t graph = nullptr;
+        FEMD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        int st = FEMD_OK;
+        for (int k = 0; k < W.chpc && st == FEMD_OK; ++k) {
+            launch_spmv<double, double, true>(W.shape, gs, s, Q->indptr.p, Q->indices.p, K->data.p, W.p.p, W.Ap.p, n, W.part.p,
+                                              W.st.p);
+            k_pc_update<<<gr, RED_BLOCK, 0, counted(s)>>>(W.wx.p, W.r.p, W.p.p, W.Ap.p, n, W.part.p, W.st.p);
+            st = precond_enqueue(P, W.r.p, W.z.p, done, s);
+            k_pc_rz<false><<<gr, RED_BLOCK, 0, counted(s)>>>(W.r.p, W.z.p, nullptr, n, W.part.p, W.st.p);
+            k_pc_direction<<<gr, RED_BLOCK, 0, counted(s)>>>(W.p.p, W.z.p, n, W.st.p);
+        }
+        cudaError_t ce = cudaStreamEndCapture(s, &graph);
+        if (st != FEMD_OK) { if (graph) cudaGraphDestroy(graph); W.pc_for = nullptr; return st; }
+        if (ce != cudaSuccess) {
+            W.pc_for = nullptr;
+            set_error(std::string("cg: graph capture: ") + cudaGetErrorString(ce));
+            return FEMD_ECUDA;
+        }
+        ce = cudaGraphInstantiate(&W.xpc, graph, 0);
+        cudaGraphGetNodes(graph, nullptr, &W.nodespc);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) {
+            W.xpc = nullptr;
+            W.pc_for = nullptr;
+            set_error(std::string("cg: graph instantiate: ") + cudaGetErrorString(ce));
+            return FEMD_ECUDA;
+        }
+    }
+    *W.maxit_host = max_iter;
+    FEMD_TRY_CUDA(cudaEventRecord(W.e0, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.wb.p, b, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(W.wx.p, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    FEMD_TRY_CUDA(cudaMemsetAsync(W.st.p, 0, sizeof(CGState<double>), s));
+    launch_spmv<double, double, false>(W.shape, gs, s, Q->indptr.p, Q->indices.p, K->data.p, W.wx.p, W.Ap.p, n, nullptr, nullptr);
+    k_pc_start<<<gr, RED_BLOCK, 0, counted(s)>>>(W.wb.p, W.Ap.p, W.r.p, n, W.part.p, W.st.p, tol);
+    FEMD_TRY(precond_enqueue(P, W.r.p, W.z.p, done, s));
+    k_pc_rz<true><<<gr, RED_BLOCK, 0, counted(s)>>>(W.r.p, W.z.p, W.p.p, n, W.part.p, W.st.p);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&W.st.p->max_iter, W.maxit_host, sizeof(int), cudaMemcpyHostToDevice, s));
+    int status = FEMD_OK;
+    const long long max_chunks = (long long)max_iter / W.chpc + 2;
+    cudaError_t ce = cudaSuccess;
+    for (long long c = 0; c < max_chunks && ce == cudaSuccess; ++c) {
+        ce = launch_graph(W.xpc, W.nodespc, s);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(W.st_host, W.st.p, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+        if (ce == cudaSuccess && W.st_host->done) break;
+    }
+    if (ce != cudaSuccess) { set_error(std::string("cg: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; }
+    if (status == FEMD_OK) {
+        // finish (cg.hpp:222-237)
+        launch_spmv<double, double, false>(W.shape, gs, s, Q->indptr.p, Q->indices.p, K->data.p, W.wx.p, W.Ap.p, n, nullptr,
+                                           nullptr);
+        k_cg_finish<<<gr, RED_BLOCK, 0, counted(s)>>>(W.wb.p, W.Ap.p, W.r.p, n, W.part.p, W.st.p);
+        ce = cudaMemcpyAsync(W.st_host, W.st.p, sizeof(CGState<double>), cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(x, W.wx.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (ce == cudaSuccess) ce = cudaEventRecord(W.e1, s);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+        if (ce != cudaSuccess) { set_error(std::string("cg: ") + cudaGetErrorString(ce)); status = FEMD_ECUDA; }
+    }
+    if (status == FEMD_OK) {
+        const CGState<double> &S = *W.st_host;
+        if (S.nb == 0.0) {
+            cudaMemsetAsync(x, 0, (size_t)n * sizeof(double), s);
+            cudaStreamSynchronize(s);
+            *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
+        } else {
+            res->iterations = S.it;
+            res->breakdown = S.breakdown;
+            res->residual = S.res64 / S.nb;
+            int conv = !S.breakdown && res->residual <= tol * (1.0 + 1e-6) + 1e-15;
+            if (!conv && !S.breakdown && res->residual <= 10.0 * tol && S.it < max_iter) conv = 1;
+            res->converged = conv;
+            res->status = FEMD_OK;
+            res->outer = 0;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, W.e0, W.e1);
+        res->seconds = ms * 1e-3;
+    }
+    return status;
+}
+
 }  // namespace femd
 
 using namespace femd;
@@ -1191,6 +1402,24 @@ int femd_cuda_kernel_time(femd_ctx ctx, femd_matrix K, int kernel, int reps, dou
     FEMD_TRY_CUDA(cudaEventElapsedTime(&ms, W.e0, W.e1));
     *us_out = (double)ms * 1e3 / reps;
     return FEMD_OK;
+}
+
+int femd_cuda_cg_precond(femd_ctx ctx, femd_matrix K, femd_precond P, const double *b_dev, double *x_dev, int max_iter,
+                         double tol, femd_cg_result *res)
+{
+    clear_error();
+    K = as_matrix(K);
+    FEMD_CHECK_ARG(ctx && K && P && res, "cg: NULL argument");
+    FEMD_CHECK_ARG(K->pattern->nrows == K->pattern->ncols, "cg: the matrix must be square");
+    FEMD_CHECK_ARG(precond_pattern(P) == K->pattern && precond_ctx(P) == ctx,
+                   "krylov: the preconditioner was built on another matrix pattern or context");
+    const int n = K->pattern->nrows;
+    FEMD_CHECK_ARG(n == 0 || (b_dev && x_dev), "cg: NULL vector");
+    FEMD_CHECK_ARG(max_iter >= 0, "cg: max_iter must be >= 0");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
+    if (n == 0) return FEMD_OK;
+    return pc_run(ctx, K, P, b_dev, x_dev, max_iter, tol, res);
 }
 
 int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host, const int *indices_host, const double *data_host,

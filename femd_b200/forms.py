@@ -25,8 +25,8 @@ import warnings
 import numpy as np
 
 from . import _native as N
-from .core import (Cache2D, Coef, CSRMatrix, JacobiPreconditioner, LagrangeSpace2D, _torch, assemble_matrix_2d,
-                   assemble_vector_2d, cg_solve, check, context, lib)
+from .core import (Cache2D, Coef, CSRMatrix, ILU0Preconditioner, JacobiPreconditioner, LagrangeSpace2D,
+                   SSORPreconditioner, _torch, assemble_matrix_2d, assemble_vector_2d, cg_solve, check, context, lib)
 from .krylov import KrylovInfo
 
 # opcodes of the reference's instruction set (integrand.hpp:33-45)
@@ -380,12 +380,13 @@ class SparseSolver:
     340-483): solve(b, into=None, lift=None) as the reference's does, .backend, .info (the
     KrylovInfo of the last solve).
 
-    backend "cg" / "cuda-cg": Jacobi-PCG in FP64 (krylov.cg with M="jacobi" or None);
-    "cuda-cg-mixed": the FP32-inner / FP64-refined PCG; "auto" (the reference's default picks
-    its sparse Cholesky for a symmetric matrix with a positive diagonal, which this path does not
-    build): Jacobi-PCG for such a matrix, and ValueError otherwise.  The matrix, its inverse
-    diagonal and the solver's workspace (vectors, captured CUDA graphs) stay resident between
-    solves."""
+    backend "cg": krylov.cg with the reference's default M="ilu0" (ILU(0), natural ordering,
+    the reference's factors; "ssor", "jacobi" or None too); "cuda-cg": Jacobi-PCG in FP64 (the fast
+    path: the fused SpMV / update kernels); "cuda-cg-mixed": the FP32-inner / FP64-refined PCG;
+    "auto" (the reference's default picks its sparse Cholesky for a symmetric matrix with a
+    positive diagonal, which this path does not build): Jacobi-PCG for such a matrix, and
+    ValueError otherwise.  The matrix, its preconditioner and the solver's workspace (vectors,
+    captured CUDA graphs) stay resident between solves."""
 
     def __init__(self, A: CSRMatrix, backend="auto", **options):
         b = getattr(backend, "name", backend)
@@ -396,7 +397,7 @@ class SparseSolver:
             raise ValueError(f"unknown backend {backend!r} on the GPU path: 'auto' (default), 'cg' / 'cuda-cg' "
                              "(Jacobi-PCG) or 'cuda-cg-mixed'")
         self.A, self.info = A, None
-        M = options.pop("M", "jacobi")
+        M = options.pop("M", "ilu0" if b == "cg" else "jacobi")
         self.tol = float(options.pop("tol", 1e-10))
         self.maxiter = options.pop("maxiter", None)
         self.x0 = options.pop("x0", None)
@@ -409,13 +410,14 @@ class SparseSolver:
                                  "(Jacobi-PCG); this one is not (SparseMatrix.symmetric is False or a diagonal entry "
                                  "is <= 0)")
             b = "cuda-cg"
-        self.backend = "cuda-cg" if b == "cg" else b
+        self.backend = b
         if isinstance(M, str):
-            if M.lower() != "jacobi":
-                raise ValueError(f"preconditioner {M!r}: the GPU path has 'jacobi' (or None)")
-            M = JacobiPreconditioner(A)
-        if M is not None and not isinstance(M, JacobiPreconditioner):
-            raise TypeError("solver(): M is 'jacobi', a JacobiPreconditioner or None on the GPU path")
+            M = preconditioner(A, M)
+        if M is not None and not isinstance(M, (JacobiPreconditioner, ILU0Preconditioner, SSORPreconditioner)):
+            raise TypeError("solver(): M is 'ilu0', 'ssor', 'jacobi', a preconditioner of this path or None")
+        if self.backend in ("cuda-cg", "cuda-cg-mixed") and not (M is None or isinstance(M, JacobiPreconditioner)):
+            raise ValueError(f"solver({self.backend!r}): the fused GPU loop is Jacobi-preconditioned; use backend 'cg' for "
+                             f"{M.name}")
         if self.backend == "cuda-cg-mixed" and M is None:
             raise ValueError("solver('cuda-cg-mixed'): the mixed-precision solve is Jacobi-preconditioned")
         self._M = M
@@ -452,6 +454,21 @@ class SparseSolver:
 
     def __repr__(self):
         return f"SparseSolver({self.backend}, n={self.size})"
+
+
+def preconditioner(A: CSRMatrix, name: str):
+    """A.preconditioner(name) (python/femd/sparse.py): "ilu0", "ssor" or "jacobi"."""
+    n = str(name).lower()
+    if n == "ilu0":
+        return ILU0Preconditioner(A)
+    if n == "ssor":
+        return SSORPreconditioner(A)
+    if n == "jacobi":
+        return JacobiPreconditioner(A)
+    raise ValueError(f"preconditioner {name!r}: 'ilu0', 'ssor' or 'jacobi' on the GPU path")
+
+
+CSRMatrix.preconditioner = preconditioner
 
 
 def solver(A: CSRMatrix, backend="auto", **options) -> SparseSolver:

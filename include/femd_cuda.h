@@ -47,10 +47,12 @@ extern "C" {
 #define FEMD_EZERODIAG   5   /* Jacobi: zero diagonal entry (reference: std::invalid_argument) */
 #define FEMD_ETIMEOUT    6   /* a bounded device-side wait ran out (batched / served solves) */
 #define FEMD_EABORT      7   /* a host-requested abort stopped a batched solve */
+#define FEMD_EPIVOT      8   /* ILU(0): a zero pivot (reference: std::runtime_error -> RuntimeError) */
 
 typedef struct femd_ctx_s *femd_ctx;
 typedef struct femd_pattern_s *femd_pattern;
 typedef struct femd_matrix_s *femd_matrix;
+typedef struct femd_precond_s *femd_precond;
 
 /* Last error text of this host thread ("" when none). */
 FEMD_API const char *femd_cuda_last_error(void);
@@ -316,6 +318,31 @@ FEMD_API int femd_cuda_cg_solve_host(femd_ctx ctx, int n, const int *indptr_host
  * direction update p = D^-1 r + b p.  Runs on K's solver workspace with a = b = 0 (the same bytes
  * as a real iteration).  Instrumentation with no reference counterpart.  Synchronizes. */
 FEMD_API int femd_cuda_kernel_time(femd_ctx ctx, femd_matrix K, int kernel, int reps, double *us_out);
+
+/* ======================================================================================
+ * The stronger preconditioners: ILU(0) and SSOR on the natural ordering, and CG with them.
+ * Replace ILU0Preconditioner(A) and SSORPreconditioner(A, omega) (include/femd/sparse/precond.hpp:
+ * 105-213; python/src/femd_bindings*.cpp, A.preconditioner("ilu0" / "ssor")) and krylov::cg with a
+ * general preconditioner (include/femd/krylov/cg.hpp:245-290), reached by A.solver("cg") whose
+ * default M is "ilu0" (python/femd/sparse.py:440-446).  The factors and every application are
+ * bit-identical to the reference's (each row's arithmetic is the reference's, rows of one level of
+ * the triangular dependency done together); CG's reductions are deterministic in their own order.
+ * Errors: FEMD_EINVAL "ILU(0): zero diagonal entry in row i" / "SSOR: ..." and "SSOR: omega must
+ * lie in (0, 2)"; FEMD_EPIVOT "ILU(0): zero pivot in row i".  The preconditioner copies K's values
+ * (later changes to K do not reach it) and keeps K's pattern.
+ * ====================================================================================== */
+#define FEMD_PC_ILU0 1
+#define FEMD_PC_SSOR 2
+FEMD_API int femd_cuda_precond_create(femd_ctx ctx, femd_matrix K, int kind, double omega, femd_precond *out);
+/* kind, the forward and backward level counts (the sweeps' sequential steps), ILU(0)'s smallest pivot
+ * (min_pivot(): negative means the factorization is indefinite). */
+FEMD_API int femd_cuda_precond_info(femd_precond P, int *kind, int *levels_forward, int *levels_backward, double *min_pivot);
+/* z = M^{-1} r (r and z device vectors of nrows, distinct), asynchronous on the context's stream. */
+FEMD_API int femd_cuda_precond_apply(femd_ctx ctx, femd_precond P, const double *r_dev, double *z_dev);
+/* krylov::cg(A, M, x, b, max_iter, tol) with M = P (built on K's pattern): the stopping rule, final true
+ * residual, 10 tol acceptance and breakdown tests of cg.hpp:245-290 and 222-237. */
+FEMD_API int femd_cuda_cg_precond(femd_ctx ctx, femd_matrix K, femd_precond P, const double *b_dev, double *x_dev,
+                                  int max_iter, double tol, femd_cg_result *res);
 
 /* Mixed precision: inner Jacobi-PCG on an FP32 copy of K with FP32 vectors and FP32
  * accumulation; the residual r = b - A x is recomputed on the FP64 matrix and the solution
