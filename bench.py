@@ -646,7 +646,7 @@ def ours_c4(args, rank, world, dist):
     alg = batch_bytes(last, lib, mixed=True)
     t_launch = launch_s[-1]
     achieved = alg / t_launch / 1e9
-    lockstep = args.engine == "lockstep"
+    lockstep = args.engine in ("lockstep", "continuous")
     traffic = _traffic("k_ls_spmv_mixed_traffic.json" if lockstep else "k_batch_pcg_traffic.json", alg)
     nnz = sum(lib.get(sp["N"], sp["k"])["nnz"] for sp in spec)
     n = sum(lib.get(sp["N"], sp["k"])["n"] for sp in spec)
@@ -668,7 +668,8 @@ def ours_c4(args, rank, world, dist):
                    "served_over_plain": round(value / pst["solves_per_s"], 3),
                    "checker": chk,
                    "engine": args.engine,
-                   "batch_shape": srv.batch.params() if not lockstep else srv.batch.lockstep_params(),
+                   "batch_shape": srv.batch.params() if not lockstep else dict(srv.batch.lockstep_params(),
+                                                                               **srv.batch.lockstep_stats()),
                    "l2": "working set > 4 GB, larger than L2; no flush",
                    "parallelism": f"replicas x{world}", "setup_s": round(setup_s, 2)},
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": int(sum(b.nbytes for b in rhs)),
@@ -712,7 +713,7 @@ def c5_sweep(fb, torch, nreq=120, nsessions=16, seed=21, lambdas=LAMBDAS):
             if path == "plain":
                 st = serve.run_plain(lib, sessions, trace, tol=TOL, realtime=True)
             else:
-                srv = serve.Server(lib, sessions, mixed=True, engine="lockstep")
+                srv = serve.Server(lib, sessions, mixed=True, engine="continuous")
                 st = srv.run(trace, realtime=True)
                 del srv
             row[path] = {"solves_per_s": round(st["solves_per_s"], 3), "p50_ms": round(st["p50_ms"], 1),
@@ -748,8 +749,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-c5", action="store_true", help="skip the config-5 serving sweep leg of the c4s line")
     ap.add_argument("--c5-requests", type=int, default=120, help="requests per lambda of the config-5 sweep")
-    ap.add_argument("--engine", default="lockstep", choices=["lockstep", "persistent"],
-                    help="batched engine of the config-4 stream")
+    ap.add_argument("--engine", default="continuous", choices=["continuous", "lockstep", "persistent"],
+                    help="batched engine of the config-4 stream (continuous: the lockstep engine, resumable)")
     ap.add_argument("--workload", default="c4s", choices=["c4s", "c2", "c5"],
                     help="c4s: the served config-4 stream (default); c2: one P2 solve on 1024x1024; c5: the serving sweep")
     args = ap.parse_args()

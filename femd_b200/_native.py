@@ -111,6 +111,7 @@ SIGNATURES = {
     "femd_cuda_batch_solve_lockstep": (_I, [_P, _P, _P, _P, _I, _D, _I, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_lockstep_configure": (_I, [_P, _I, _I, _I, _I]),
     "femd_cuda_batch_step_lockstep": (_I, [_P, _P, _I, _PI, _PI, C.POINTER(femd_cg_result)]),
+    "femd_cuda_batch_advance_lockstep": (_I, [_P, _P, _I, _I, _PI, _PI, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_abort": (_I, [_P]),
     "femd_cuda_batch_lockstep_stats": (_I, [_P, C.POINTER(C.c_longlong)]),
     "femd_cuda_batch_info": (_I, [_P, _PI, _PI, _PI, _PI]),

@@ -176,9 +176,11 @@ class Batch:
 
     def step(self, iters: int, *, mixed=True, engine="persistent"):
         """Advance the armed members.  engine "persistent": one launch, every armed member by at
-        most iters iterations; "lockstep": every armed member to completion (iters unused).
-        Returns [(id, result dict)] of the members that finished."""
-        if engine not in ("persistent", "lockstep"):
+        most iters iterations; "lockstep": every armed member to completion (one wave; iters
+        unused); "continuous": the lockstep engine resumable -- members armed since the last step
+        join, every member in flight advances by about iters iterations (whole chunks), the ones
+        done leave.  Returns [(id, result dict)] of the members that finished."""
+        if engine not in ("persistent", "lockstep", "continuous"):
             raise ValueError(f"batch: unknown engine {engine!r}")
         n = max(len(self._armed), 1)
         ids = (C.c_int * n)()
@@ -187,6 +189,9 @@ class Batch:
         self.ctx.enter()
         if engine == "persistent":
             st = lib.femd_cuda_batch_step(self.ctx.h, self.h, int(iters), int(bool(mixed)), C.byref(nf), ids, res)
+        elif engine == "continuous":
+            chunks = max(1, int(iters) // max(1, self._ls_shape["chunk"]))
+            st = lib.femd_cuda_batch_advance_lockstep(self.ctx.h, self.h, int(bool(mixed)), chunks, C.byref(nf), ids, res)
         else:
             st = lib.femd_cuda_batch_step_lockstep(self.ctx.h, self.h, int(bool(mixed)), C.byref(nf), ids, res)
         self.ctx.leave()

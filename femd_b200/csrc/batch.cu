@@ -1351,6 +1351,9 @@ struct Member {
 
 }  // namespace
 
+struct LsLive;
+static void live_free(LsLive *L);
+
 struct femd_batch_s : femd::HandleBase {
     femd_ctx ctx = nullptr;
     std::vector<std::unique_ptr<Member>> mem;   // index = member id (null: free)
@@ -1384,6 +1387,10 @@ struct femd_batch_s : femd::HandleBase {
     bool ls_windows = false;                    // SpMV by windows (else by row groups)
     bool ls_compact = true;                     // mixed precision: the compact layout where it applies
     long long ls_stats[4] = {0, 0, 0, 0};       // last lockstep solve: compact members, plain members, widest window, entries
+    struct LiveDel {
+        void operator()(LsLive *L) const { live_free(L); }
+    };
+    std::unique_ptr<LsLive, LiveDel> live;      // the continuous lockstep engine's state (members in flight)
     int *abort_dev = nullptr;
     femd_batch_s() : HandleBase(femd::KIND_BATCH) {}
     void drop_graphs()
@@ -1977,6 +1984,85 @@ struct PinnedBuf {
 }  // namespace
 
 // One lockstep solve of the members `ids` (armed, one precision).  The final states go to out.
+// One member's part of a lockstep launch: its descriptor (FP32 compact, FP32 plain or FP64 layout)
+// and its table entries (r0, r1, w0, w1); maxwin grows to its widest shared-memory window.
+static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb &desc, std::vector<std::array<int, 4>> &E,
+                           bool &compact, int &maxwin)
+{
+    int st;
+    Member &M = *B->mem[id];
+    desc = describe(B, id, mx);
+    desc.tpr = ls_tpr(M);
+    desc.wrow = nullptr;
+    desc.iperm = desc.cptr = nullptr;
+    desc.coff = nullptr;
+    if (B->ls_windows && (st = ls_windows_of(B, M))) return st;
+    E.clear();
+    compact = false;
+    if (mx && B->ls_compact && !B->ls_windows) {
+        femd_pattern P = M.K->pattern;
+        if ((st = build_compact(ctx, P))) return st;
+        if (P->cl_state == 1) {
+            // rows per entry: a multiple of the tile near nnz_per_entry nonzeros, halved while
+            // some entry's column window is wider than the shared-memory window
+            int R = std::max(CL_TILE, ls_rows_per_entry(B, M) / CL_TILE * CL_TILE);
+            while (!compact) {
+                E.clear();
+                int wmax = 0;
+                for (int r = 0; r < M.n; r += R) {
+                    const int r1 = std::min(M.n, r + R);
+                    int lo = INT_MAX, hi = INT_MIN;
+                    for (int t = r / CL_TILE; t <= (r1 - 1) / CL_TILE; ++t) {
+                        lo = std::min(lo, P->cl_tile_lo[t]);
+                        hi = std::max(hi, P->cl_tile_hi[t]);
+                    }
+                    E.push_back({r, r1, lo, hi + 1});
+                    wmax = std::max(wmax, hi + 1 - lo);
+                }
+                if (wmax <= CL_WIN_MAX) {
+                    compact = true;
+                    maxwin = std::max(maxwin, wmax);
+                } else if (R > CL_TILE) {
+                    R = std::max(CL_TILE, R / 2 / CL_TILE * CL_TILE);
+                } else {
+                    break;
+                }
+            }
+            if (!compact) E.clear();
+        }
+    }
+    if (compact) {
+        femd_pattern P = M.K->pattern;
+        desc.iperm = P->cl_iperm.p;
+        desc.cptr = P->cl_indptr.p;
+        desc.coff = P->cl_off.p;
+    } else if (B->ls_windows && !M.ls_wrow.empty()) {
+        desc.wrow = M.ls_tab.p;
+        const int nw = (int)M.ls_wrow.size() - 1;
+        const int G = std::max(1, B->ls_nnz / LS_W);
+        for (int w = 0; w < nw; w += G) {
+            const int w1 = std::min(nw, w + G);
+            E.push_back({M.ls_wrow[w], M.ls_wrow[w1], w, w1});
+        }
+    } else {
+        const int R = ls_rows_per_entry(B, M);
+        for (int r = 0; r < M.n; r += R) E.push_back({r, std::min(M.n, r + R), 0, 0});
+    }
+    if (mx && (M.need_f32 || M.f32_compact != compact)) {
+        cudaStream_t s = ctx->stream;
+        const unsigned g = grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count);
+        if (compact)
+            k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, M.K->pattern->cl_dst.p, desc.A32, M.nnz, M.K->inv.p,
+                                                     M.K->pattern->cl_iperm.p, desc.inv32, M.n);
+        else
+            k_batch_f32<<<g, 256, 0, counted(s)>>>(M.K->data.p, desc.A32, M.nnz, M.K->inv.p, desc.inv32, M.n);
+        FEMD_TRY_CUDA(cudaGetLastError());
+        M.need_f32 = false;
+        M.f32_compact = compact;
+    }
+    return FEMD_OK;
+}
+
 static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bool mx, std::vector<LState> &out, double *seconds)
 {
     cudaStream_t s = ctx->stream;
@@ -1994,79 +2080,13 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     int maxwin = 0;                                     // the widest column window of a compact entry
     for (int k = 0; k < nm; ++k) {
         Member &M = *B->mem[ids[k]];
-        desc[k] = describe(B, ids[k], mx);
-        desc[k].tpr = ls_tpr(M);
-        desc[k].wrow = nullptr;
-        desc[k].iperm = desc[k].cptr = nullptr;
-        desc[k].coff = nullptr;
-        if (B->ls_windows && (st = ls_windows_of(B, M))) return st;
         auto &E = ents[k];
-        E.clear();
         bool compact = false;
-        if (mx && B->ls_compact && !B->ls_windows) {
-            femd_pattern P = M.K->pattern;
-            if ((st = build_compact(ctx, P))) return st;
-            if (P->cl_state == 1) {
-                // rows per entry: a multiple of the tile near nnz_per_entry nonzeros, halved while
-                // some entry's column window is wider than the shared-memory window
-                int R = std::max(CL_TILE, ls_rows_per_entry(B, M) / CL_TILE * CL_TILE);
-                while (!compact) {
-                    E.clear();
-                    int wmax = 0;
-                    for (int r = 0; r < M.n; r += R) {
-                        const int r1 = std::min(M.n, r + R);
-                        int lo = INT_MAX, hi = INT_MIN;
-                        for (int t = r / CL_TILE; t <= (r1 - 1) / CL_TILE; ++t) {
-                            lo = std::min(lo, P->cl_tile_lo[t]);
-                            hi = std::max(hi, P->cl_tile_hi[t]);
-                        }
-                        E.push_back({r, r1, lo, hi + 1});
-                        wmax = std::max(wmax, hi + 1 - lo);
-                    }
-                    if (wmax <= CL_WIN_MAX) {
-                        compact = true;
-                        maxwin = std::max(maxwin, wmax);
-                    } else if (R > CL_TILE) {
-                        R = std::max(CL_TILE, R / 2 / CL_TILE * CL_TILE);
-                    } else {
-                        break;
-                    }
-                }
-                if (!compact) E.clear();
-            }
-        }
-        if (compact) {
-            femd_pattern P = M.K->pattern;
-            desc[k].iperm = P->cl_iperm.p;
-            desc[k].cptr = P->cl_indptr.p;
-            desc[k].coff = P->cl_off.p;
-        } else if (B->ls_windows && !M.ls_wrow.empty()) {
-            desc[k].wrow = M.ls_tab.p;
-            const int nw = (int)M.ls_wrow.size() - 1;
-            const int G = std::max(1, B->ls_nnz / LS_W);
-            for (int w = 0; w < nw; w += G) {
-                const int w1 = std::min(nw, w + G);
-                E.push_back({M.ls_wrow[w], M.ls_wrow[w1], w, w1});
-            }
-        } else {
-            const int R = ls_rows_per_entry(B, M);
-            for (int r = 0; r < M.n; r += R) E.push_back({r, std::min(M.n, r + R), 0, 0});
-        }
+        if ((st = ls_member_setup(ctx, B, ids[k], mx, desc[k], E, compact, maxwin))) return st;
         nent[k] = (int)E.size();
         FEMD_CHECK_ARG((long long)NEfull + nent[k] < INT_MAX / 4, "batch: too many table entries");
         NEfull += nent[k];
         max_it = std::max(max_it, M.max_iter);
-        if (mx && (M.need_f32 || M.f32_compact != compact)) {
-            const unsigned g = grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count);
-            if (compact)
-                k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, M.K->pattern->cl_dst.p, desc[k].A32, M.nnz, M.K->inv.p,
-                                                         M.K->pattern->cl_iperm.p, desc[k].inv32, M.n);
-            else
-                k_batch_f32<<<g, 256, 0, counted(s)>>>(M.K->data.p, desc[k].A32, M.nnz, M.K->inv.p, desc[k].inv32, M.n);
-            FEMD_TRY_CUDA(cudaGetLastError());
-            M.need_f32 = false;
-            M.f32_compact = compact;
-        }
     }
     {
         long long nc = 0;
@@ -2254,6 +2274,259 @@ static int ls_solve(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, 
     return st2;
 }
 
+// ---- the lockstep engine, continuous ---------------------------------------------------------
+// The same kernels, resumable: every call admits the members armed since the last one (their
+// start kernels run first), runs a number of chunks of iterations over every member in flight, and
+// finishes and returns the members that are done; the others stay on the device for the next call.
+// Mixed-precision members run in one table and FP64 members (a mixed member whose FP32 recurrence
+// stagnated comes back as one at the next call) in another; each iteration launches the kernels of
+// both.  A member's iterates do not depend on when it joined or on the other members.
+struct LsLive {
+    std::vector<int> ids;                                  // members in flight, in admission order
+    std::vector<char> in, f64, started;                    // per member id
+    std::vector<std::vector<std::array<int, 4>>> ents;     // per member id: its entries
+    int maxwin = 0;
+    int cap = 0;
+    size_t tab_cap = 0;
+    DevBuf<BProb> d_desc;
+    DevBuf<LState> d_state;
+    DevBuf<LBlock> d_tab;
+    DevBuf<double> d_part;
+    DevBuf<int> d_int;                                     // active (unused), ru_count, ru_list (tab_cap)
+    void *pin = nullptr;                                   // pinned: states (cap), descriptor staging, table
+    size_t pin_b = 0;
+    ~LsLive()
+    {
+        if (pin) cudaFreeHost(pin);
+    }
+};
+
+static void live_free(LsLive *L) { delete L; }
+
+static int live_grow(femd_batch_s *B, LsLive &L, size_t ntab)
+{
+    cudaStream_t s = B->ctx->stream;
+    const int cap = B->cap;
+    if (L.cap < cap) {
+        DevBuf<BProb> nd;
+        DevBuf<LState> ns;
+        int st;
+        if ((st = nd.alloc(cap)) || (st = ns.alloc(cap))) return st;
+        FEMD_TRY_CUDA(cudaMemsetAsync(ns.p, 0, (size_t)cap * sizeof(LState), s));
+        if (L.cap) {
+            FEMD_TRY_CUDA(cudaMemcpyAsync(nd.p, L.d_desc.p, (size_t)L.cap * sizeof(BProb), cudaMemcpyDeviceToDevice, s));
+            FEMD_TRY_CUDA(cudaMemcpyAsync(ns.p, L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToDevice, s));
+        }
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+        std::swap(L.d_desc.p, nd.p);
+        std::swap(L.d_desc.n, nd.n);
+        std::swap(L.d_state.p, ns.p);
+        std::swap(L.d_state.n, ns.n);
+        L.in.resize(cap, 0);
+        L.f64.resize(cap, 0);
+        L.started.resize(cap, 0);
+        L.ents.resize(cap);
+        L.cap = cap;
+    }
+    if (ntab > L.tab_cap) {
+        const size_t nc = std::max(ntab, 2 * L.tab_cap);
+        int st;
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+        if ((st = L.d_tab.alloc(nc)) || (st = L.d_part.alloc(3 * nc + 3)) || (st = L.d_int.alloc(nc + 2))) return st;
+        L.tab_cap = nc;
+    }
+    const size_t need = (size_t)cap * sizeof(LState) + sizeof(BProb) + L.tab_cap * sizeof(LBlock) + 64;
+    if (need > L.pin_b) {
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+        if (L.pin) cudaFreeHost(L.pin);
+        L.pin = nullptr;
+        L.pin_b = 0;
+        FEMD_TRY_CUDA(cudaHostAlloc(&L.pin, 2 * need, cudaHostAllocDefault));
+        L.pin_b = 2 * need;
+    }
+    return FEMD_OK;
+}
+
+// the table of the members `sel` (each member's entries together, its b0 / b1 within the table)
+static int live_table(const LsLive &L, const std::vector<int> &sel, LBlock *T)
+{
+    int e = 0;
+    for (int id : sel) {
+        const int b0 = e, b1 = b0 + (int)L.ents[id].size();
+        for (const auto &x : L.ents[id]) T[e++] = LBlock{id, x[0], x[1], b0, b1, x[2], x[3]};
+    }
+    return e;
+}
+
+static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *nfin, int *fin_ids, femd_cg_result *fin_res)
+{
+    cudaStream_t s = ctx->stream;
+    if (!B->live) B->live.reset(new LsLive());
+    LsLive &L = *B->live;
+    int st;
+    *nfin = 0;
+    // members armed since the last call join (a stagnated mixed member comes back in FP64)
+    std::vector<int> fresh;
+    size_t ntab = 0;
+    if ((st = live_grow(B, L, 1))) return st;
+    for (int id = 0; id < (int)B->mem.size(); ++id)
+        if (B->mem[id] && B->mem[id]->armed && !L.in[id]) fresh.push_back(id);
+    for (int id : L.ids) ntab += L.ents[id].size();
+    for (int id : fresh) {
+        Member &M = *B->mem[id];
+        const bool m32 = mx && !M.force_fp64;
+        if ((st = member_vectors(B, M, m32))) return st;
+        BProb d{};
+        bool compact = false;
+        if ((st = ls_member_setup(ctx, B, id, m32, d, L.ents[id], compact, L.maxwin))) return st;
+        BProb *h = reinterpret_cast<BProb *>(L.pin);
+        *h = d;
+        FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_desc.p + id, h, sizeof(BProb), cudaMemcpyHostToDevice, s));
+        FEMD_TRY_CUDA(cudaMemsetAsync(L.d_state.p + id, 0, sizeof(LState), s));
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));           // the staging slot is reused
+        L.in[id] = 1;
+        L.f64[id] = !m32;
+        L.started[id] = 0;
+        L.ids.push_back(id);
+        ntab += L.ents[id].size();
+    }
+    if (L.ids.empty()) return FEMD_OK;
+    FEMD_CHECK_ARG(ntab < (size_t)INT_MAX / 4, "batch: too many table entries");
+    if ((st = live_grow(B, L, ntab + 1))) return st;
+    LState *hs = reinterpret_cast<LState *>(static_cast<char *>(L.pin) + sizeof(BProb) + 64);
+    LBlock *ht = reinterpret_cast<LBlock *>(hs + L.cap);
+    int *active = L.d_int.p, *ru_count = L.d_int.p + 1, *ru_list = L.d_int.p + 2;
+    const int G1 = std::max(1, 8 * ctx->sm_count);
+    const size_t win_b = (size_t)L.maxwin * sizeof(float);
+    FEMD_TRY_CUDA(cudaFuncSetAttribute(k_ls_spmv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(CL_WIN_MAX * sizeof(float))));
+    FEMD_TRY_CUDA(cudaMemsetAsync(L.d_int.p, 0, 2 * sizeof(int), s));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    FEMD_TRY_CUDA(cudaEventCreate(&t0));
+    FEMD_TRY_CUDA(cudaEventCreate(&t1));
+    struct EvG {
+        cudaEvent_t a, b;
+        ~EvG() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
+    } evg{t0, t1};
+    FEMD_TRY_CUDA(cudaEventRecord(t0, s));
+    {
+        // the layout of the members in flight (femd_cuda_batch_lockstep_stats)
+        long long nc = 0;
+        size_t ne = 0;
+        for (int id : L.ids) {
+            nc += B->mem[id]->f32_compact && !L.f64[id];
+            ne += L.ents[id].size();
+        }
+        B->ls_stats[0] = nc;
+        B->ls_stats[1] = (long long)L.ids.size() - nc;
+        B->ls_stats[2] = L.maxwin;
+        B->ls_stats[3] = (long long)ne;
+    }
+    // the start of the new members (r = b - A x, ||b||, z, the first direction's state)
+    {
+        std::vector<int> n32, n64;
+        for (int id : L.ids)
+            if (!L.started[id]) (L.f64[id] ? n64 : n32).push_back(id);
+        const int NE32 = live_table(L, n32, ht), NE64 = live_table(L, n64, ht + NE32);
+        if (NE32 + NE64) {
+            FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_tab.p, ht, (size_t)(NE32 + NE64) * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+            if (NE32)
+                k_ls_resid<true, 0><<<NE32, LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p, NE32, L.d_state.p, L.d_part.p, active,
+                                                                     ru_list, ru_count);
+            if (NE64)
+                k_ls_resid<false, 0><<<NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p + NE32, NE64, L.d_state.p, L.d_part.p,
+                                                                      active, ru_list, ru_count);
+            FEMD_TRY_CUDA(cudaGetLastError());
+            FEMD_TRY_CUDA(cudaStreamSynchronize(s));       // the host table is rewritten below
+        }
+        for (int id : L.ids) L.started[id] = 1;
+    }
+    // chunks of iterations over the members in flight; the states are read after each chunk
+    const int C = std::max(1, B->ls_chunk);
+    FEMD_TRY_CUDA(cudaMemcpyAsync(hs, L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    for (int j = 0; j < std::max(1, chunks); ++j) {
+        std::vector<int> l32, l64;
+        for (int id : L.ids)
+            if (!hs[id].done) (L.f64[id] ? l64 : l32).push_back(id);
+        if (l32.empty() && l64.empty()) break;
+        const int NE32 = live_table(L, l32, ht), NE64 = live_table(L, l64, ht + NE32);
+        FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_tab.p, ht, (size_t)(NE32 + NE64) * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+        const LBlock *T32 = L.d_tab.p, *T64 = L.d_tab.p + NE32;
+        for (int c = 0; c < C; ++c) {
+            if (NE32) {
+                k_ls_spmv<true><<<NE32, LS_BB, win_b, counted(s)>>>(L.d_desc.p, T32, NE32, L.d_state.p, L.d_part.p, active,
+                                                                   ru_count);
+                k_ls_update<true><<<NE32, LS_BB, 0, counted(s)>>>(L.d_desc.p, T32, NE32, L.d_state.p, L.d_part.p, active, ru_list,
+                                                                 ru_count);
+                k_ls_flush<false><<<std::min(G1, NE32), LS_BB, 0, counted(s)>>>(L.d_desc.p, T32, NE32, L.d_state.p, ru_list,
+                                                                                ru_count);
+                k_ls_resid<true, 1><<<std::min(G1, NE32), LS_BB, 0, counted(s)>>>(L.d_desc.p, T32, NE32, L.d_state.p, L.d_part.p,
+                                                                                  active, ru_list, ru_count);
+            }
+            if (NE64) {
+                k_ls_spmv<false><<<NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, T64, NE64, L.d_state.p, L.d_part.p, active, ru_count);
+                k_ls_update<false><<<NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, T64, NE64, L.d_state.p, L.d_part.p, active, ru_list,
+                                                                  ru_count);
+            }
+        }
+        FEMD_TRY_CUDA(cudaGetLastError());
+        FEMD_TRY_CUDA(cudaMemcpyAsync(hs, L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
+        FEMD_TRY_CUDA(cudaStreamSynchronize(s));           // the host table is rewritten next chunk
+        if (*(volatile int *)B->abort_host) break;
+    }
+    // the members that are done: the end of their solve (the final true residual in FP64, the
+    // flush of a mixed member that broke down, x = 0 for b = 0), then their results
+    std::vector<int> d32, d64, back, keep;
+    for (int id : L.ids) {
+        const LState &S = hs[id];
+        if (!S.done) { keep.push_back(id); continue; }
+        Member &M = *B->mem[id];
+        if (!L.f64[id] && S.fallback) {
+            // the FP32 recurrence stagnated: FP64 from this iterate at the next call
+            M.force_fp64 = true;
+            M.prior_its += S.it;
+            M.prior_rus += S.rus;
+            M.max_iter = std::max(1, M.max_iter - S.it);
+            back.push_back(id);
+            continue;
+        }
+        (L.f64[id] ? d64 : d32).push_back(id);
+    }
+    const int NE32 = live_table(L, d32, ht), NE64 = live_table(L, d64, ht + NE32);
+    if (NE32 + NE64) {
+        FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_tab.p, ht, (size_t)(NE32 + NE64) * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+        if (NE32)
+            k_ls_flush<true><<<std::min(G1, NE32), LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p, NE32, L.d_state.p, ru_list,
+                                                                           ru_count);
+        if (NE64)
+            k_ls_resid<false, 2><<<NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p + NE32, NE64, L.d_state.p, L.d_part.p,
+                                                                  active, ru_list, ru_count);
+        k_ls_zero<<<NE32 + NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p, L.d_state.p);
+        FEMD_TRY_CUDA(cudaGetLastError());
+        FEMD_TRY_CUDA(cudaMemcpyAsync(hs, L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
+    }
+    FEMD_TRY_CUDA(cudaEventRecord(t1, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    int nf = 0;
+    for (const auto *set : {&d32, &d64})
+        for (int id : *set) {
+            Member &M = *B->mem[id];
+            if (fin_res) ls_result(M, hs[id], fin_res[nf], ms * 1e-3);
+            if (fin_ids) fin_ids[nf] = id;
+            ++nf;
+            M.armed = false;
+            L.in[id] = 0;
+        }
+    for (int id : back) L.in[id] = 0;                       // re-admitted (FP64) at the next call
+    L.ids = keep;
+    *nfin = nf;
+    if (*(volatile int *)B->abort_host) { set_error("batch: aborted by the host"); return FEMD_EABORT; }
+    return FEMD_OK;
+}
+
 extern "C" {
 
 int femd_cuda_batch_create(femd_ctx ctx, int nprob, const femd_matrix *mats, int nnz_per_block, femd_batch *out)
@@ -2296,6 +2569,13 @@ int femd_cuda_batch_remove(femd_batch handle, int id)
     clear_error();
     femd_batch_s *B = as_batch(handle);
     FEMD_CHECK_ARG(B && id >= 0 && id < (int)B->mem.size() && B->mem[id], "batch_remove: no such member");
+    if (B->live && id < (int)B->live->in.size() && B->live->in[id]) {
+        // a member in flight in the continuous lockstep engine leaves it (its solve is dropped)
+        FEMD_TRY_CUDA(cudaStreamSynchronize(B->ctx->stream));
+        auto &ids = B->live->ids;
+        ids.erase(std::remove(ids.begin(), ids.end(), id), ids.end());
+        B->live->in[id] = 0;
+    }
     B->free_vectors(*B->mem[id]);
     B->mem[id].reset();
     return FEMD_OK;
@@ -2340,6 +2620,20 @@ int femd_cuda_batch_step_lockstep(femd_ctx ctx, femd_batch handle, int mixed, in
         if (finished) finished[p] = res[p];
     }
     if (nfinished) *nfinished = (int)ids.size();
+    return st;
+}
+
+int femd_cuda_batch_advance_lockstep(femd_ctx ctx, femd_batch handle, int mixed, int chunks, int *nfinished,
+                                     int *finished_ids, femd_cg_result *finished)
+{
+    clear_error();
+    femd_batch_s *B = as_batch(handle);
+    FEMD_CHECK_ARG(ctx && B && ctx == B->ctx && chunks >= 1, "batch_advance_lockstep: bad arguments");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    *(volatile int *)B->abort_host = 0;
+    int nf = 0;
+    const int st = ls_advance(ctx, B, mixed != 0, chunks, &nf, finished_ids, finished);
+    if (nfinished) *nfinished = nf;
     return st;
 }
 

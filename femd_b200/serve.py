@@ -57,10 +57,11 @@ class SpaceLibrary:
         return s
 
 
-def stiffness(lib, N, k, c=1.0):
-    """c (grad u, grad v) on the library's (N, k) space, with its Jacobi inverse diagonal."""
+def stiffness(lib, N, k, c=1.0, into=None):
+    """c (grad u, grad v) on the library's (N, k) space, with its Jacobi inverse diagonal (into: a
+    CSRMatrix on that space's pattern to overwrite instead of a new one)."""
     s = lib.get(N, k)
-    K = fb.CSRMatrix(s["P"], symmetric=True)
+    K = into if into is not None else fb.CSRMatrix(s["P"], symmetric=True)
     fb.assemble_matrix_2d(s["Qk"], s["Qk"], [1, 2], [1, 2], [c, c], K)
     return K
 
@@ -183,15 +184,17 @@ class Server:
     hold.  big_nnz: requests whose matrix has at least that many nonzeros are solved one at a time
     on the whole GPU (femd_b200.cg_solve, the same precision) between batch launches -- a large
     system streams HBM better with every block on it than as one team among many.  engine:
-    "persistent" (members join and leave between launches of at most iters iterations) or
-    "lockstep" (the admitted requests are solved together to completion, one wave at a time;
-    requests that arrive meanwhile wait for the next wave)."""
+    "continuous" (the lockstep engine, resumable: requests join at the next chunk boundary
+    after they are admitted, every request in flight advances by about iters iterations per
+    step, finished ones leave), "persistent" (members join and leave between cooperative launches
+    of at most iters iterations) or "lockstep" (the admitted requests are solved together to
+    completion, one wave at a time; requests that arrive meanwhile wait for the next wave)."""
 
     def __init__(self, lib, sessions=(), *, mixed=True, iters=64, tol=1e-10, reserve_bytes=2 << 30, free_memory=None,
                  hbm_budget=None, max_members=1024, keep_solutions=False, shape=None, big_nnz=None,
-                 engine="persistent"):
+                 engine="continuous"):
         torch = _torch()
-        if engine not in ("persistent", "lockstep"):
+        if engine not in ("persistent", "lockstep", "continuous"):
             raise ValueError(f"serve: unknown engine {engine!r}")
         self.engine = engine
         self.lib, self.sessions = lib, list(sessions)
@@ -211,6 +214,9 @@ class Server:
         self.active = {}
         self.direct = collections.deque()           # admitted requests for the whole-GPU path
         self.last_launch_s = 0.0
+        # finished Poisson requests leave their matrix and batch member here, per (N, k), for the
+        # next request on that space: in steady state a request allocates nothing
+        self._pool = collections.defaultdict(list)
 
     def _big(self, nnz):
         return self.big_nnz is not None and nnz >= self.big_nnz
@@ -234,13 +240,16 @@ class Server:
                 self.batch.arm(S.member, b, x, tol=self.tol)
                 self.active[S.member] = (r, S, None, b, x, need)
         else:
-            K = stiffness(self.lib, r.N, r.k, r.c)
+            pool = self._pool[(r.N, r.k)]
+            K, mid = pool.pop() if pool else (None, None)
+            K = stiffness(self.lib, r.N, r.k, r.c, into=K)
             b = _rhs(r, K.nrows)
             x = torch.zeros(K.nrows, dtype=torch.float64, device=b.device)
             if self._big(K.nnz):
                 self.direct.append((r, None, K, b, x, need))
             else:
-                mid = self.batch.add(K)
+                if mid is None:
+                    mid = self.batch.add(K)
                 self.batch.arm(mid, b, x, tol=self.tol)
                 self.active[mid] = (r, None, K, b, x, need)
         return need
@@ -312,7 +321,7 @@ class Server:
                     self.last_launch_s = res["seconds"]
                     self._finish(r, S, x, res, t_done)
                     if S is None:
-                        self.batch.remove(mid)
+                        self._pool[(r.N, r.k)].append((K, mid))
                 if self.batch.last_status != 0:
                     raise RuntimeError(f"serve: batch launch failed with status {self.batch.last_status}")
             if self.direct:

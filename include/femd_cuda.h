@@ -402,6 +402,16 @@ FEMD_API int femd_cuda_batch_solve_lockstep(femd_ctx ctx, femd_batch B, const do
  * femd_cuda_batch_step's finished members.  No reference counterpart. */
 FEMD_API int femd_cuda_batch_step_lockstep(femd_ctx ctx, femd_batch B, int mixed, int *nfinished, int *finished_ids,
                                            femd_cg_result *finished);
+/* The lockstep engine, continuous: admits every member armed since the last call (members armed
+ * while others are in flight join here, at a chunk boundary), runs up to `chunks` chunks of
+ * iterations (the configured chunk length each) over every member in flight, finishes the members
+ * that are done (the final FP64 residual, or the flush of a mixed member that broke down) and lists
+ * them like femd_cuda_batch_step (disarmed); the others stay on the device for the next call.  A mixed
+ * member whose FP32 recurrence stagnates goes on in FP64 from the next call (its result counts both
+ * phases).  A member's iterates do not depend on when it joined or on the other members.  No
+ * reference counterpart (continuous batching of cg_jacobi, cg.hpp:296-350). */
+FEMD_API int femd_cuda_batch_advance_lockstep(femd_ctx ctx, femd_batch B, int mixed, int chunks, int *nfinished,
+                                              int *finished_ids, femd_cg_result *finished);
 /* Shape of the lockstep engine: nonzeros per row range of a member (one thread block each;
  * default 16384), iterations enqueued between two reads of the members' states (default 8), the
  * SpMV by windows of whole rows read by coalesced loads (windows = 1) or by row groups of a few

@@ -40,7 +40,7 @@ def exact13(t):
                          + np.exp(-13 * np.pi ** 2 * t) * np.sin(3 * np.pi * x) * np.sin(2 * np.pi * y))
 
 
-@pytest.mark.parametrize("path", ["served_mixed", "served_fp64", "served_lockstep", "plain"])
+@pytest.mark.parametrize("path", ["served_mixed", "served_fp64", "served_lockstep", "served_continuous", "plain"])
 def test_example13_heat_loop_pin(sv, lib, path):
     """100 backward-Euler steps to t = 0.1: the reference prints L2 error 1.35e-03."""
     from femd_b200.workloads import l2_error
@@ -50,14 +50,14 @@ def test_example13_heat_loop_pin(sv, lib, path):
         st = sv.run_plain(lib, [S], trace, tol=1e-12, realtime=False)
     else:
         srv = sv.Server(lib, [S], mixed=(path != "served_fp64"), iters=16, tol=1e-12,
-                        engine="lockstep" if path == "served_lockstep" else "persistent")
+                        engine={"served_lockstep": "lockstep", "served_continuous": "continuous"}.get(path, "persistent"))
         st = srv.run(trace, realtime=False)
     assert st["completed"] == 100 and st["all_converged"]
     err = l2_error(lib.get(20, 2)["V"], S.u, exact13(0.1))
     assert f"{err:.2e}" == "1.35e-03", err
 
 
-@pytest.mark.parametrize("engine", ["persistent", "lockstep"])
+@pytest.mark.parametrize("engine", ["persistent", "lockstep", "continuous"])
 def test_served_results_alone_and_in_the_mix(sv, lib, engine):
     sessions = sv.make_sessions(lib, 5, 3, sizes=SMALL)
     trace = sv.make_trace(11, 1e6, 24, len(sessions), sizes=SMALL)
@@ -79,7 +79,7 @@ def test_served_results_alone_and_in_the_mix(sv, lib, engine):
             sessions[r.session].reset()
 
 
-@pytest.mark.parametrize("engine", ["persistent", "lockstep"])
+@pytest.mark.parametrize("engine", ["persistent", "lockstep", "continuous"])
 def test_served_matches_plain_fp64(sv, lib, engine):
     sessions = sv.make_sessions(lib, 6, 2, sizes=SMALL)
     trace = sv.make_trace(12, 1e6, 16, len(sessions), sizes=SMALL)
@@ -125,3 +125,31 @@ def test_no_admission_below_the_reserve(sv, lib):
     srv = sv.Server(lib, [], mixed=True, iters=8, reserve_bytes=1 << 30, free_memory=lambda: 1 << 20)
     st = srv.run(trace, realtime=False, max_seconds=0.5)
     assert st["completed"] == 0 and srv.launches == 0
+
+
+def test_continuous_admits_mid_flight(sv, lib):
+    """Continuous batching: a small request armed while a large one is in flight joins at the next
+    chunk boundary, finishes first, and has the same bits as when it is solved alone; the large
+    one too."""
+    import torch
+    from femd_b200.batch import Batch
+    big = sv.stiffness(lib, 64, 3, 1.3)
+    small = sv.stiffness(lib, 16, 1, 0.7)
+    bb = torch.as_tensor(np.random.default_rng(1).standard_normal(big.nrows)).cuda()
+    bs = torch.as_tensor(np.random.default_rng(2).standard_normal(small.nrows)).cuda()
+    B = Batch()
+    ib, is_ = B.add(big), B.add(small)
+    xb = torch.zeros(big.nrows, dtype=torch.float64, device="cuda")
+    xs = torch.zeros(small.nrows, dtype=torch.float64, device="cuda")
+    B.arm(ib, bb, xb)
+    fin = B.step(16, mixed=True, engine="continuous")          # the big one alone, 16 iterations
+    assert fin == []
+    B.arm(is_, bs, xs)                                          # arrives mid-flight
+    order = []
+    while len(order) < 2:
+        order += [i for i, r in B.step(16, mixed=True, engine="continuous")]
+    assert order == [is_, ib]
+    for K, b, x in ((small, bs, xs), (big, bb, xb)):
+        xa, ra = Batch([K]).solve([b], mixed=True, engine="lockstep")
+        assert ra[0]["converged"]
+        assert np.array_equal(xa[0].cpu().numpy(), x.cpu().numpy())
