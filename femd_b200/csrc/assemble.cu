@@ -22,6 +22,7 @@
 //          coefficients are contracted point by point.
 // Coefficients given as closed forms or as a field are first evaluated at the points into a
 // scratch array [e nq + q] (the reference's coefficient arrays, assembler_2d.hpp:393-410).
+#include <climits>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -593,7 +594,137 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows_off(
     }
 }
 
-// The pair offsets: for rc index c (row i, cell entry code = cell nloc + l), byte j of
+// ---- K3e: one thread per nonzero over the inverted scatter map --------------------------------
+// Every matrix position p has the list of its element entries (cell nloc^2 + l nloc + j) in
+// increasing cell order (cptr / cent, built once per pattern by k_contrib_*).  A thread owns a
+// position: it forms each entry from the cell's factors and the reference tensors in shared memory
+// (the same contraction as K3d: sum over the active pairs k of F_k S^k(l, j), then the point terms)
+// and adds them in cell order in a register, then writes the value once -- consecutive threads
+// write consecutive positions.  No accumulator in shared memory and no atomics; the value is the
+// sum of its element contributions in increasing element order, as in the reference.
+template <int NLOC, int NPAIR>
+__global__ void __launch_bounds__(256) k_assemble_nnz(const int *__restrict__ cptr, const int *__restrict__ cent,
+                                                      long long nnz, int nq, const double *__restrict__ factors,
+                                                      const double *__restrict__ g_S, const double *__restrict__ g_R,
+                                                      FastSpec fs, double *__restrict__ data)
+{
+    extern __shared__ double smem[];
+    constexpr int NL2 = NLOC * NLOC;
+    double *sS = smem;
+    double *sR = sS + (fs.has_const ? NPAIR * NL2 : 0);
+    if (fs.has_const)
+        for (int t = threadIdx.x; t < NPAIR * NL2; t += blockDim.x) sS[t] = g_S[t];
+    if (fs.has_var)
+        for (int t = threadIdx.x; t < nq * 3 * NLOC; t += blockDim.x) sR[t] = g_R[t];
+    __syncthreads();
+    const int cst = fs.has_const ? NPAIR : 0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x) {
+        const int c0 = __ldcs(&cptr[p]), c1 = __ldcs(&cptr[p + 1]);
+        double acc = 0.0;
+        for (int c = c0; c < c1; ++c) {
+            const int code = __ldcs(&cent[c]);
+            const int e = code / NL2, lj = code - e * NL2, l = lj / NLOC, j = lj - l * NLOC;
+            const double *F = factors + (size_t)e * fs.nf;
+            double v = 0.0;
+            if (fs.has_const) {
+#pragma unroll
+                for (int k = 0; k < NPAIR; ++k) v += __ldg(&F[k]) * sS[k * NL2 + l * NLOC + j];
+            }
+            if (fs.has_var) {
+                const double *H = F + cst;
+                for (int q = 0; q < nq; ++q) {
+                    const double *R = sR + q * 3 * NLOC;
+#pragma unroll
+                    for (int k = 0; k < NPAIR; ++k) v += (__ldg(&H[q * NPAIR + k]) * R[fs.pr[k] * NLOC + l]) * R[fs.ps[k] * NLOC + j];
+                }
+            }
+            acc += v;
+        }
+        data[p] = acc;
+    }
+}
+
+// the inverse diagonal from the assembled values (JacobiPreconditioner, precond.hpp:82-102)
+__global__ void k_asm_inv(const int *__restrict__ diag_pos, const double *__restrict__ data, double *__restrict__ inv, int n,
+                          int *__restrict__ status)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int d = diag_pos[i];
+        const double a = d >= 0 ? data[d] : 0.0;
+        if (d < 0 || a == 0.0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
+        inv[i] = 1.0 / a;
+    }
+}
+
+// the inverted scatter map, pass 1: per position the number of element entries (one thread per
+// row walks its (cell, local) pairs and their row offsets; a row's positions are its own)
+__global__ void k_contrib_count(const int *__restrict__ rc_ptr, const int *__restrict__ indptr,
+                                const unsigned char *__restrict__ off, int nrows, int nloc, int offs, int *__restrict__ cnt)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x) {
+        const int rlo = indptr[i];
+        for (int c = rc_ptr[i]; c < rc_ptr[i + 1]; ++c)
+            for (int j = 0; j < nloc; ++j) {
+                const unsigned o = off[(size_t)c * offs + j];
+                if (o != 0xffu) cnt[rlo + o] += 1;
+            }
+    }
+}
+
+// pass 2: the entries, in the row's cell order (so each position's list is in increasing cell
+// order); cur starts as the exclusive prefix of the counts
+__global__ void k_contrib_fill(const int *__restrict__ rc_ptr, const int *__restrict__ rc_code,
+                               const int *__restrict__ indptr, const unsigned char *__restrict__ off, int nrows, int nloc,
+                               int offs, int *__restrict__ cur, int *__restrict__ cent)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x) {
+        const int rlo = indptr[i];
+        for (int c = rc_ptr[i]; c < rc_ptr[i + 1]; ++c) {
+            const int code = rc_code[c];
+            for (int j = 0; j < nloc; ++j) {
+                const unsigned o = off[(size_t)c * offs + j];
+                if (o != 0xffu) cent[cur[rlo + o]++] = code * nloc + j;
+            }
+        }
+    }
+}
+
+static int build_pair_offsets(femd_ctx ctx, femd_pattern p);
+
+// the inverted scatter map of a pattern (once): contrib_ptr (nnz + 1), contrib (every element entry)
+static int build_contrib(femd_ctx ctx, femd_pattern p)
+{
+    if (p->contrib_ptr.p) return FEMD_OK;
+    cudaStream_t s = ctx->stream;
+    FEMD_CHECK_ARG(p->max_row_len < 255, "assembly: a row is too long for the byte offsets of the inverted scatter map");
+    FEMD_TRY(build_pair_offsets(ctx, p));
+    const int offs = (p->nloc + 3) / 4 * 4, n = p->nrows;
+    const long long nnz = p->nnz;
+    FEMD_CHECK_ARG(nnz < INT_MAX && (long long)p->ncells * p->nloc * p->nloc < INT_MAX,
+                   "assembly: the pattern is too large for the inverted scatter map");
+    DevBuf<int> cnt, tmp;
+    FEMD_TRY(cnt.alloc((size_t)nnz + 1));
+    FEMD_TRY(tmp.alloc(scan_tmp_ints((size_t)nnz + 1)));
+    FEMD_TRY(p->contrib_ptr.alloc((size_t)nnz + 1));
+    FEMD_TRY_CUDA(cudaMemsetAsync(cnt.p, 0, ((size_t)nnz + 1) * sizeof(int), s));
+    const unsigned g = grid_for((size_t)n, 256, 1u << 20);
+    k_contrib_count<<<g, 256, 0, counted(s)>>>(p->rc_ptr.p, p->indptr.p, p->pair_off.p, n, p->nloc, offs, cnt.p);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY(exclusive_scan_int(cnt.p, p->contrib_ptr.p, (size_t)nnz + 1, tmp.p, s));
+    int total = 0;
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&total, p->contrib_ptr.p + nnz, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    int st = p->contrib.alloc((size_t)std::max(total, 1));
+    if (st) { p->contrib_ptr.release(); return st; }
+    FEMD_TRY_CUDA(cudaMemcpyAsync(cnt.p, p->contrib_ptr.p, ((size_t)nnz + 1) * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    k_contrib_fill<<<g, 256, 0, counted(s)>>>(p->rc_ptr.p, p->rc_code.p, p->indptr.p, p->pair_off.p, n, p->nloc, offs, cnt.p,
+                                               p->contrib.p);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // cnt and tmp are released on return
+    return FEMD_OK;
+}
+
+// The pair offsets: for rc index c (row i, cell entry code = cell nloc + l), byte j of// The pair offsets: for rc index c (row i, cell entry code = cell nloc + l), byte j of
 // off[c * OFFS + j] = position of (i, dof(cell, j)) minus indptr[i], 255 where constrained.
 // OFFS = nloc rounded up to a multiple of 4, so a pair's offsets load as whole 32-bit words.
 __global__ void k_pair_offsets(const int *__restrict__ rc_ptr, const int *__restrict__ rc_code,
@@ -880,6 +1011,29 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
         const size_t sho = ((fs.has_const ? (size_t)fs.npair * nl2 : 0) + (fs.has_var ? nref : 0) +
                             (size_t)maxlen * FAST_BLOCK) * sizeof(double) +
                            (FAST_BLOCK / 32) * 33 * sizeof(int) + (size_t)FAST_BLOCK * maxlen;
+#define FEMD_NNZ(NL, NP)                                                                                               \
+        if (!done && nl == NL && fs.npair == NP && p->nnz > 0 && B_NNZ) {                                             \
+            const size_t shn = ((fs.has_const ? (size_t)NP * NL * NL : 0) + (fs.has_var ? nref : 0)) * sizeof(double); \
+            cudaFuncSetAttribute(k_assemble_nnz<NL, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shn);       \
+            k_assemble_nnz<NL, NP><<<grid_for((size_t)p->nnz, 256, (unsigned)ctx->sm_count * 64), 256, shn, counted(s)>>>( \
+                p->contrib_ptr.p, p->contrib.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs, K->data.p);                \
+            if (inv) k_asm_inv<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(p->diag_pos.p, K->data.p,   \
+                                                                                            inv, n, ctx->status_dev);  \
+            done = true;                                                                                               \
+        }
+        // the nonzero-parallel kernel where the inverted scatter map can be built
+        const bool B_NNZ = p->contrib_ptr.p || build_contrib(ctx, p) == FEMD_OK;
+        if (!B_NNZ) {
+            // no room (or a row too long): the row kernels below
+            p->contrib_ptr.release();
+            p->contrib.release();
+            cudaGetLastError();
+            clear_error();
+        }
+        FEMD_NNZ(3, 1) FEMD_NNZ(3, 3) FEMD_NNZ(3, 4) FEMD_NNZ(3, 5)
+        FEMD_NNZ(6, 1) FEMD_NNZ(6, 3) FEMD_NNZ(6, 4) FEMD_NNZ(6, 5)
+        FEMD_NNZ(10, 1) FEMD_NNZ(10, 3) FEMD_NNZ(10, 4) FEMD_NNZ(10, 5)
+#undef FEMD_NNZ
 #define FEMD_ROWS_OFF(NL, NP)                                                                                          \
         if (!done && nl == NL && fs.npair == NP && maxlen < 255) {                                                     \
             FEMD_TRY(build_pair_offsets(ctx, p));                                                                      \
