@@ -529,12 +529,12 @@ def _traffic(name, alg):
 
 
 # ---- config 4: the served stream ---------------------------------------------------------------
-def batch_bytes(reqs, lib, mixed=True):
+def batch_bytes(reqs, lib, mixed=True, compact=False):
     """Algorithmic HBM bytes of the batched solve that served these requests
     (femd_b200.workloads.batch_bytes)."""
     from femd_b200.workloads import batch_bytes as bb
     sizes = [(lib.get(r.N, r.k)["n"], lib.get(r.N, r.k)["nnz"]) for r in reqs]
-    return bb(sizes, [dict(iterations=r.iterations, reliable_updates=r.outer) for r in reqs], mixed)
+    return bb(sizes, [dict(iterations=r.iterations, reliable_updates=r.outer) for r in reqs], mixed, compact)
 
 
 def checker(spec, rhs, served, plain):
@@ -643,7 +643,9 @@ def ours_c4(args, rank, world, dist):
     xs_served.clear()
     chk = checker(spec, rhs, keep_s, keep_p) if rank == 0 else None
     # ---- roofline of the batched solve of the last timed step
-    alg = batch_bytes(last, lib, mixed=True)
+    lst = srv.batch.lockstep_stats() if args.engine != "persistent" else {"compact": 0, "plain": 1}
+    all_compact = lst["compact"] > 0 and lst["plain"] == 0
+    alg = batch_bytes(last, lib, mixed=True, compact=all_compact)
     t_launch = launch_s[-1]
     achieved = alg / t_launch / 1e9
     lockstep = args.engine in ("lockstep", "continuous")

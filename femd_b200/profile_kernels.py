@@ -5,6 +5,7 @@
     python -m femd_b200.profile_kernels cg --n 640 --k 2
     python -m femd_b200.profile_kernels batch --nmin 150 --nmax 256 --nprob 24 --iters 100 --mixed
     python -m femd_b200.profile_kernels lockstep --nmin 0 --kmin 1 --nprob 16 --iters 0 --reps 1
+    python -m femd_b200.profile_kernels lockstep --nmin 0 --kmin 1 --nprob 16 --iters 120 --reps 1 --mixed
 
 Workload: -Lap u + u = f on rectangle_mesh(0, 0, 1, 1, n, n), P_k, zero Dirichlet (the form of
 the config-2 benchmark at another size).  Prints the sizes and a CUDA-event time per launch.
@@ -24,7 +25,8 @@ PI = math.pi
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("kernel", choices=["spmv", "assemble", "rhs", "cg", "cg_mixed", "pattern", "batch", "lockstep"])
+    ap.add_argument("kernel", choices=["spmv", "assemble", "assemble_values", "rhs", "cg", "cg_mixed", "pattern", "batch",
+                                       "lockstep"])
     ap.add_argument("--n", type=int, default=640)
     ap.add_argument("--k", type=int, default=2)
     ap.add_argument("--reps", type=int, default=3)
@@ -60,6 +62,8 @@ def main():
             fb.lib.femd_cuda_spmv(ctx.h, K.h, _ptr(x), _ptr(y))
         elif a.kernel == "assemble":
             fb.assemble_matrix_2d(Qa, Qa, [1, 2, 0], [1, 2, 0], [1.0, 1.0, 1.0], K)
+        elif a.kernel == "assemble_values":
+            fb.assemble_matrix_2d(Qa, Qa, [1, 2, 0], [1, 2, 0], [1.0, 1.0, 1.0], K, jacobi=False)
         elif a.kernel == "rhs":
             fb.assemble_vector_2d(Qf, [0], [fb.Coef.helmholtz_sinsin(2 * PI * PI, PI, PI)], P, out=y)
         elif a.kernel == "pattern":
@@ -92,13 +96,23 @@ def batch(a):
     for _ in range(a.reps):
         xs, res = B.solve(bs, tol=1e-10, max_iter=a.iters, mixed=a.mixed, engine=engine)
     sizes = [(K.nrows, K.nnz) for K, _ in probs]
-    alg = W.batch_bytes(sizes, res, a.mixed)
+    compact = engine == "lockstep" and a.mixed and B.lockstep_stats()["plain"] == 0
+    alg = W.batch_bytes(sizes, res, a.mixed, compact)
     t = res[0]["seconds"]
     if engine == "lockstep":
         its = [r["iterations"] for r in res]
-        print(f"lockstep ({'mixed' if a.mixed else 'fp64'}): {len(probs)} problems, n {sum(n for n, _ in sizes)} "
-              f"nnz {sum(z for _, z in sizes)}, iterations max {max(its)} sum {sum(its)}: {t * 1e3:.3f} ms, "
-              f"algorithmic {alg} B = {alg / t / 1e9:.1f} GB/s")
+        n_all, z_all = sum(n for n, _ in sizes), sum(z for _, z in sizes)
+        print(f"lockstep ({'mixed' if a.mixed else 'fp64'}): {len(probs)} problems, n {n_all} nnz {z_all}, iterations "
+              f"max {max(its)} sum {sum(its)}: {t * 1e3:.3f} ms, algorithmic {alg} B = {alg / t / 1e9:.1f} GB/s; "
+              f"layout {B.lockstep_stats()}")
+        # one launch of each kernel while every member runs (what an ncu capture of an early launch sees)
+        st = B.lockstep_stats()
+        if a.mixed and st["compact"] == len(probs):
+            spmv = 6 * z_all + 4 * (n_all + len(probs)) + 16 * n_all
+            upd = 32 * n_all
+            print(f"per launch, every member running: k_ls_spmv<true> (compact) {spmv} B (6 B / nonzero: value and 16-bit "
+                  f"offset; 4 B / row pointer; z and the previous direction read, the direction and A p written: "
+                  f"16 B / row), k_ls_update<true> {upd} B (r, A p, inv, d, p read; r, z, d written: 32 B / row)")
         return
     pr = B.profile()
     print(f"batch ({'mixed' if a.mixed else 'fp64'}): {len(probs)} problems, n {sum(n for n, _ in sizes)} "

@@ -74,19 +74,21 @@ def l2_error(V, coeffs, exact, degree=None):
     return float(np.sqrt(np.sum(det[:, None] * Q.w[None, :] * err * err)))
 
 
-def batch_bytes(sizes, results, mixed=True):
-    """Algorithmic HBM bytes of one batched PCG launch, from each member's (n, nnz) and its result
+def batch_bytes(sizes, results, mixed=True, compact=False):
+    """Algorithmic HBM bytes of one batched PCG solve, from each member's (n, nnz) and its result
     (iterations, reliable_updates).  Per member and iteration: the SpMV's matrix (8 B / nonzero
-    in FP32, value + column index; 12 in FP64) and vectors (gathers of z and the previous
-    direction, stores of the direction and A p; the update's loads of r, A p, inv, x or d, p and
-    stores of r, z, x or d: 12 accesses of 4 or 8 B per row); per reliable update and at the start
-    an FP64 residual (12 B / nonzero, and b, x, inv, r, z: 40 B / row); in mixed mode the FP32 copy
-    of the matrix made at the start (12 B / nonzero)."""
+    in FP32, value + column index -- 6 in the compact layout, value + 16-bit offset; 12 in FP64)
+    and vectors (reads of z and the previous direction, stores of the direction and A p; the
+    update's loads of r, A p, inv, x or d, p and stores of r, z, x or d: 12 accesses of 4 or 8 B
+    per row); per reliable update and at the start an FP64 residual (12 B / nonzero, and b, x,
+    inv, r, z: 40 B / row); in mixed mode the FP32 copy of the matrix made at the start (12 B /
+    nonzero; 16 with the compact layout's position map)."""
     tot = 0
+    per_nnz = 6 if compact else 8
     for (n, nnz), r in zip(sizes, results):
         its, rus = r["iterations"], r.get("reliable_updates", 0)
         if mixed:
-            tot += its * (8 * nnz + 48 * n) + (rus + 1) * (12 * nnz + 40 * n) + 12 * nnz
+            tot += its * (per_nnz * nnz + 48 * n) + (rus + 1) * (12 * nnz + 40 * n) + (16 if compact else 12) * nnz
         else:
             tot += its * (12 * nnz + 96 * n) + 2 * (12 * nnz + 40 * n)
     return tot
