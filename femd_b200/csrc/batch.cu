@@ -2293,10 +2293,20 @@ struct LsLive {
     DevBuf<LBlock> d_tab;
     DevBuf<double> d_part;
     DevBuf<int> d_int;                                     // active (unused), ru_count, ru_list (tab_cap)
-    void *pin = nullptr;                                   // pinned: states (cap), descriptor staging, table
+    void *pin = nullptr;                                   // pinned: descriptor staging, states (2 x cap), tables (2 x tab_cap)
     size_t pin_b = 0;
+    // the CUDA graph of a chunk and the table shape it was captured for
+    cudaGraphExec_t gx = nullptr;
+    size_t g_nodes = 0;
+    int g_ne32 = -1, g_ne64 = -1, g_chunk = 0;
+    const LBlock *g_tab = nullptr;
+    const BProb *g_desc = nullptr;
+    const LState *g_state = nullptr;
+    size_t g_win = 0;
+    bool g_refused = false;
     ~LsLive()
     {
+        if (gx) cudaGraphExecDestroy(gx);
         if (pin) cudaFreeHost(pin);
     }
 };
@@ -2335,7 +2345,7 @@ static int live_grow(femd_batch_s *B, LsLive &L, size_t ntab)
         if ((st = L.d_tab.alloc(nc)) || (st = L.d_part.alloc(3 * nc + 3)) || (st = L.d_int.alloc(nc + 2))) return st;
         L.tab_cap = nc;
     }
-    const size_t need = (size_t)cap * sizeof(LState) + sizeof(BProb) + L.tab_cap * sizeof(LBlock) + 64;
+    const size_t need = 2 * (size_t)cap * sizeof(LState) + sizeof(BProb) + 2 * L.tab_cap * sizeof(LBlock) + 64;
     if (need > L.pin_b) {
         FEMD_TRY_CUDA(cudaStreamSynchronize(s));
         if (L.pin) cudaFreeHost(L.pin);
@@ -2394,7 +2404,7 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
     FEMD_CHECK_ARG(ntab < (size_t)INT_MAX / 4, "batch: too many table entries");
     if ((st = live_grow(B, L, ntab + 1))) return st;
     LState *hs = reinterpret_cast<LState *>(static_cast<char *>(L.pin) + sizeof(BProb) + 64);
-    LBlock *ht = reinterpret_cast<LBlock *>(hs + L.cap);
+    LBlock *ht = reinterpret_cast<LBlock *>(hs + 2 * (size_t)L.cap);
     int *active = L.d_int.p, *ru_count = L.d_int.p + 1, *ru_list = L.d_int.p + 2;
     const int G1 = std::max(1, 8 * ctx->sm_count);
     const size_t win_b = (size_t)L.maxwin * sizeof(float);
@@ -2443,15 +2453,12 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
     }
     // chunks of iterations over the members in flight; the states are read after each chunk
     const int C = std::max(1, B->ls_chunk);
-    FEMD_TRY_CUDA(cudaMemcpyAsync(hs, L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
-    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
-    for (int j = 0; j < std::max(1, chunks); ++j) {
-        std::vector<int> l32, l64;
-        for (int id : L.ids)
-            if (!hs[id].done) (L.f64[id] ? l64 : l32).push_back(id);
-        if (l32.empty() && l64.empty()) break;
-        const int NE32 = live_table(L, l32, ht), NE64 = live_table(L, l64, ht + NE32);
-        FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_tab.p, ht, (size_t)(NE32 + NE64) * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+    // host buffers: the states after the previous chunk and after this one, two tables (an upload
+    // may still be pending from one while the other is rewritten)
+    LState *hsb[2] = {hs, hs + L.cap};
+    LBlock *htb[2] = {reinterpret_cast<LBlock *>(hs + 2 * (size_t)L.cap), nullptr};
+    htb[1] = htb[0] + L.tab_cap;
+    auto enqueue_chunk = [&](int NE32, int NE64) {
         const LBlock *T32 = L.d_tab.p, *T64 = L.d_tab.p + NE32;
         for (int c = 0; c < C; ++c) {
             if (NE32) {
@@ -2470,11 +2477,94 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
                                                                   ru_count);
             }
         }
-        FEMD_TRY_CUDA(cudaGetLastError());
-        FEMD_TRY_CUDA(cudaMemcpyAsync(hs, L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
-        FEMD_TRY_CUDA(cudaStreamSynchronize(s));           // the host table is rewritten next chunk
-        if (*(volatile int *)B->abort_host) break;
+    };
+    // a chunk runs as one CUDA graph, captured again only when the table changes (the kernels read
+    // the table from device memory, so a table of the same shape reuses the graph)
+    auto launch_chunk = [&](int NE32, int NE64) -> cudaError_t {
+        const bool same = L.gx && L.g_ne32 == NE32 && L.g_ne64 == NE64 && L.g_tab == L.d_tab.p && L.g_desc == L.d_desc.p &&
+                          L.g_state == L.d_state.p && L.g_win == win_b && L.g_chunk == C;
+        if (!same && !L.g_refused) {
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                enqueue_chunk(NE32, NE64);
+                e = cudaStreamEndCapture(s, &g);
+            }
+            if (e == cudaSuccess && L.gx) {
+                cudaGraphExecUpdateResultInfo info;
+                if (cudaGraphExecUpdate(L.gx, g, &info) != cudaSuccess) {
+                    cudaGetLastError();
+                    cudaGraphExecDestroy(L.gx);
+                    L.gx = nullptr;
+                }
+            }
+            if (e == cudaSuccess && !L.gx) e = cudaGraphInstantiate(&L.gx, g, 0);
+            if (e == cudaSuccess) cudaGraphGetNodes(g, nullptr, &L.g_nodes);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                // this runtime did not capture the chunk: direct launches from now on
+                cudaGetLastError();
+                if (L.gx) cudaGraphExecDestroy(L.gx);
+                L.gx = nullptr;
+                L.g_refused = true;
+            } else {
+                L.g_ne32 = NE32;
+                L.g_ne64 = NE64;
+                L.g_tab = L.d_tab.p;
+                L.g_desc = L.d_desc.p;
+                L.g_state = L.d_state.p;
+                L.g_win = win_b;
+                L.g_chunk = C;
+            }
+        }
+        if (L.gx && !L.g_refused) return launch_graph(L.gx, L.g_nodes, s);
+        enqueue_chunk(NE32, NE64);
+        return cudaGetLastError();
+    };
+    // the table of the live members (their entries in admission order)
+    auto build = [&](const LState *S, LBlock *T, int &NE32, int &NE64) {
+        std::vector<int> l32, l64;
+        for (int id : L.ids)
+            if (!S[id].done) (L.f64[id] ? l64 : l32).push_back(id);
+        NE32 = live_table(L, l32, T);
+        NE64 = live_table(L, l64, T + NE32);
+        return NE32 + NE64;
+    };
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    FEMD_TRY_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    FEMD_TRY_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    struct EvG2 {
+        cudaEvent_t *e;
+        ~EvG2() { for (int k = 0; k < 2; ++k) if (e[k]) cudaEventDestroy(e[k]); }
+    } evg2{ev};
+    FEMD_TRY_CUDA(cudaMemcpyAsync(hsb[0], L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    int tb = 0, NE32 = 0, NE64 = 0;
+    int NE = build(hsb[0], htb[tb], NE32, NE64);
+    if (NE) FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_tab.p, htb[tb], (size_t)NE * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+    const int nchunks = std::max(1, chunks);
+    for (int j = 0; j < nchunks && NE; ++j) {
+        FEMD_TRY_CUDA(launch_chunk(NE32, NE64));
+        FEMD_TRY_CUDA(cudaMemcpyAsync(hsb[j & 1], L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
+        FEMD_TRY_CUDA(cudaEventRecord(ev[j & 1], s));
+        if (j == 0) continue;
+        // the states after the previous chunk (this one stays queued behind them)
+        FEMD_TRY_CUDA(cudaEventSynchronize(ev[(j - 1) & 1]));
+        const LState *S = hsb[(j - 1) & 1];
+        int live_e = 0, live = 0;
+        for (int id : L.ids)
+            if (!S[id].done) { ++live; live_e += (int)L.ents[id].size(); }
+        if (live == 0 || *(volatile int *)B->abort_host) break;
+        if (live_e <= (NE * 7) / 10) {
+            // compact the table to the live members (uploaded behind the queued chunk)
+            tb ^= 1;
+            NE = build(S, htb[tb], NE32, NE64);
+            FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_tab.p, htb[tb], (size_t)NE * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+        }
     }
+    FEMD_TRY_CUDA(cudaMemcpyAsync(hs, L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));                // hs: the states after the last chunk
+    ht = htb[tb ^ 1];                                       // free for the finishing table below
     // the members that are done: the end of their solve (the final true residual in FP64, the
     // flush of a mixed member that broke down, x = 0 for b = 0), then their results
     std::vector<int> d32, d64, back, keep;
@@ -2493,16 +2583,16 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
         }
         (L.f64[id] ? d64 : d32).push_back(id);
     }
-    const int NE32 = live_table(L, d32, ht), NE64 = live_table(L, d64, ht + NE32);
-    if (NE32 + NE64) {
-        FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_tab.p, ht, (size_t)(NE32 + NE64) * sizeof(LBlock), cudaMemcpyHostToDevice, s));
-        if (NE32)
-            k_ls_flush<true><<<std::min(G1, NE32), LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p, NE32, L.d_state.p, ru_list,
+    const int FE32 = live_table(L, d32, ht), FE64 = live_table(L, d64, ht + FE32);
+    if (FE32 + FE64) {
+        FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_tab.p, ht, (size_t)(FE32 + FE64) * sizeof(LBlock), cudaMemcpyHostToDevice, s));
+        if (FE32)
+            k_ls_flush<true><<<std::min(G1, FE32), LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p, FE32, L.d_state.p, ru_list,
                                                                            ru_count);
-        if (NE64)
-            k_ls_resid<false, 2><<<NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p + NE32, NE64, L.d_state.p, L.d_part.p,
+        if (FE64)
+            k_ls_resid<false, 2><<<FE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p + FE32, FE64, L.d_state.p, L.d_part.p,
                                                                   active, ru_list, ru_count);
-        k_ls_zero<<<NE32 + NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p, L.d_state.p);
+        k_ls_zero<<<FE32 + FE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, L.d_tab.p, L.d_state.p);
         FEMD_TRY_CUDA(cudaGetLastError());
         FEMD_TRY_CUDA(cudaMemcpyAsync(hs, L.d_state.p, (size_t)L.cap * sizeof(LState), cudaMemcpyDeviceToHost, s));
     }
