@@ -978,13 +978,27 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
                     S[(size_t)k * nl2 + l * nl + j] = acc;
                 }
     }
-    if (p->ws_tables.n < tab.size()) FEMD_TRY(p->ws_tables.alloc(tab.size()));
     if (p->ws_factors.n < (size_t)ne * fs.nf + 1) FEMD_TRY(p->ws_factors.alloc((size_t)ne * fs.nf + 1));
-    FEMD_TRY_CUDA(cudaMemcpyAsync(p->ws_tables.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    const double *d_ref = p->ws_tables.p + 3 * nq, *d_S = d_ref + nref;
+    // the slot holding these tables, else the least recently used one, refilled (stream-ordered,
+    // so kernels still reading the slot's old tables finish first)
+    femd_pattern_s::TableSlot *slot = nullptr;
+    for (auto &t : p->tables)
+        if (t.host == tab) { slot = &t; break; }
+    if (!slot) {
+        slot = &p->tables[0];
+        for (auto &t : p->tables)
+            if (t.used < slot->used) slot = &t;
+        slot->host.clear();
+        if (slot->dev.n < tab.size()) FEMD_TRY(slot->dev.alloc(tab.size()));
+        FEMD_TRY_CUDA(cudaMemcpyAsync(slot->dev.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        slot->host = std::move(tab);
+    }
+    slot->used = ++p->table_clock;
+    const double *d_tab = slot->dev.p;
+    const double *d_ref = d_tab + 3 * nq, *d_S = d_ref + nref;
     if (ne)
         k_elem_factors<<<grid_for((size_t)ne, 256, 1u << 22), 256, 0, counted(s)>>>(
-            mesh->points_dev, mesh->tris_dev, ne, nq, nl, p->cell_dofs.p, p->ws_tables.p, fs, p->ws_factors.p);
+            mesh->points_dev, mesh->tris_dev, ne, nq, nl, p->cell_dofs.p, d_tab, fs, p->ws_factors.p);
     FEMD_TRY_CUDA(cudaGetLastError());
     if (vector) {
         const size_t shm = (3 * (size_t)nl + nref) * sizeof(double);

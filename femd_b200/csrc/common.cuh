@@ -113,7 +113,18 @@ struct femd_pattern_s : femd::HandleBase {
     int max_row_cells = 0, max_row_len = 0;
     // assembly workspace, grown on demand and reused across calls (no allocation per call
     // once it has its size): per-element factors, the rule's tables
-    femd::DevBuf<double> ws_factors, ws_tables;
+    femd::DevBuf<double> ws_factors;
+    // the rule's tables (weights, points, reference values, the pair tensors) of the last few
+    // forms, each with the host copy it was uploaded from: a repeated assembly of the same form
+    // uploads nothing (a pageable upload can wait for the stream)
+    struct TableSlot {
+        femd::DevBuf<double> dev;
+        std::vector<double> host;
+        unsigned long long used = 0;
+    };
+    static constexpr int TABLE_SLOTS = 4;
+    TableSlot tables[TABLE_SLOTS];
+    unsigned long long table_clock = 0;
     // the scatter map inverted: for every matrix position, its element entries
     // (cell nloc^2 + l nloc + j) in increasing cell order (built on the first FAST assembly)
     femd::DevBuf<int> contrib_ptr, contrib;
