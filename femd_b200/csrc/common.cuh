@@ -97,6 +97,10 @@ void ctx_release(femd_ctx ctx);
 // the preconditioners of precond.cu: z = M^{-1} r enqueued on s (skipped when *skip is set)
 int precond_enqueue(femd_precond P, const double *r, double *z, const int *skip, cudaStream_t s);
 int precond_rows(femd_precond P);
+// The FP32 copy of a matrix in row-sum form (the mixed-precision inner iteration): position q of
+// the original CSR goes to a32[dst ? dst[q] : q] as (float) a[q], except each row's diagonal
+// position, which takes (float) of the row's FP64 sum.  Needs every diagonal position.
+int f32_rowsum_copy(femd_pattern P, const double *a, const int *dst, float *a32, cudaStream_t s);
 femd_ctx precond_ctx(femd_precond P);
 femd_pattern precond_pattern(femd_precond P);
 }  // namespace femd
@@ -110,6 +114,7 @@ struct femd_pattern_s : femd::HandleBase {
     femd::DevBuf<int> rc_ptr, rc_code; // row -> (cell nloc + local), increasing cell order
     femd::DevBuf<int> map;             // scatter map, ne nloc^2 (built on demand)
     femd::DevBuf<int> diag_pos;        // position of (i, i), -1 when absent
+    bool all_diag = false;             // every row i holds the position (i, i)
     int max_row_cells = 0, max_row_len = 0;
     // assembly workspace, grown on demand and reused across calls (no allocation per call
     // once it has its size): per-element factors, the rule's tables

@@ -15,6 +15,7 @@
 // HBM bytes per FP64 iteration (n rows, nnz entries): SpMV 12 nnz + 4 (n+1) + 8 n (p) + 8 n (Ap);
 // update 40 n read + 16 n written; direction 24 n read + 8 n written.
 #include <climits>
+#include <type_traits>
 #include <cmath>
 #include <memory>
 #include <mutex>
@@ -97,6 +98,11 @@ __device__ __forceinline__ void reduce_partials(const T *part, int np, int ld, T
 // index and value loads are issued together, then the U gathers of x, then the U products
 // (memory-level parallelism for a latency-bound stream).  The lane's additions stay in entry
 // order, so U does not change the result; TPR does (the shuffle tree).
+// With FP32 values (the mixed-precision copy, made by f32_rowsum_copy) the row is in row-sum
+// form: y_i = s_i x_i + sum_{j != i} a_ij (x_j - x_i), s_i the row's sum, held at the diagonal
+// position.  The represented matrix keeps the FP64 matrix's row sums, so rounding the entries to
+// FP32 perturbs its quadratic form by O(eps_32) relative instead of O(eps_32 cond(A)), and the
+// differences keep the FP32 products of smooth vectors accurate.
 template <class V, class T, int TPR, int U, bool DOT>
 __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indptr, const int *__restrict__ indices,
                                                     const V *__restrict__ vals, const T *__restrict__ x,
@@ -104,6 +110,7 @@ __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indp
                                                     CGState<T> *__restrict__ st)
 {
     __shared__ double sh[32];
+    constexpr bool ROWSUM = std::is_same<V, float>::value;
     if (DOT && (st->done || st->want_ru)) return;
     const int lane = threadIdx.x % TPR;
     constexpr int GPW = 32 / TPR;   // rows per warp per step
@@ -115,6 +122,7 @@ __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indp
         T s = T(0);
         if (i < n) {
             const int lo = indptr[i], hi = indptr[i + 1];
+            const T xi = ROWSUM ? __ldg(&x[i]) : T(0);
             for (int base = lo + lane; base < hi; base += U * TPR) {
                 int c[U];
                 V v[U];
@@ -131,7 +139,7 @@ __global__ void __launch_bounds__(RED_BLOCK) k_spmv(const int *__restrict__ indp
                 for (int u = 0; u < U; ++u) xv[u] = base + u * TPR < hi ? __ldg(&x[c[u]]) : T(0);
 #pragma unroll
                 for (int u = 0; u < U; ++u)
-                    if (base + u * TPR < hi) s += (T)v[u] * xv[u];
+                    if (base + u * TPR < hi) s += (T)v[u] * (ROWSUM && c[u] != i ? xv[u] - xi : xv[u]);
             }
         }
 #pragma unroll
@@ -792,6 +800,35 @@ static int cg_run(femd_ctx ctx, femd_matrix K, bool jac, const double *b, double
     return status;
 }
 
+__global__ void k_f32_rowsum(const int *__restrict__ indptr, const int *__restrict__ diag_pos, const double *__restrict__ a,
+                             const int *__restrict__ dst, float *__restrict__ a32, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int lo = indptr[i], hi = indptr[i + 1];
+        double sum = 0.0;
+        for (int q = lo; q < hi; ++q) {
+            const double v = a[q];
+            sum += v;
+            a32[dst ? dst[q] : q] = (float)v;
+        }
+        const int d = diag_pos[i];
+        a32[dst ? dst[d] : d] = (float)sum;
+    }
+}
+
+int f32_rowsum_copy(femd_pattern P, const double *a, const int *dst, float *a32, cudaStream_t s)
+{
+    if (!P->all_diag) {
+        set_error("mixed precision: a row of the matrix has no diagonal entry (the matrix is not SPD)");
+        return FEMD_EINVAL;
+    }
+    if (P->nrows)
+        k_f32_rowsum<<<grid_for((size_t)P->nrows, 128, 1u << 20), 128, 0, counted(s)>>>(P->indptr.p, P->diag_pos.p, a, dst, a32,
+                                                                                       P->nrows);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    return FEMD_OK;
+}
+
 static int ensure_f32(femd_ctx ctx, femd_matrix K)
 {
     if (K->f32_valid) return FEMD_OK;
@@ -799,7 +836,7 @@ static int ensure_f32(femd_ctx ctx, femd_matrix K)
     const int n = K->pattern->nrows;
     if (!K->data32.p) FEMD_TRY(K->data32.alloc((size_t)nnz + 1));
     if (!K->inv32.p) FEMD_TRY(K->inv32.alloc((size_t)n + 1));
-    if (nnz) k_to_f32<<<grid_for((size_t)nnz, 256, 1u << 20), 256, 0, counted(ctx->stream)>>>(K->data.p, K->data32.p, nnz);
+    FEMD_TRY(f32_rowsum_copy(K->pattern, K->data.p, nullptr, K->data32.p, ctx->stream));
     if (n) k_to_f32<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(ctx->stream)>>>(K->inv.p, K->inv32.p, n);
     FEMD_TRY_CUDA(cudaGetLastError());
     K->f32_valid = true;

@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(PAT_WARPS * 32) k_pattern_rows(const int *__re
 }
 
 __global__ void k_diag_pos(const int *__restrict__ indptr, const int *__restrict__ indices, int nrows, int ncols,
-                           int *__restrict__ diag)
+                           int *__restrict__ diag, int *__restrict__ missing)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nrows) return;
@@ -132,6 +132,7 @@ __global__ void k_diag_pos(const int *__restrict__ indptr, const int *__restrict
         if (indices[mid] < i) lo = mid + 1; else hi = mid;
     }
     diag[i] = (i < ncols && lo < end && indices[lo] == i) ? lo : -1;
+    if (diag[i] < 0 && missing) atomicAdd(missing, 1);
 }
 
 // ---- K2: scatter map ------------------------------------------------------------------------
@@ -229,11 +230,11 @@ int femd_cuda_pattern_from_cells(femd_ctx ctx, int nrows, int ncells, int nloc, 
     DevBuf<int> maxc;
     if ((st = cnt.alloc((size_t)nrows + 1)) || (st = tmp.alloc(scan_tmp_ints((size_t)nrows + 1))) ||
         (st = p->rc_ptr.alloc((size_t)nrows + 1)) || (st = p->indptr.alloc((size_t)nrows + 1)) ||
-        (st = fill.alloc((size_t)nrows + 1)) || (st = rowlen.alloc((size_t)nrows + 1)) || (st = maxc.alloc(1)))
+        (st = fill.alloc((size_t)nrows + 1)) || (st = rowlen.alloc((size_t)nrows + 1)) || (st = maxc.alloc(2)))
         return fail(st);
     if ((st = reset_status(ctx))) return fail(st);
     cudaMemsetAsync(cnt.p, 0, ((size_t)nrows + 1) * sizeof(int), s);
-    cudaMemsetAsync(maxc.p, 0, sizeof(int), s);
+    cudaMemsetAsync(maxc.p, 0, 2 * sizeof(int), s);   // the most cells of a row, the rows without a diagonal
     if (tot) k_count_rows<<<grid_for((size_t)tot, 256, 1u << 20), 256, 0, counted(s)>>>(p->cell_dofs.p, tot, nrows, cnt.p, ctx->status_dev);
     if ((st = exclusive_scan_int(cnt.p, p->rc_ptr.p, (size_t)nrows + 1, tmp.p, s))) return fail(st);
     int flags = 0;
@@ -274,15 +275,16 @@ int femd_cuda_pattern_from_cells(femd_ctx ctx, int nrows, int ncells, int nloc, 
         k_pattern_rows<true><<<pgrid, PAT_WARPS * 32, 0, counted(s)>>>(p->cell_dofs.p, nloc, p->rc_ptr.p, p->rc_code.p, nrows,
                                                                nullptr, p->indptr.p, p->indices.p, ctx->status_dev);
     if ((st = p->diag_pos.alloc((size_t)nrows + 1))) return fail(st);
-    if (nrows) k_diag_pos<<<grid_for((size_t)nrows, 256), 256, 0, counted(s)>>>(p->indptr.p, p->indices.p, nrows, nrows, p->diag_pos.p);
+    if (nrows)
+        k_diag_pos<<<grid_for((size_t)nrows, 256), 256, 0, counted(s)>>>(p->indptr.p, p->indices.p, nrows, nrows, p->diag_pos.p,
+                                                                          maxc.p + 1);
     e = cudaGetLastError();
     if (e != cudaSuccess) { set_error(std::string("cell_pattern: ") + cudaGetErrorString(e)); return fail(FEMD_ECUDA); }
-    int mc = 0;
-    e = cudaMemcpyAsync(&ctx->status_host[3], maxc.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(&ctx->status_host[2], maxc.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { set_error(std::string("cell_pattern: ") + cudaGetErrorString(e)); return fail(FEMD_ECUDA); }
-    mc = ctx->status_host[3];
-    p->max_row_cells = mc;
+    p->max_row_cells = ctx->status_host[2];
+    p->all_diag = ctx->status_host[3] == 0;
     *out = p;
     return FEMD_OK;
 }
@@ -296,8 +298,12 @@ int femd_cuda_pattern_from_csr_host(femd_ctx ctx, int nrows, int ncols, const in
     *out = nullptr;
     const int nnz = indptr_host[nrows];
     FEMD_CHECK_ARG(indptr_host[0] == 0 && nnz >= 0, "CSRMatrix: indptr must start at 0");
+    bool all_diag = nrows == ncols;
     for (int i = 0; i < nrows; ++i) {
         FEMD_CHECK_ARG(indptr_host[i + 1] >= indptr_host[i], "CSRMatrix: indptr must be non-decreasing");
+        bool has = false;
+        for (int q = indptr_host[i]; q < indptr_host[i + 1] && !has; ++q) has = indices_host[q] == i;
+        all_diag = all_diag && has;
         for (int q = indptr_host[i] + 1; q < indptr_host[i + 1]; ++q)
             FEMD_CHECK_ARG(indices_host[q] > indices_host[q - 1],
                            "CSRMatrix.from_arrays: column indices must be sorted (call sort_indices())");
@@ -312,6 +318,7 @@ int femd_cuda_pattern_from_csr_host(femd_ctx ctx, int nrows, int ncols, const in
     p->nrows = nrows;
     p->ncols = ncols;
     p->nnz = nnz;
+    p->all_diag = all_diag;
     int st;
     if ((st = p->indptr.alloc((size_t)nrows + 1)) || (st = p->indices.alloc((size_t)nnz + 1)) ||
         (st = p->diag_pos.alloc((size_t)nrows + 1))) { delete p; return st; }
@@ -319,7 +326,8 @@ int femd_cuda_pattern_from_csr_host(femd_ctx ctx, int nrows, int ncols, const in
     if (e == cudaSuccess && nnz)
         e = cudaMemcpyAsync(p->indices.p, indices_host, (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess && nrows) {
-        k_diag_pos<<<grid_for((size_t)nrows, 256), 256, 0, counted(ctx->stream)>>>(p->indptr.p, p->indices.p, nrows, ncols, p->diag_pos.p);
+        k_diag_pos<<<grid_for((size_t)nrows, 256), 256, 0, counted(ctx->stream)>>>(p->indptr.p, p->indices.p, nrows, ncols, p->diag_pos.p,
+                                                                                      nullptr);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
