@@ -602,11 +602,51 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows_off(
 // and adds them in cell order in a register, then writes the value once -- consecutive threads
 // write consecutive positions.  No accumulator in shared memory and no atomics; the value is the
 // sum of its element contributions in increasing element order, as in the reference.
+//
+// The chain of loads per position (list bounds, then entry codes, then the cell's factors) is
+// latency-bound when a thread walks one position at a time, so with constant coefficients a
+// thread takes U positions of a tile (p = tile + u blockDim + tid, coalesced for every u) and
+// issues each level's loads for all of them, the first two entries of every position included
+// (most positions have one or two), before the next level; longer lists finish in a loop.
 template <int NLOC, int NPAIR>
-__global__ void __launch_bounds__(256) k_assemble_nnz(const int *__restrict__ cptr, const int *__restrict__ cent,
-                                                      long long nnz, int nq, const double *__restrict__ factors,
-                                                      const double *__restrict__ g_S, const double *__restrict__ g_R,
-                                                      FastSpec fs, double *__restrict__ data)
+__device__ __forceinline__ double nnz_entry(int code, const double *__restrict__ F, const double *sS, const double *sR,
+                                            int nq, const FastSpec &fs)
+{
+    constexpr int NL2 = NLOC * NLOC;
+    const int e = code / NL2, lj = code - e * NL2, l = lj / NLOC, j = lj - l * NLOC;
+    F += (size_t)e * fs.nf;
+    double v = 0.0;
+    if (fs.has_const) {
+#pragma unroll
+        for (int k = 0; k < NPAIR; ++k) v += __ldg(&F[k]) * sS[k * NL2 + l * NLOC + j];
+    }
+    if (fs.has_var) {
+        const double *H = F + (fs.has_const ? NPAIR : 0);
+        for (int q = 0; q < nq; ++q) {
+            const double *R = sR + q * 3 * NLOC;
+#pragma unroll
+            for (int k = 0; k < NPAIR; ++k) v += (__ldg(&H[q * NPAIR + k]) * R[fs.pr[k] * NLOC + l]) * R[fs.ps[k] * NLOC + j];
+        }
+    }
+    return v;
+}
+
+template <int NLOC, int NPAIR>
+__device__ __forceinline__ double nnz_const(int code, const double (&f)[NPAIR], const double *sS)
+{
+    constexpr int NL2 = NLOC * NLOC;
+    const int lj = code % NL2;
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < NPAIR; ++k) v += f[k] * sS[k * NL2 + lj];
+    return v;
+}
+
+template <int NLOC, int NPAIR, int U, bool VAR>
+__global__ void __launch_bounds__(256, 2) k_assemble_nnz(const int *__restrict__ cptr, const int *__restrict__ cent,
+                                                         long long nnz, int nq, const double *__restrict__ factors,
+                                                         const double *__restrict__ g_S, const double *__restrict__ g_R,
+                                                         FastSpec fs, double *__restrict__ data)
 {
     extern __shared__ double smem[];
     constexpr int NL2 = NLOC * NLOC;
@@ -614,33 +654,60 @@ __global__ void __launch_bounds__(256) k_assemble_nnz(const int *__restrict__ cp
     double *sR = sS + (fs.has_const ? NPAIR * NL2 : 0);
     if (fs.has_const)
         for (int t = threadIdx.x; t < NPAIR * NL2; t += blockDim.x) sS[t] = g_S[t];
-    if (fs.has_var)
+    if (VAR)
         for (int t = threadIdx.x; t < nq * 3 * NLOC; t += blockDim.x) sR[t] = g_R[t];
     __syncthreads();
-    const int cst = fs.has_const ? NPAIR : 0;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x) {
-        const int c0 = __ldcs(&cptr[p]), c1 = __ldcs(&cptr[p + 1]);
-        double acc = 0.0;
-        for (int c = c0; c < c1; ++c) {
-            const int code = __ldcs(&cent[c]);
-            const int e = code / NL2, lj = code - e * NL2, l = lj / NLOC, j = lj - l * NLOC;
-            const double *F = factors + (size_t)e * fs.nf;
-            double v = 0.0;
-            if (fs.has_const) {
-#pragma unroll
-                for (int k = 0; k < NPAIR; ++k) v += __ldg(&F[k]) * sS[k * NL2 + l * NLOC + j];
-            }
-            if (fs.has_var) {
-                const double *H = F + cst;
-                for (int q = 0; q < nq; ++q) {
-                    const double *R = sR + q * 3 * NLOC;
-#pragma unroll
-                    for (int k = 0; k < NPAIR; ++k) v += (__ldg(&H[q * NPAIR + k]) * R[fs.pr[k] * NLOC + l]) * R[fs.ps[k] * NLOC + j];
-                }
-            }
-            acc += v;
+    if (VAR) {
+        for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x) {
+            const int c0 = __ldcs(&cptr[p]), c1 = __ldcs(&cptr[p + 1]);
+            double acc = 0.0;
+            for (int c = c0; c < c1; ++c) acc += nnz_entry<NLOC, NPAIR>(__ldcs(&cent[c]), factors, sS, sR, nq, fs);
+            data[p] = acc;
         }
-        data[p] = acc;
+        return;
+    }
+    const int nf = fs.nf;
+    const long long tile = (long long)U * blockDim.x;
+    for (long long base = (long long)blockIdx.x * tile; base < nnz; base += (long long)gridDim.x * tile) {
+        int c0[U], c1[U], k0[U], k1[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long p = base + u * (long long)blockDim.x + threadIdx.x;
+            c0[u] = p < nnz ? __ldcs(&cptr[p]) : 0;
+            c1[u] = p < nnz ? __ldcs(&cptr[p + 1]) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            k0[u] = c0[u] < c1[u] ? __ldcs(&cent[c0[u]]) : -1;
+            k1[u] = c0[u] + 1 < c1[u] ? __ldcs(&cent[c0[u] + 1]) : -1;
+        }
+        double f0[U][NPAIR], f1[U][NPAIR];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double *F0 = factors + (size_t)(k0[u] < 0 ? 0 : k0[u] / NL2) * nf;
+            const double *F1 = factors + (size_t)(k1[u] < 0 ? 0 : k1[u] / NL2) * nf;
+#pragma unroll
+            for (int k = 0; k < NPAIR; ++k) {
+                f0[u][k] = k0[u] >= 0 ? __ldg(&F0[k]) : 0.0;
+                f1[u][k] = k1[u] >= 0 ? __ldg(&F1[k]) : 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long p = base + u * (long long)blockDim.x + threadIdx.x;
+            double acc = 0.0;
+            if (k0[u] >= 0) acc += nnz_const<NLOC, NPAIR>(k0[u], f0[u], sS);
+            if (k1[u] >= 0) acc += nnz_const<NLOC, NPAIR>(k1[u], f1[u], sS);
+            for (int c = c0[u] + 2; c < c1[u]; ++c) {
+                const int code = __ldcs(&cent[c]);
+                const double *F = factors + (size_t)(code / NL2) * nf;
+                double f[NPAIR];
+#pragma unroll
+                for (int k = 0; k < NPAIR; ++k) f[k] = __ldg(&F[k]);
+                acc += nnz_const<NLOC, NPAIR>(code, f, sS);
+            }
+            if (p < nnz) data[p] = acc;
+        }
     }
 }
 
@@ -940,6 +1007,10 @@ static int prepare_terms(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
 }
 
 static constexpr int FAST_MAX_ROW = 96;   // longest row the shared-memory accumulator holds
+#ifndef FEMD_NNZ_U
+#define FEMD_NNZ_U 4
+#endif
+static constexpr int NNZ_U = FEMD_NNZ_U;  // positions per thread in flight in k_assemble_nnz
 
 // FAST assembly of a matrix (K non-null) or a vector (f non-null).  Tables and factors live in
 // the pattern's workspace; no allocation once the workspace has its size.
@@ -1028,9 +1099,17 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
 #define FEMD_NNZ(NL, NP)                                                                                               \
         if (!done && nl == NL && fs.npair == NP && p->nnz > 0 && B_NNZ) {                                             \
             const size_t shn = ((fs.has_const ? (size_t)NP * NL * NL : 0) + (fs.has_var ? nref : 0)) * sizeof(double); \
-            cudaFuncSetAttribute(k_assemble_nnz<NL, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shn);       \
-            k_assemble_nnz<NL, NP><<<grid_for((size_t)p->nnz, 256, (unsigned)ctx->sm_count * 64), 256, shn, counted(s)>>>( \
-                p->contrib_ptr.p, p->contrib.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs, K->data.p);                \
+            const unsigned gq = (unsigned)ctx->sm_count * 64;                                                         \
+            if (fs.has_var) {                                                                                          \
+                cudaFuncSetAttribute(k_assemble_nnz<NL, NP, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shn); \
+                k_assemble_nnz<NL, NP, 1, true><<<grid_for((size_t)p->nnz, 256, gq), 256, shn, counted(s)>>>(           \
+                    p->contrib_ptr.p, p->contrib.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs, K->data.p);            \
+            } else {                                                                                                   \
+                cudaFuncSetAttribute(k_assemble_nnz<NL, NP, NNZ_U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                     (int)shn);                                                                        \
+                k_assemble_nnz<NL, NP, NNZ_U, false><<<grid_for((size_t)p->nnz, 256 * NNZ_U, gq), 256, shn, counted(s)>>>( \
+                    p->contrib_ptr.p, p->contrib.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs, K->data.p);            \
+            }                                                                                                          \
             if (inv) k_asm_inv<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(p->diag_pos.p, K->data.p,   \
                                                                                             inv, n, ctx->status_dev);  \
             done = true;                                                                                               \
