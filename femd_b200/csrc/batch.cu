@@ -106,6 +106,18 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 }
 
 __device__ __forceinline__ float pdir(const float *z, const float *p, float beta, int j) { return __fmaf_rn(beta, p[j], z[j]); }
+
+// an L2 prefetch (cp.async.bulk.prefetch) of the whole 16-byte granules inside [b, e), in 4 KB
+// pieces spread over the lanes of a warp: only addresses of the range are touched
+__device__ __forceinline__ void l2_prefetch_range(const void *b, const void *e, int lane)
+{
+    const unsigned long long lo = ((unsigned long long)b + 15ull) & ~15ull, hi = (unsigned long long)e & ~15ull;
+    constexpr unsigned long long CH = 4096;
+    for (unsigned long long c = lo + (unsigned long long)lane * CH; c < hi; c += 32 * CH) {
+        const unsigned n = (unsigned)(hi - c < CH ? hi - c : CH);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c), "r"(n) : "memory");
+    }
+}
 __device__ __forceinline__ double pdir(const double *z, const double *p, double beta, int j) { return __fma_rn(beta, p[j], z[j]); }
 
 // team barrier: false when the batch has to stop (timeout or abort).  lead_sync: the block has
@@ -1098,10 +1110,36 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ 
         // compact layout: p over the entry's column window [w0, w1) into shared memory (the
         // owner's values to pnew), then the rows read it there
         const int c0 = L.w0, c1 = L.w1;
-        for (int w = c0 + (int)threadIdx.x; w < c1; w += LS_BB) {
-            const float pw = pdir((const float *)z, (const float *)pold, (float)beta, w);
-            ls_win[w - c0] = pw;
-            if (w >= L.r0 && w < L.r1) ((float *)pnew)[w] = pw;
+        // the last warp first asks L2 for the entry's values and offsets, which stream in while
+        // the window is formed
+        if (threadIdx.x >= LS_BB - 32) {
+            const int q0 = P.cptr[L.r0], q1 = P.cptr[L.r1];
+            l2_prefetch_range(A + q0, A + q1, threadIdx.x & 31);
+            l2_prefetch_range(P.coff + q0, P.coff + q1, threadIdx.x & 31);
+        }
+        // WU columns per thread and round, their loads issued before any store (the stores to
+        // pnew could alias z and pold for the compiler, which would serialise the round trips)
+        constexpr int WU = 4;
+        const float *zf = (const float *)z, *pf = (const float *)pold;
+        float *pn = (float *)pnew;
+        const float bf = (float)beta;
+        for (int w0 = c0 + (int)threadIdx.x; w0 < c1; w0 += WU * LS_BB) {
+            float zv[WU], pv[WU];
+#pragma unroll
+            for (int u = 0; u < WU; ++u) {
+                const int w = w0 + u * LS_BB;
+                zv[u] = w < c1 ? zf[w] : 0.0f;
+                pv[u] = w < c1 ? pf[w] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < WU; ++u) {
+                const int w = w0 + u * LS_BB;
+                if (w < c1) {
+                    const float pw = __fmaf_rn(bf, pv[u], zv[u]);
+                    ls_win[w - c0] = pw;
+                    if (w >= L.r0 && w < L.r1) pn[w] = pw;
+                }
+            }
         }
         __syncthreads();
         switch (P.tpr) {
@@ -1154,14 +1192,34 @@ __global__ void __launch_bounds__(LS_BB) k_ls_update(const BProb *__restrict__ p
     F *acc = MIXED ? (F *)P.d32 : (F *)P.x;
     const F alpha = (F)S.alpha;
     double v[2] = {0.0, 0.0};
-    for (int i = L.r0 + (int)threadIdx.x; i < L.r1; i += LS_BB) {
-        const F ri = r[i] - alpha * Ap[i];
-        const F zi = inv[i] * ri;
-        r[i] = ri;
-        z[i] = zi;
-        acc[i] = acc[i] + alpha * p[i];
-        v[0] += (double)ri * (double)ri;
-        v[1] += (double)ri * (double)zi;
+    // UU rows per thread and round (rows i, i + LS_BB, ...: the order of the sums is that of a
+    // row at a time), every load of the round issued before its stores
+    constexpr int UU = 4;
+    for (int i0 = L.r0 + (int)threadIdx.x; i0 < L.r1; i0 += UU * LS_BB) {
+        F rv[UU], av[UU], iv[UU], cv[UU], pv[UU];
+#pragma unroll
+        for (int u = 0; u < UU; ++u) {
+            const int i = i0 + u * LS_BB;
+            const bool ok = i < L.r1;
+            rv[u] = ok ? r[i] : F(0);
+            av[u] = ok ? Ap[i] : F(0);
+            iv[u] = ok ? inv[i] : F(0);
+            cv[u] = ok ? acc[i] : F(0);
+            pv[u] = ok ? p[i] : F(0);
+        }
+#pragma unroll
+        for (int u = 0; u < UU; ++u) {
+            const int i = i0 + u * LS_BB;
+            if (i < L.r1) {
+                const F ri = rv[u] - alpha * av[u];
+                const F zi = iv[u] * ri;
+                r[i] = ri;
+                z[i] = zi;
+                acc[i] = cv[u] + alpha * pv[u];
+                v[0] += (double)ri * (double)ri;
+                v[1] += (double)ri * (double)zi;
+            }
+        }
     }
     double tot[2];
     if (!ls_member_sum<2>(v, part, NE, e, L, &S.t2, tot)) return;
