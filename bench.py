@@ -662,10 +662,13 @@ def ours_c4(args, rank, world, dist):
                                f"FP32-inner / FP64-refined batched Jacobi-PCG to 1e-10 ({args.engine} engine)",
                    "problems": NPROB, "n_total": n, "nnz_total": nnz, "arrivals": "burst at t=0",
                    "p50_ms": round(st["p50_ms"], 2), "p99_ms": round(st["p99_ms"], 2),
-                   "mean_iterations": round(st["mean_iterations"], 1), "all_converged": st["all_converged"],
+                   "mean_iterations": round(st["mean_iterations"], 1), "max_iterations": st["max_iterations"],
+                   "slowest": [[r.N, r.k, r.iterations, r.outer] for r in sorted(last, key=lambda r: -r.iterations)[:4]],
+                   "all_converged": st["all_converged"],
                    "max_rel_diff_vs_plain_fp64": err,
                    "plain_fp64_gpu": {"solves_per_s": round(pst["solves_per_s"], 3), "p50_ms": round(pst["p50_ms"], 2),
                                       "p99_ms": round(pst["p99_ms"], 2), "mean_iterations": round(pst["mean_iterations"], 1),
+                                      "max_iterations": pst["max_iterations"],
                                       "path": "per request: FP64 assembly + cg_solve (CUDA-graph CG), FIFO"},
                    "served_over_plain": round(value / pst["solves_per_s"], 3),
                    "checker": chk,

@@ -365,6 +365,7 @@ __global__ void __launch_bounds__(256) k_elem_factors(const double *__restrict__
                 }
                 F[o++] = ad * acc;
             }
+            if (!fs.has_var && (fs.npair & 1)) F[o++] = 0.0;
         }
         if (fs.has_var) {
             for (int q = 0; q < nq; ++q) {
@@ -631,15 +632,36 @@ __device__ __forceinline__ double nnz_entry(int code, const double *__restrict__
     return v;
 }
 
+// constant coefficients: the cell's factors as NP2 double2 (the count padded to even), the pair
+// tensors interleaved in shared memory as S2[l nloc + j][k] (k padded to 2 NP2), so an entry is
+// 2 NP2 vector loads; the products are added in pair order, as in nnz_entry
+template <int NPAIR>
+struct NnzPairs {
+    static constexpr int NP2 = (NPAIR + 1) / 2, NPP = 2 * NP2;
+};
+
 template <int NLOC, int NPAIR>
-__device__ __forceinline__ double nnz_const(int code, const double (&f)[NPAIR], const double *sS)
+__device__ __forceinline__ double nnz_const(int code, const double2 (&f)[NnzPairs<NPAIR>::NP2], const double *sS2)
 {
-    constexpr int NL2 = NLOC * NLOC;
+    constexpr int NL2 = NLOC * NLOC, NP2 = NnzPairs<NPAIR>::NP2, NPP = NnzPairs<NPAIR>::NPP;
     const int lj = code % NL2;
+    const double2 *s2 = reinterpret_cast<const double2 *>(sS2 + lj * NPP);
     double v = 0.0;
 #pragma unroll
-    for (int k = 0; k < NPAIR; ++k) v += f[k] * sS[k * NL2 + lj];
+    for (int h = 0; h < NP2; ++h) {
+        const double2 sv = s2[h];
+        v += f[h].x * sv.x;
+        if (2 * h + 1 < NPAIR) v += f[h].y * sv.y;
+    }
     return v;
+}
+
+template <int NPAIR>
+__device__ __forceinline__ void nnz_factors(const double *factors, int nf, int code, int nl2, double2 (&f)[NnzPairs<NPAIR>::NP2])
+{
+    const double2 *F = reinterpret_cast<const double2 *>(factors + (size_t)(code < 0 ? 0 : code / nl2) * nf);
+#pragma unroll
+    for (int h = 0; h < NnzPairs<NPAIR>::NP2; ++h) f[h] = code >= 0 ? __ldg(&F[h]) : make_double2(0.0, 0.0);
 }
 
 template <int NLOC, int NPAIR, int U, bool VAR>
@@ -648,14 +670,20 @@ __global__ void __launch_bounds__(256, 2) k_assemble_nnz(const int *__restrict__
                                                          const double *__restrict__ g_S, const double *__restrict__ g_R,
                                                          FastSpec fs, double *__restrict__ data)
 {
-    extern __shared__ double smem[];
-    constexpr int NL2 = NLOC * NLOC;
+    extern __shared__ __align__(16) double smem[];
+    constexpr int NL2 = NLOC * NLOC, NP2 = NnzPairs<NPAIR>::NP2, NPP = NnzPairs<NPAIR>::NPP;
     double *sS = smem;
     double *sR = sS + (fs.has_const ? NPAIR * NL2 : 0);
-    if (fs.has_const)
-        for (int t = threadIdx.x; t < NPAIR * NL2; t += blockDim.x) sS[t] = g_S[t];
-    if (VAR)
+    if (VAR) {
+        if (fs.has_const)
+            for (int t = threadIdx.x; t < NPAIR * NL2; t += blockDim.x) sS[t] = g_S[t];
         for (int t = threadIdx.x; t < nq * 3 * NLOC; t += blockDim.x) sR[t] = g_R[t];
+    } else {
+        for (int t = threadIdx.x; t < NL2 * NPP; t += blockDim.x) {
+            const int lj = t / NPP, k = t - lj * NPP;
+            sS[t] = k < NPAIR ? g_S[k * NL2 + lj] : 0.0;
+        }
+    }
     __syncthreads();
     if (VAR) {
         for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x) {
@@ -681,16 +709,11 @@ __global__ void __launch_bounds__(256, 2) k_assemble_nnz(const int *__restrict__
             k0[u] = c0[u] < c1[u] ? __ldcs(&cent[c0[u]]) : -1;
             k1[u] = c0[u] + 1 < c1[u] ? __ldcs(&cent[c0[u] + 1]) : -1;
         }
-        double f0[U][NPAIR], f1[U][NPAIR];
+        double2 f0[U][NP2], f1[U][NP2];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const double *F0 = factors + (size_t)(k0[u] < 0 ? 0 : k0[u] / NL2) * nf;
-            const double *F1 = factors + (size_t)(k1[u] < 0 ? 0 : k1[u] / NL2) * nf;
-#pragma unroll
-            for (int k = 0; k < NPAIR; ++k) {
-                f0[u][k] = k0[u] >= 0 ? __ldg(&F0[k]) : 0.0;
-                f1[u][k] = k1[u] >= 0 ? __ldg(&F1[k]) : 0.0;
-            }
+            nnz_factors<NPAIR>(factors, nf, k0[u], NL2, f0[u]);
+            nnz_factors<NPAIR>(factors, nf, k1[u], NL2, f1[u]);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -700,10 +723,8 @@ __global__ void __launch_bounds__(256, 2) k_assemble_nnz(const int *__restrict__
             if (k1[u] >= 0) acc += nnz_const<NLOC, NPAIR>(k1[u], f1[u], sS);
             for (int c = c0[u] + 2; c < c1[u]; ++c) {
                 const int code = __ldcs(&cent[c]);
-                const double *F = factors + (size_t)(code / NL2) * nf;
-                double f[NPAIR];
-#pragma unroll
-                for (int k = 0; k < NPAIR; ++k) f[k] = __ldg(&F[k]);
+                double2 f[NP2];
+                nnz_factors<NPAIR>(factors, nf, code, NL2, f);
                 acc += nnz_const<NLOC, NPAIR>(code, f, sS);
             }
             if (p < nnz) data[p] = acc;
@@ -904,6 +925,9 @@ static void fast_spec(int nterms, const int *a, const int *b, const femd_coef *c
             ++fs.npair;
         }
     fs.nf = (fs.has_const ? fs.npair : 0) + (fs.has_var ? nq * fs.npair : 0);
+    // constant coefficients only: an even count per cell (one zero pad), so that a cell's factors
+    // start on a 16-byte boundary and load as double2
+    if (!fs.has_var && (fs.nf & 1)) fs.nf += 1;
 }
 
 static int check_common(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p, int nterms,
@@ -1008,7 +1032,7 @@ static int prepare_terms(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
 
 static constexpr int FAST_MAX_ROW = 96;   // longest row the shared-memory accumulator holds
 #ifndef FEMD_NNZ_U
-#define FEMD_NNZ_U 4
+#define FEMD_NNZ_U 2
 #endif
 static constexpr int NNZ_U = FEMD_NNZ_U;  // positions per thread in flight in k_assemble_nnz
 
@@ -1098,7 +1122,8 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
                            (FAST_BLOCK / 32) * 33 * sizeof(int) + (size_t)FAST_BLOCK * maxlen;
 #define FEMD_NNZ(NL, NP)                                                                                               \
         if (!done && nl == NL && fs.npair == NP && p->nnz > 0 && B_NNZ) {                                             \
-            const size_t shn = ((fs.has_const ? (size_t)NP * NL * NL : 0) + (fs.has_var ? nref : 0)) * sizeof(double); \
+            const size_t shn = (fs.has_var ? (fs.has_const ? (size_t)NP * NL * NL : 0) + nref                          \
+                                           : (size_t)NL * NL * NnzPairs<NP>::NPP) * sizeof(double);                    \
             const unsigned gq = (unsigned)ctx->sm_count * 64;                                                         \
             if (fs.has_var) {                                                                                          \
                 cudaFuncSetAttribute(k_assemble_nnz<NL, NP, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shn); \

@@ -173,6 +173,7 @@ def summarize(trace, elapsed):
                 solves_per_s=len(done) / elapsed if elapsed > 0 else 0.0,
                 p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
                 mean_iterations=float(np.mean([r.iterations for r in done])) if done else 0.0,
+                max_iterations=int(max([r.iterations for r in done])) if done else 0,
                 all_converged=all(r.converged for r in done))
 
 
