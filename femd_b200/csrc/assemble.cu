@@ -607,8 +607,11 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows_off(
 // The chain of loads per position (list bounds, then entry codes, then the cell's factors) is
 // latency-bound when a thread walks one position at a time, so with constant coefficients a
 // thread takes U positions of a tile (p = tile + u blockDim + tid, coalesced for every u) and
-// issues each level's loads for all of them, the first two entries of every position included
-// (most positions have one or two), before the next level; longer lists finish in a loop.
+// issues each level's loads for all of them, before the next level.  This pass adds the first two
+// entries of every position (most have one or two); the few positions with more (a vertex's
+// diagonal has one per cell around it) are listed once per pattern and finished by
+// k_assemble_nnz_long, which adds the rest to the stored value in the same cell order.  Left in
+// this pass, they would make almost every warp wait for their serial round trips.
 template <int NLOC, int NPAIR>
 __device__ __forceinline__ double nnz_entry(int code, const double *__restrict__ F, const double *sS, const double *sR,
                                             int nq, const FastSpec &fs)
@@ -721,15 +724,55 @@ __global__ void __launch_bounds__(256, 2) k_assemble_nnz(const int *__restrict__
             double acc = 0.0;
             if (k0[u] >= 0) acc += nnz_const<NLOC, NPAIR>(k0[u], f0[u], sS);
             if (k1[u] >= 0) acc += nnz_const<NLOC, NPAIR>(k1[u], f1[u], sS);
-            for (int c = c0[u] + 2; c < c1[u]; ++c) {
-                const int code = __ldcs(&cent[c]);
-                double2 f[NP2];
-                nnz_factors<NPAIR>(factors, nf, code, NL2, f);
-                acc += nnz_const<NLOC, NPAIR>(code, f, sS);
-            }
             if (p < nnz) data[p] = acc;
         }
     }
+}
+
+// the positions with more than two element entries: entries 2.. added to the stored sum of the
+// first two, in cell order; LU codes (and their factors) in flight per round
+template <int NLOC, int NPAIR>
+__global__ void __launch_bounds__(256) k_assemble_nnz_long(const int *__restrict__ lpos, int nlong, const int *__restrict__ cptr,
+                                                           const int *__restrict__ cent, const double *__restrict__ factors,
+                                                           const double *__restrict__ g_S, int nf, double *__restrict__ data)
+{
+    extern __shared__ __align__(16) double smem[];
+    constexpr int NL2 = NLOC * NLOC, NP2 = NnzPairs<NPAIR>::NP2, NPP = NnzPairs<NPAIR>::NPP, LU = 4;
+    double *sS = smem;
+    for (int t = threadIdx.x; t < NL2 * NPP; t += blockDim.x) {
+        const int lj = t / NPP, k = t - lj * NPP;
+        sS[t] = k < NPAIR ? g_S[k * NL2 + lj] : 0.0;
+    }
+    __syncthreads();
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nlong; t += gridDim.x * blockDim.x) {
+        const int p = lpos[t];
+        const int c1 = cptr[p + 1];
+        double acc = data[p];
+        for (int c = cptr[p] + 2; c < c1; c += LU) {
+            int code[LU];
+            double2 f[LU][NP2];
+#pragma unroll
+            for (int u = 0; u < LU; ++u) code[u] = c + u < c1 ? __ldcs(&cent[c + u]) : -1;
+#pragma unroll
+            for (int u = 0; u < LU; ++u) nnz_factors<NPAIR>(factors, nf, code[u], NL2, f[u]);
+#pragma unroll
+            for (int u = 0; u < LU; ++u)
+                if (code[u] >= 0) acc += nnz_const<NLOC, NPAIR>(code[u], f[u], sS);
+        }
+        data[p] = acc;
+    }
+}
+
+__global__ void k_long_flags(const int *__restrict__ cptr, long long nnz, int *__restrict__ flag)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x)
+        flag[p] = cptr[p + 1] - cptr[p] > 2 ? 1 : 0;
+}
+
+__global__ void k_long_fill(const int *__restrict__ flag, const int *__restrict__ idx, long long nnz, int *__restrict__ lpos)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x)
+        if (flag[p]) lpos[idx[p]] = (int)p;
 }
 
 // the inverse diagonal from the assembled values (JacobiPreconditioner, precond.hpp:82-102)
@@ -808,11 +851,25 @@ static int build_contrib(femd_ctx ctx, femd_pattern p)
     k_contrib_fill<<<g, 256, 0, counted(s)>>>(p->rc_ptr.p, p->rc_code.p, p->indptr.p, p->pair_off.p, n, p->nloc, offs, cnt.p,
                                                p->contrib.p);
     FEMD_TRY_CUDA(cudaGetLastError());
-    FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // cnt and tmp are released on return
+    // the positions with more than two entries, in increasing order (flags, scan, fill)
+    DevBuf<int> idx;
+    if ((st = idx.alloc((size_t)nnz + 1))) { p->contrib_ptr.release(); p->contrib.release(); return st; }
+    const unsigned gz = grid_for((size_t)std::max<long long>(nnz, 1), 256, 1u << 20);
+    k_long_flags<<<gz, 256, 0, counted(s)>>>(p->contrib_ptr.p, nnz, cnt.p);
+    FEMD_TRY_CUDA(cudaMemsetAsync(cnt.p + nnz, 0, sizeof(int), s));
+    FEMD_TRY(exclusive_scan_int(cnt.p, idx.p, (size_t)nnz + 1, tmp.p, s));
+    int nlong = 0;
+    FEMD_TRY_CUDA(cudaMemcpyAsync(&nlong, idx.p + nnz, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
+    if ((st = p->contrib_long.alloc((size_t)std::max(nlong, 1)))) { p->contrib_ptr.release(); p->contrib.release(); return st; }
+    p->n_long = nlong;
+    if (nlong) k_long_fill<<<gz, 256, 0, counted(s)>>>(cnt.p, idx.p, nnz, p->contrib_long.p);
+    FEMD_TRY_CUDA(cudaGetLastError());
+    FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // cnt, idx and tmp are released on return
     return FEMD_OK;
 }
 
-// The pair offsets: for rc index c (row i, cell entry code = cell nloc + l), byte j of// The pair offsets: for rc index c (row i, cell entry code = cell nloc + l), byte j of
+// The pair offsets: for rc index c (row i, cell entry code = cell nloc + l), byte j of
 // off[c * OFFS + j] = position of (i, dof(cell, j)) minus indptr[i], 255 where constrained.
 // OFFS = nloc rounded up to a multiple of 4, so a pair's offsets load as whole 32-bit words.
 __global__ void k_pair_offsets(const int *__restrict__ rc_ptr, const int *__restrict__ rc_code,
@@ -1134,6 +1191,13 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
                                      (int)shn);                                                                        \
                 k_assemble_nnz<NL, NP, NNZ_U, false><<<grid_for((size_t)p->nnz, 256 * NNZ_U, gq), 256, shn, counted(s)>>>( \
                     p->contrib_ptr.p, p->contrib.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs, K->data.p);            \
+                if (p->n_long) {                                                                                       \
+                    cudaFuncSetAttribute(k_assemble_nnz_long<NL, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                                         (int)shn);                                                                    \
+                    k_assemble_nnz_long<NL, NP><<<grid_for((size_t)p->n_long, 256, gq), 256, shn, counted(s)>>>(        \
+                        p->contrib_long.p, p->n_long, p->contrib_ptr.p, p->contrib.p, p->ws_factors.p, d_S, fs.nf,      \
+                        K->data.p);                                                                                    \
+                }                                                                                                      \
             }                                                                                                          \
             if (inv) k_asm_inv<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(p->diag_pos.p, K->data.p,   \
                                                                                             inv, n, ctx->status_dev);  \
@@ -1145,6 +1209,7 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
             // no room (or a row too long): the row kernels below
             p->contrib_ptr.release();
             p->contrib.release();
+            p->contrib_long.release();
             cudaGetLastError();
             clear_error();
         }
