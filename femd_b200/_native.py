@@ -114,6 +114,7 @@ SIGNATURES = {
     "femd_cuda_batch_advance_lockstep": (_I, [_P, _P, _I, _I, _PI, _PI, C.POINTER(femd_cg_result)]),
     "femd_cuda_batch_abort": (_I, [_P]),
     "femd_cuda_batch_lockstep_stats": (_I, [_P, C.POINTER(C.c_longlong)]),
+    "femd_cuda_pattern_batch_layout": (_I, [_P, _P, C.POINTER(C.c_int)]),
     "femd_cuda_batch_info": (_I, [_P, _PI, _PI, _PI, _PI]),
     "femd_cuda_batch_debug": (_I, [_P, _I, C.c_longlong]),
     "femd_cuda_batch_profile": (_I, [_P, C.POINTER(C.c_longlong)]),

@@ -303,6 +303,14 @@ class SparsityPattern(_Handle):
         check(lib.femd_cuda_pattern_arrays(self.h, C.byref(ip), C.byref(ix)))
         return ip.value, ix.value
 
+    def batch_layout(self):
+        """Build the batched engine's compact layout of this pattern now (else the first
+        mixed-precision lockstep solve on it does); returns the reordered bandwidth, -1 when the
+        pattern keeps the plain layout."""
+        bw = C.c_int()
+        check(lib.femd_cuda_pattern_batch_layout(self.ctx.h, self.h, C.byref(bw)))
+        return bw.value
+
     @staticmethod
     def from_arrays(nrows, ncols, indptr, indices, ctx=None):
         ctx = ctx or context()

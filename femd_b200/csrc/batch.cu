@@ -2943,6 +2943,17 @@ int femd_cuda_batch_tune(femd_ctx ctx, femd_batch handle, const double *const *b
     return FEMD_OK;
 }
 
+int femd_cuda_pattern_batch_layout(femd_ctx ctx, femd_pattern p, int *bandwidth)
+{
+    clear_error();
+    FEMD_CHECK_ARG(ctx && p && p->kind == KIND_PATTERN, "pattern_batch_layout: NULL argument or not a pattern");
+    FEMD_CHECK_ARG(p->nrows == p->ncols, "pattern_batch_layout: the pattern must be square");
+    FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    FEMD_TRY(build_compact(ctx, p));
+    if (bandwidth) *bandwidth = p->cl_state == 1 ? p->cl_bw : -1;
+    return FEMD_OK;
+}
+
 int femd_cuda_batch_lockstep_stats(femd_batch handle, long long *out)
 {
     clear_error();

@@ -52,6 +52,7 @@ class SpaceLibrary:
             m = fb.rectangle_mesh(0, 0, 1, 1, N, N)
             V = fb.LagrangeSpace2D(m, k, bc="dirichlet")
             P = V.pattern()
+            P.batch_layout()                        # the batched engine's layout, before any clock
             s = self.spaces[(N, k)] = dict(mesh=m, V=V, P=P, Qk=V.cache(fb.quad_degree("gradgrad", k)),
                                            Qm=V.cache(fb.quad_degree("mass", k)), n=V.dim, nnz=P.nnz)
         return s

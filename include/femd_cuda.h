@@ -428,6 +428,13 @@ FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry,
  * in the plain layout, [2] the widest shared-memory column window (columns), [3] table entries.
  * Instrumentation with no reference counterpart. */
 FEMD_API int femd_cuda_batch_lockstep_stats(femd_batch B, long long *out);
+/* Build (once per pattern) the lockstep engine's compact layout of a square pattern: the reverse
+ * Cuthill-McKee order, 16-bit column offsets, the column window of every 32-row tile.  Mixed-
+ * precision members on the pattern use it; without this call it is built by the first lockstep
+ * solve that meets the pattern (host work, seconds for millions of rows), so a server calls it
+ * while it sets its meshes up.  *bandwidth: the reordered bandwidth, -1 when over 32,767 (the
+ * pattern then keeps the plain layout).  No reference counterpart. */
+FEMD_API int femd_cuda_pattern_batch_layout(femd_ctx ctx, femd_pattern p, int *bandwidth);
 /* Add a member (a square matrix with its Jacobi inverse diagonal); *id_out its id (a free id is
  * reused).  Remove frees its solver vectors; a removed member's solve is dropped. */
 FEMD_API int femd_cuda_batch_add(femd_batch B, femd_matrix K, int *id_out);

@@ -127,3 +127,15 @@ def test_lockstep_unknown_engine_is_rejected(fb, problems):
     _, K, b = problems[0]
     with pytest.raises(ValueError):
         fb.Batch([K]).solve([b], engine="nope")
+
+
+def test_pattern_batch_layout(fb, problems):
+    """The compact layout built ahead of the first solve: its bandwidth (the same on a repeated
+    call, which builds nothing), and a rectangular pattern refused."""
+    _, K, _ = problems[-1]
+    P = K.pattern
+    bw = P.batch_layout()
+    assert 0 < bw < P.nrows and P.batch_layout() == bw
+    R = fb.SparsityPattern.from_arrays(2, 3, np.array([0, 1, 2]), np.array([0, 2]))
+    with pytest.raises(ValueError, match="square"):
+        R.batch_layout()
