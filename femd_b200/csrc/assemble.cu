@@ -608,10 +608,10 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows_off(
 // latency-bound when a thread walks one position at a time, so with constant coefficients a
 // thread takes U positions of a tile (p = tile + u blockDim + tid, coalesced for every u) and
 // issues each level's loads for all of them, before the next level.  This pass adds the first two
-// entries of every position (most have one or two); the few positions with more (a vertex's
-// diagonal has one per cell around it) are listed once per pattern and finished by
-// k_assemble_nnz_long, which adds the rest to the stored value in the same cell order.  Left in
-// this pass, they would make almost every warp wait for their serial round trips.
+// entries of every position (most have one or two), read as one int2 per position (pcode, -1
+// for none), so a position needs one load before its cells' factors; the few positions with more
+// (a vertex's diagonal has one per cell around it) are listed once per pattern and finished by
+// k_assemble_nnz_long, which adds the rest to the stored value in the same cell order.
 template <int NLOC, int NPAIR>
 __device__ __forceinline__ double nnz_entry(int code, const double *__restrict__ F, const double *sS, const double *sR,
                                             int nq, const FastSpec &fs)
@@ -669,6 +669,7 @@ __device__ __forceinline__ void nnz_factors(const double *factors, int nf, int c
 
 template <int NLOC, int NPAIR, int U, bool VAR>
 __global__ void __launch_bounds__(256, 2) k_assemble_nnz(const int *__restrict__ cptr, const int *__restrict__ cent,
+                                                         const int2 *__restrict__ pcode,
                                                          long long nnz, int nq, const double *__restrict__ factors,
                                                          const double *__restrict__ g_S, const double *__restrict__ g_R,
                                                          FastSpec fs, double *__restrict__ data)
@@ -698,32 +699,38 @@ __global__ void __launch_bounds__(256, 2) k_assemble_nnz(const int *__restrict__
         return;
     }
     const int nf = fs.nf;
-    const long long tile = (long long)U * blockDim.x;
-    for (long long base = (long long)blockIdx.x * tile; base < nnz; base += (long long)gridDim.x * tile) {
-        int c0[U], c1[U], k0[U], k1[U];
+    const long long tile = (long long)U * blockDim.x, stride = (long long)gridDim.x * tile;
+    // the codes of the next round are loaded before the current round's factors and sums, so the
+    // stream of codes waits on memory while the previous round computes
+    int2 nxt[U];
+    long long base = (long long)blockIdx.x * tile;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const long long p = base + u * (long long)blockDim.x + threadIdx.x;
+        nxt[u] = p < nnz ? __ldcs(&pcode[p]) : make_int2(-1, -1);
+    }
+    for (; base < nnz; base += stride) {
+        int2 cur[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) cur[u] = nxt[u];
+        const long long nb = base + stride;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const long long p = base + u * (long long)blockDim.x + threadIdx.x;
-            c0[u] = p < nnz ? __ldcs(&cptr[p]) : 0;
-            c1[u] = p < nnz ? __ldcs(&cptr[p + 1]) : 0;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            k0[u] = c0[u] < c1[u] ? __ldcs(&cent[c0[u]]) : -1;
-            k1[u] = c0[u] + 1 < c1[u] ? __ldcs(&cent[c0[u] + 1]) : -1;
+            const long long p = nb + u * (long long)blockDim.x + threadIdx.x;
+            nxt[u] = p < nnz ? __ldcs(&pcode[p]) : make_int2(-1, -1);
         }
         double2 f0[U][NP2], f1[U][NP2];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            nnz_factors<NPAIR>(factors, nf, k0[u], NL2, f0[u]);
-            nnz_factors<NPAIR>(factors, nf, k1[u], NL2, f1[u]);
+            nnz_factors<NPAIR>(factors, nf, cur[u].x, NL2, f0[u]);
+            nnz_factors<NPAIR>(factors, nf, cur[u].y, NL2, f1[u]);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const long long p = base + u * (long long)blockDim.x + threadIdx.x;
             double acc = 0.0;
-            if (k0[u] >= 0) acc += nnz_const<NLOC, NPAIR>(k0[u], f0[u], sS);
-            if (k1[u] >= 0) acc += nnz_const<NLOC, NPAIR>(k1[u], f1[u], sS);
+            if (cur[u].x >= 0) acc += nnz_const<NLOC, NPAIR>(cur[u].x, f0[u], sS);
+            if (cur[u].y >= 0) acc += nnz_const<NLOC, NPAIR>(cur[u].y, f1[u], sS);
             if (p < nnz) data[p] = acc;
         }
     }
@@ -760,6 +767,14 @@ __global__ void __launch_bounds__(256) k_assemble_nnz_long(const int *__restrict
                 if (code[u] >= 0) acc += nnz_const<NLOC, NPAIR>(code[u], f[u], sS);
         }
         data[p] = acc;
+    }
+}
+
+__global__ void k_pair_codes(const int *__restrict__ cptr, const int *__restrict__ cent, long long nnz, int2 *__restrict__ pcode)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x) {
+        const int c0 = cptr[p], c1 = cptr[p + 1];
+        pcode[p] = make_int2(c0 < c1 ? cent[c0] : -1, c0 + 1 < c1 ? cent[c0 + 1] : -1);
     }
 }
 
@@ -864,6 +879,11 @@ static int build_contrib(femd_ctx ctx, femd_pattern p)
     if ((st = p->contrib_long.alloc((size_t)std::max(nlong, 1)))) { p->contrib_ptr.release(); p->contrib.release(); return st; }
     p->n_long = nlong;
     if (nlong) k_long_fill<<<gz, 256, 0, counted(s)>>>(cnt.p, idx.p, nnz, p->contrib_long.p);
+    if ((st = p->contrib_pair.alloc((size_t)nnz + 1))) {
+        p->contrib_ptr.release(); p->contrib.release(); p->contrib_long.release();
+        return st;
+    }
+    k_pair_codes<<<gz, 256, 0, counted(s)>>>(p->contrib_ptr.p, p->contrib.p, nnz, p->contrib_pair.p);
     FEMD_TRY_CUDA(cudaGetLastError());
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // cnt, idx and tmp are released on return
     return FEMD_OK;
@@ -1185,12 +1205,14 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
             if (fs.has_var) {                                                                                          \
                 cudaFuncSetAttribute(k_assemble_nnz<NL, NP, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shn); \
                 k_assemble_nnz<NL, NP, 1, true><<<grid_for((size_t)p->nnz, 256, gq), 256, shn, counted(s)>>>(           \
-                    p->contrib_ptr.p, p->contrib.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs, K->data.p);            \
+                    p->contrib_ptr.p, p->contrib.p, p->contrib_pair.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs,     \
+                    K->data.p);                                                                                        \
             } else {                                                                                                   \
                 cudaFuncSetAttribute(k_assemble_nnz<NL, NP, NNZ_U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
                                      (int)shn);                                                                        \
                 k_assemble_nnz<NL, NP, NNZ_U, false><<<grid_for((size_t)p->nnz, 256 * NNZ_U, gq), 256, shn, counted(s)>>>( \
-                    p->contrib_ptr.p, p->contrib.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs, K->data.p);            \
+                    p->contrib_ptr.p, p->contrib.p, p->contrib_pair.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs,     \
+                    K->data.p);                                                                                        \
                 if (p->n_long) {                                                                                       \
                     cudaFuncSetAttribute(k_assemble_nnz_long<NL, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
                                          (int)shn);                                                                    \
@@ -1210,6 +1232,7 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
             p->contrib_ptr.release();
             p->contrib.release();
             p->contrib_long.release();
+            p->contrib_pair.release();
             cudaGetLastError();
             clear_error();
         }

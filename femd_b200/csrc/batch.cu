@@ -107,17 +107,6 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 
 __device__ __forceinline__ float pdir(const float *z, const float *p, float beta, int j) { return __fmaf_rn(beta, p[j], z[j]); }
 
-// an L2 prefetch (cp.async.bulk.prefetch) of the whole 16-byte granules inside [b, e), in 4 KB
-// pieces spread over the lanes of a warp: only addresses of the range are touched
-__device__ __forceinline__ void l2_prefetch_range(const void *b, const void *e, int lane)
-{
-    const unsigned long long lo = ((unsigned long long)b + 15ull) & ~15ull, hi = (unsigned long long)e & ~15ull;
-    constexpr unsigned long long CH = 4096;
-    for (unsigned long long c = lo + (unsigned long long)lane * CH; c < hi; c += 32 * CH) {
-        const unsigned n = (unsigned)(hi - c < CH ? hi - c : CH);
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c), "r"(n) : "memory");
-    }
-}
 __device__ __forceinline__ double pdir(const double *z, const double *p, double beta, int j) { return __fma_rn(beta, p[j], z[j]); }
 
 // team barrier: false when the batch has to stop (timeout or abort).  lead_sync: the block has
@@ -1110,13 +1099,6 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ 
         // compact layout: p over the entry's column window [w0, w1) into shared memory (the
         // owner's values to pnew), then the rows read it there
         const int c0 = L.w0, c1 = L.w1;
-        // the last warp first asks L2 for the entry's values and offsets, which stream in while
-        // the window is formed
-        if (threadIdx.x >= LS_BB - 32) {
-            const int q0 = P.cptr[L.r0], q1 = P.cptr[L.r1];
-            l2_prefetch_range(A + q0, A + q1, threadIdx.x & 31);
-            l2_prefetch_range(P.coff + q0, P.coff + q1, threadIdx.x & 31);
-        }
         // WU columns per thread and round, their loads issued before any store (the stores to
         // pnew could alias z and pold for the compiler, which would serialise the round trips)
         constexpr int WU = 4;

@@ -134,6 +134,7 @@ struct femd_pattern_s : femd::HandleBase {
     // (cell nloc^2 + l nloc + j) in increasing cell order (built on the first FAST assembly)
     femd::DevBuf<int> contrib_ptr, contrib;
     femd::DevBuf<int> contrib_long;    // the positions with more than two entries, increasing
+    femd::DevBuf<int2> contrib_pair;   // per position its first two entries (-1: none)
     int n_long = 0;
     // for every (row, cell) pair of the rc lists, the offsets within the row of the cell's nloc
     // columns (uint8, 255 = constrained): the scatter map in the rows' own order, a quarter of
