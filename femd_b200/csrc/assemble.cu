@@ -1109,7 +1109,7 @@ static int prepare_terms(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
 
 static constexpr int FAST_MAX_ROW = 96;   // longest row the shared-memory accumulator holds
 #ifndef FEMD_NNZ_U
-#define FEMD_NNZ_U 2
+#define FEMD_NNZ_U 1
 #endif
 static constexpr int NNZ_U = FEMD_NNZ_U;  // positions per thread in flight in k_assemble_nnz
 

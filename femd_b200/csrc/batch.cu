@@ -765,11 +765,14 @@ __global__ void k_batch_f32(const double *__restrict__ a, float *__restrict__ a3
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv32[i] = (float)inv[i];
 }
 
-// the inverse diagonal for the compact layout: original row i goes to reordered row iperm[i]
-// (the values go by f32_rowsum_copy, in row-sum form)
-__global__ void k_ls_inv32_perm(const double *__restrict__ inv, const int *__restrict__ iperm, float *__restrict__ inv32, int n)
+// the same for the compact layout: value q of the original CSR goes to position dst[q] of the
+// reordered one, the inverse diagonal of original row i to reordered row iperm[i]
+__global__ void k_ls_f32_perm(const double *__restrict__ a, const int *__restrict__ dst, float *__restrict__ a32,
+                              long long nnz, const double *__restrict__ inv, const int *__restrict__ iperm,
+                              float *__restrict__ inv32, int n)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += stride) a32[dst[q]] = (float)a[q];
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv32[iperm[i]] = (float)inv[i];
 }
 
@@ -900,8 +903,6 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
 // memory over the entry's column window [c0, ...): TPR lanes per row, U value / offset loads in
 // flight per lane, the products read p from shared memory (no gathers from global memory).  Each
 // lane adds its entries in increasing position and the row's lanes combine by a fixed shuffle tree.
-// The values are in row-sum form (f32_rowsum_copy): y_i = s_i p_i + sum_{j != i} a_ij (p_j - p_i),
-// s_i at the diagonal position (offset 0).
 template <int TPR>
 __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restrict__ A, const float *win, int c0, int r0,
                                           int r1, float *__restrict__ Ap, double &dot)
@@ -924,7 +925,6 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
             hi_n = P.cptr[inext + 1];
         }
         const float *wrow = win + (i - c0);
-        const float pi = i < r1 ? wrow[0] : 0.0f;
         float s = 0.0f;
         for (int base = lo + lane; base < hi; base += U * TPR) {
             short o[U];
@@ -937,7 +937,7 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
             }
 #pragma unroll
             for (int u = 0; u < U; ++u)
-                if (base + u * TPR < hi) s += v[u] * (o[u] ? wrow[o[u]] - pi : pi);
+                if (base + u * TPR < hi) s += v[u] * wrow[o[u]];
         }
 #pragma unroll
         for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
@@ -2039,7 +2039,7 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
     if (B->ls_windows && (st = ls_windows_of(B, M))) return st;
     E.clear();
     compact = false;
-    if (mx && B->ls_compact && !B->ls_windows && M.K->pattern->all_diag) {
+    if (mx && B->ls_compact && !B->ls_windows) {
         femd_pattern P = M.K->pattern;
         if ((st = build_compact(ctx, P))) return st;
         if (P->cl_state == 1) {
@@ -2091,11 +2091,10 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
     if (mx && (M.need_f32 || M.f32_compact != compact)) {
         cudaStream_t s = ctx->stream;
         const unsigned g = grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count);
-        if (compact) {
-            FEMD_TRY(f32_rowsum_copy(M.K->pattern, M.K->data.p, M.K->pattern->cl_dst.p, desc.A32, s));
-            k_ls_inv32_perm<<<grid_for((size_t)M.n, 256, 4 * (unsigned)ctx->sm_count), 256, 0, counted(s)>>>(
-                M.K->inv.p, M.K->pattern->cl_iperm.p, desc.inv32, M.n);
-        } else
+        if (compact)
+            k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, M.K->pattern->cl_dst.p, desc.A32, M.nnz, M.K->inv.p,
+                                                     M.K->pattern->cl_iperm.p, desc.inv32, M.n);
+        else
             k_batch_f32<<<g, 256, 0, counted(s)>>>(M.K->data.p, desc.A32, M.nnz, M.K->inv.p, desc.inv32, M.n);
         FEMD_TRY_CUDA(cudaGetLastError());
         M.need_f32 = false;
