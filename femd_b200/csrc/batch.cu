@@ -839,18 +839,13 @@ struct LState {
     double rz, alpha, beta, nb, maxr, rz_prev, rn_rec, prt, res;
     int it, done, want_ru, breakdown, conv, rus, stall, fallback, zero, started;
     unsigned t1, t2, t3;   // last-block tickets of the SpMV, the update and the residual
-    int stage_fail;        // a bulk copy of the compact SpMV did not land in time (FEMD_ETIMEOUT)
+    int pad;
 };
 
 struct LBlock {
     int m, r0, r1, b0, b1;  // member, its rows [r0, r1), the member's entries [b0, b1)
-    int w0, w1;             // its SpMV windows [w0, w1) (window mode), its column window (compact)
-    int qa, qn;             // compact layout: the nonzeros [qa, qa + qn) staged in shared memory
-                            // (qa and qn multiples of 8, covering the rows' nonzeros; qn 0: not staged)
+    int w0, w1;             // its SpMV windows [w0, w1) (window mode)
 };
-
-// the compact layout's staging: entries of about LS_STAGE_NNZ nonzeros, at most LS_STAGE_MAX staged
-static constexpr int LS_STAGE_NNZ = 8192, LS_STAGE_MAX = 12288;
 
 static constexpr int LS_BB = 256;
 
@@ -908,9 +903,9 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
 // memory over the entry's column window [c0, ...): TPR lanes per row, U value / offset loads in
 // flight per lane, the products read p from shared memory (no gathers from global memory).  Each
 // lane adds its entries in increasing position and the row's lanes combine by a fixed shuffle tree.
-template <int TPR, bool STAGED>
+template <int TPR>
 __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restrict__ A, const float *win, int c0, int r0,
-                                          int r1, float *__restrict__ Ap, double &dot, const float *sv, const short *so, int qa)
+                                          int r1, float *__restrict__ Ap, double &dot)
 {
     constexpr int U = 4, GPW = 32 / TPR, STEP = (LS_BB / 32) * GPW;
     const int lane = threadIdx.x % TPR;
@@ -937,13 +932,8 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int q = base + u * TPR;
-                if (STAGED) {
-                    o[u] = q < hi ? so[q - qa] : (short)0;
-                    v[u] = q < hi ? sv[q - qa] : 0.0f;
-                } else {
-                    o[u] = q < hi ? __ldcs(&P.coff[q]) : (short)0;
-                    v[u] = q < hi ? __ldcs(&A[q]) : 0.0f;
-                }
+                o[u] = q < hi ? __ldcs(&P.coff[q]) : (short)0;
+                v[u] = q < hi ? __ldcs(&A[q]) : 0.0f;
             }
 #pragma unroll
             for (int u = 0; u < U; ++u)
@@ -1085,10 +1075,10 @@ __device__ __forceinline__ void ls_finish(LState &S, int *active)
 // blocks per SM (with the loads issued ahead, 60 registers and 4 blocks ran 14 % slower).
 template <bool MIXED>
 __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
-                                                   LState *st, double *part, int *active, int *ru_count, int stage_cap)
+                                                   LState *st, double *part, int *active, int *ru_count)
 {
     using F = typename std::conditional<MIXED, float, double>::type;
-    extern __shared__ __align__(16) float ls_win[];
+    extern __shared__ float ls_win[];
     if (MIXED && blockIdx.x == 0 && threadIdx.x == 0) *ru_count = 0;
     const int e = blockIdx.x;
     const LBlock L = blks[e];
@@ -1107,27 +1097,7 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ 
     double dot = 0.0;
     if (MIXED && P.coff) {
         // compact layout: p over the entry's column window [w0, w1) into shared memory (the
-        // owner's values to pnew), then the rows read it there.  Dynamic shared memory: the staged
-        // values (stage_cap floats) and column offsets (stage_cap shorts), then the window.
-        __shared__ uint64_t cs_bar;
-        unsigned char *dyn = reinterpret_cast<unsigned char *>(ls_win);
-        float *sv = reinterpret_cast<float *>(dyn);
-        short *so = reinterpret_cast<short *>(dyn + (size_t)stage_cap * sizeof(float));
-        float *win = reinterpret_cast<float *>(dyn + (size_t)stage_cap * (sizeof(float) + sizeof(short)));
-        const bool staged = L.qn > 0;
-        if (staged && threadIdx.x == 0) {
-            // the entry's values and offsets by bulk copies (16-byte aligned: qa and qn are
-            // multiples of 8), landing while the window is formed
-            mbar_init(&cs_bar, 1);
-            fence_mbar_init();
-            mbar_arrive_tx(&cs_bar, (unsigned)L.qn * (unsigned)(sizeof(float) + sizeof(short)));
-            constexpr int PIECE = 4096;    // nonzeros per copy
-            for (int q = 0; q < L.qn; q += PIECE) {
-                const int n = min(PIECE, L.qn - q);
-                bulk_g2s(sv + q, (const float *)A + L.qa + q, (unsigned)n * sizeof(float), &cs_bar);
-                bulk_g2s(so + q, P.coff + L.qa + q, (unsigned)n * sizeof(short), &cs_bar);
-            }
-        }
+        // owner's values to pnew), then the rows read it there
         const int c0 = L.w0, c1 = L.w1;
         // WU columns per thread and round, their loads issued before any store (the stores to
         // pnew could alias z and pold for the compiler, which would serialise the round trips)
@@ -1148,34 +1118,19 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ 
                 const int w = w0 + u * LS_BB;
                 if (w < c1) {
                     const float pw = __fmaf_rn(bf, pv[u], zv[u]);
-                    win[w - c0] = pw;
+                    ls_win[w - c0] = pw;
                     if (w >= L.r0 && w < L.r1) pn[w] = pw;
                 }
             }
         }
         __syncthreads();
-        if (staged) {
-            // every thread waits for the copies itself (bounded); if any thread gave up, the
-            // block waits once more for the copies in flight, records the failure on the member
-            // (its solve ends with FEMD_ETIMEOUT) and skips the entry
-            const bool ok = mbar_wait(&cs_bar, 0);
-            if (__syncthreads_or(!ok)) {
-                if (!ok) mbar_wait(&cs_bar, 0);
-                if (threadIdx.x == 0 && atomicExch(&S.stage_fail, 1) == 0) ls_finish(S, active);
-                return;
-            }
-        }
-#define FEMD_LS_ROWS(T)                                                                                                  \
-    (staged ? ls_rows_c<T, true>(P, (const float *)A, win, c0, L.r0, L.r1, (float *)Ap, dot, sv, so, L.qa)               \
-            : ls_rows_c<T, false>(P, (const float *)A, win, c0, L.r0, L.r1, (float *)Ap, dot, sv, so, L.qa))
         switch (P.tpr) {
-        case 2: FEMD_LS_ROWS(2); break;
-        case 4: FEMD_LS_ROWS(4); break;
-        case 8: FEMD_LS_ROWS(8); break;
-        case 16: FEMD_LS_ROWS(16); break;
-        default: FEMD_LS_ROWS(32); break;
+        case 2: ls_rows_c<2>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        case 4: ls_rows_c<4>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        case 8: ls_rows_c<8>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        case 16: ls_rows_c<16>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
+        default: ls_rows_c<32>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
         }
-#undef FEMD_LS_ROWS
     } else {
         ls_spmv_entry<F, F>(
             P, A, L, [&](int j) { return pdir(z, pold, beta, j); }, [&](int i) { return pdir(z, pold, beta, i); },
@@ -1960,9 +1915,9 @@ static int ls_tpr(const Member &M)
 }
 
 // rows of one table entry of a member: about nnz_per_entry nonzeros
-static int ls_rows_per_entry(const femd_batch_s *B, const Member &M, int cap = INT_MAX)
+static int ls_rows_per_entry(const femd_batch_s *B, const Member &M)
 {
-    const long long r = (long long)std::min(B->ls_nnz, cap) * M.n / std::max(1LL, M.nnz);
+    const long long r = (long long)B->ls_nnz * M.n / std::max(1LL, M.nnz);
     return (int)std::max(32LL, std::min((long long)M.n, r));
 }
 
@@ -1996,8 +1951,6 @@ void rcm_order(int n, const std::vector<int> &ip, const std::vector<int> &ix, st
 
 static constexpr int CL_TILE = 32;          // rows per tile of the column-window bounds
 static constexpr int CL_WIN_MAX = 12288;    // largest column window of an entry (FP32: 48 KB of shared memory)
-// the compact SpMV's dynamic shared memory at most: the largest staged range and window
-static constexpr int LS_SPMV_SMEM_MAX = LS_STAGE_MAX * (int)(sizeof(float) + sizeof(short)) + CL_WIN_MAX * (int)sizeof(float);
 
 // Build the pattern's compact layout once (cl_state 1), or mark it unsuitable (-1).
 static int build_compact(femd_ctx ctx, femd_pattern P)
@@ -2045,7 +1998,7 @@ static int build_compact(femd_ctx ctx, femd_pattern P)
     }
     int st;
     if ((st = P->cl_iperm.alloc((size_t)n)) || (st = P->cl_indptr.alloc((size_t)n + 1)) ||
-        (st = P->cl_dst.alloc((size_t)std::max<long long>(nnz, 1))) || (st = P->cl_off.alloc((size_t)nnz + 8)))
+        (st = P->cl_dst.alloc((size_t)std::max<long long>(nnz, 1))) || (st = P->cl_off.alloc((size_t)std::max<long long>(nnz, 1))))
         return st;
     FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_iperm.p, iperm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
     FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_indptr.p, cptr.data(), ((size_t)n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -2056,7 +2009,6 @@ static int build_compact(femd_ctx ctx, femd_pattern P)
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // the host vectors are released on return
     P->cl_tile_lo.swap(tlo);
     P->cl_tile_hi.swap(thi);
-    P->cl_indptr_host.swap(cptr);
     P->cl_state = 1;
     return FEMD_OK;
 }
@@ -2073,10 +2025,9 @@ struct PinnedBuf {
 
 // One lockstep solve of the members `ids` (armed, one precision).  The final states go to out.
 // One member's part of a lockstep launch: its descriptor (FP32 compact, FP32 plain or FP64 layout)
-// and its table entries (r0, r1, w0, w1, qa, qn); maxwin grows to its widest shared-memory window
-// and maxstage to its largest staged nonzero range.
-static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb &desc, std::vector<std::array<int, 6>> &E,
-                           bool &compact, int &maxwin, int &maxstage)
+// and its table entries (r0, r1, w0, w1); maxwin grows to its widest shared-memory window.
+static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb &desc, std::vector<std::array<int, 4>> &E,
+                           bool &compact, int &maxwin)
 {
     int st;
     Member &M = *B->mem[id];
@@ -2094,10 +2045,10 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
         if (P->cl_state == 1) {
             // rows per entry: a multiple of the tile near nnz_per_entry nonzeros, halved while
             // some entry's column window is wider than the shared-memory window
-            int R = std::max(CL_TILE, ls_rows_per_entry(B, M, LS_STAGE_NNZ) / CL_TILE * CL_TILE);
+            int R = std::max(CL_TILE, ls_rows_per_entry(B, M) / CL_TILE * CL_TILE);
             while (!compact) {
                 E.clear();
-                int wmax = 0, smax = 0;
+                int wmax = 0;
                 for (int r = 0; r < M.n; r += R) {
                     const int r1 = std::min(M.n, r + R);
                     int lo = INT_MAX, hi = INT_MIN;
@@ -2105,18 +2056,12 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
                         lo = std::min(lo, P->cl_tile_lo[t]);
                         hi = std::max(hi, P->cl_tile_hi[t]);
                     }
-                    // the staged nonzeros: the rows' range rounded out to multiples of 8 (the
-                    // arrays have room for the rounding); entries over LS_STAGE_MAX stay unstaged
-                    const int qa = P->cl_indptr_host[r] & ~7, qb = (P->cl_indptr_host[r1] + 7) & ~7;
-                    const int qn = qb - qa <= LS_STAGE_MAX ? qb - qa : 0;
-                    E.push_back({r, r1, lo, hi + 1, qa, qn});
+                    E.push_back({r, r1, lo, hi + 1});
                     wmax = std::max(wmax, hi + 1 - lo);
-                    smax = std::max(smax, qn);
                 }
                 if (wmax <= CL_WIN_MAX) {
                     compact = true;
                     maxwin = std::max(maxwin, wmax);
-                    maxstage = std::max(maxstage, smax);
                 } else if (R > CL_TILE) {
                     R = std::max(CL_TILE, R / 2 / CL_TILE * CL_TILE);
                 } else {
@@ -2137,11 +2082,11 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
         const int G = std::max(1, B->ls_nnz / LS_W);
         for (int w = 0; w < nw; w += G) {
             const int w1 = std::min(nw, w + G);
-            E.push_back({M.ls_wrow[w], M.ls_wrow[w1], w, w1, 0, 0});
+            E.push_back({M.ls_wrow[w], M.ls_wrow[w1], w, w1});
         }
     } else {
         const int R = ls_rows_per_entry(B, M);
-        for (int r = 0; r < M.n; r += R) E.push_back({r, std::min(M.n, r + R), 0, 0, 0, 0});
+        for (int r = 0; r < M.n; r += R) E.push_back({r, std::min(M.n, r + R), 0, 0});
     }
     if (mx && (M.need_f32 || M.f32_compact != compact)) {
         cudaStream_t s = ctx->stream;
@@ -2169,16 +2114,15 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     for (int id : ids)
         if ((st = member_vectors(B, *B->mem[id], mx))) return st;
     std::vector<BProb> desc(nm);
-    std::vector<std::vector<std::array<int, 6>>> ents(nm);   // per member: r0, r1, w0, w1 of its entries
+    std::vector<std::vector<std::array<int, 4>>> ents(nm);   // per member: r0, r1, w0, w1 of its entries
     std::vector<int> nent(nm);
     int NEfull = 0, max_it = 1;
     int maxwin = 0;                                     // the widest column window of a compact entry
-    int maxstage = 0;                                   // the largest staged range of a compact entry
     for (int k = 0; k < nm; ++k) {
         Member &M = *B->mem[ids[k]];
         auto &E = ents[k];
         bool compact = false;
-        if ((st = ls_member_setup(ctx, B, ids[k], mx, desc[k], E, compact, maxwin, maxstage))) return st;
+        if ((st = ls_member_setup(ctx, B, ids[k], mx, desc[k], E, compact, maxwin))) return st;
         nent[k] = (int)E.size();
         FEMD_CHECK_ARG((long long)NEfull + nent[k] < INT_MAX / 4, "batch: too many table entries");
         NEfull += nent[k];
@@ -2215,7 +2159,7 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
         for (int k = 0; k < nm; ++k) {
             if (live && live[k].done) continue;
             const int b0 = e;
-            for (const auto &x : ents[k]) T[e++] = LBlock{k, x[0], x[1], b0, b0 + nent[k], x[2], x[3], x[4], x[5]};
+            for (const auto &x : ents[k]) T[e++] = LBlock{k, x[0], x[1], b0, b0 + nent[k], x[2], x[3]};
         }
         return e;
     };
@@ -2253,23 +2197,22 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     else
         k_ls_resid<false, 0><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
     FEMD_TRY_CUDA(cudaGetLastError());
-    // the SpMV's shared memory: the staged values and offsets, then the window
-    const size_t win_b = (size_t)maxstage * (sizeof(float) + sizeof(short)) + (size_t)maxwin * sizeof(float);
-    if (mx) FEMD_TRY_CUDA(cudaFuncSetAttribute(k_ls_spmv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, LS_SPMV_SMEM_MAX));
+    const size_t win_b = (size_t)maxwin * sizeof(float);   // the SpMV's shared-memory window
+    if (mx) FEMD_TRY_CUDA(cudaFuncSetAttribute(k_ls_spmv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)(CL_WIN_MAX * sizeof(float))));
     const int C = std::max(1, B->ls_chunk);
     const long long max_chunks = (long long)max_it / C + 4;
     int aborted = 0;
     for (long long j = 0; j <= max_chunks; ++j) {
         for (int c = 0; c < C; ++c) {
             if (mx) {
-                k_ls_spmv<true><<<NE, LS_BB, win_b, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count,
-                                                                  maxstage);
+                k_ls_spmv<true><<<NE, LS_BB, win_b, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count);
                 k_ls_update<true><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list, ru_count);
                 k_ls_flush<false><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, ru_list, ru_count);
                 k_ls_resid<true, 1><<<std::min(G1, NE), LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active,
                                                                                  ru_list, ru_count);
             } else {
-                k_ls_spmv<false><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count, 0);
+                k_ls_spmv<false><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_count);
                 k_ls_update<false><<<NE, LS_BB, 0, counted(s)>>>(d_desc.p, d_tab.p, NE, d_state.p, d_part.p, active, ru_list,
                                                                    ru_count);
             }
@@ -2326,9 +2269,9 @@ static void ls_result(const Member &M, const LState &S, femd_cg_result &r, doubl
     r.outer = S.rus + M.prior_rus;
     r.residual = S.res;
     r.breakdown = S.breakdown;
-    r.status = S.stage_fail ? FEMD_ETIMEOUT : 0;
+    r.status = 0;
     r.seconds = seconds;
-    int conv = S.stage_fail ? 0 : S.conv;
+    int conv = S.conv;
     if (!conv && !S.breakdown && S.done) {
         conv = S.res <= M.tol * (1.0 + 1e-6) + 1e-15;
         if (!conv && S.res <= 10.0 * M.tol && S.it < M.max_iter) conv = 1;
@@ -2381,8 +2324,8 @@ static int ls_solve(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, 
 struct LsLive {
     std::vector<int> ids;                                  // members in flight, in admission order
     std::vector<char> in, f64, started;                    // per member id
-    std::vector<std::vector<std::array<int, 6>>> ents;     // per member id: its entries
-    int maxwin = 0, maxstage = 0;
+    std::vector<std::vector<std::array<int, 4>>> ents;     // per member id: its entries
+    int maxwin = 0;
     int cap = 0;
     size_t tab_cap = 0;
     DevBuf<BProb> d_desc;
@@ -2400,7 +2343,6 @@ struct LsLive {
     const BProb *g_desc = nullptr;
     const LState *g_state = nullptr;
     size_t g_win = 0;
-    int g_stage = -1;
     bool g_refused = false;
     ~LsLive()
     {
@@ -2461,7 +2403,7 @@ static int live_table(const LsLive &L, const std::vector<int> &sel, LBlock *T)
     int e = 0;
     for (int id : sel) {
         const int b0 = e, b1 = b0 + (int)L.ents[id].size();
-        for (const auto &x : L.ents[id]) T[e++] = LBlock{id, x[0], x[1], b0, b1, x[2], x[3], x[4], x[5]};
+        for (const auto &x : L.ents[id]) T[e++] = LBlock{id, x[0], x[1], b0, b1, x[2], x[3]};
     }
     return e;
 }
@@ -2486,7 +2428,7 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
         if ((st = member_vectors(B, M, m32))) return st;
         BProb d{};
         bool compact = false;
-        if ((st = ls_member_setup(ctx, B, id, m32, d, L.ents[id], compact, L.maxwin, L.maxstage))) return st;
+        if ((st = ls_member_setup(ctx, B, id, m32, d, L.ents[id], compact, L.maxwin))) return st;
         BProb *h = reinterpret_cast<BProb *>(L.pin);
         *h = d;
         FEMD_TRY_CUDA(cudaMemcpyAsync(L.d_desc.p + id, h, sizeof(BProb), cudaMemcpyHostToDevice, s));
@@ -2505,9 +2447,9 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
     LBlock *ht = reinterpret_cast<LBlock *>(hs + 2 * (size_t)L.cap);
     int *active = L.d_int.p, *ru_count = L.d_int.p + 1, *ru_list = L.d_int.p + 2;
     const int G1 = std::max(1, 8 * ctx->sm_count);
-    const int stage_cap = L.maxstage;
-    const size_t win_b = (size_t)stage_cap * (sizeof(float) + sizeof(short)) + (size_t)L.maxwin * sizeof(float);
-    FEMD_TRY_CUDA(cudaFuncSetAttribute(k_ls_spmv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, LS_SPMV_SMEM_MAX));
+    const size_t win_b = (size_t)L.maxwin * sizeof(float);
+    FEMD_TRY_CUDA(cudaFuncSetAttribute(k_ls_spmv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(CL_WIN_MAX * sizeof(float))));
     FEMD_TRY_CUDA(cudaMemsetAsync(L.d_int.p, 0, 2 * sizeof(int), s));
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     FEMD_TRY_CUDA(cudaEventCreate(&t0));
@@ -2561,7 +2503,7 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
         for (int c = 0; c < C; ++c) {
             if (NE32) {
                 k_ls_spmv<true><<<NE32, LS_BB, win_b, counted(s)>>>(L.d_desc.p, T32, NE32, L.d_state.p, L.d_part.p, active,
-                                                                   ru_count, stage_cap);
+                                                                   ru_count);
                 k_ls_update<true><<<NE32, LS_BB, 0, counted(s)>>>(L.d_desc.p, T32, NE32, L.d_state.p, L.d_part.p, active, ru_list,
                                                                  ru_count);
                 k_ls_flush<false><<<std::min(G1, NE32), LS_BB, 0, counted(s)>>>(L.d_desc.p, T32, NE32, L.d_state.p, ru_list,
@@ -2570,8 +2512,7 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
                                                                                   active, ru_list, ru_count);
             }
             if (NE64) {
-                k_ls_spmv<false><<<NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, T64, NE64, L.d_state.p, L.d_part.p, active, ru_count,
-                                                                 0);
+                k_ls_spmv<false><<<NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, T64, NE64, L.d_state.p, L.d_part.p, active, ru_count);
                 k_ls_update<false><<<NE64, LS_BB, 0, counted(s)>>>(L.d_desc.p, T64, NE64, L.d_state.p, L.d_part.p, active, ru_list,
                                                                   ru_count);
             }
@@ -2581,7 +2522,7 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
     // the table from device memory, so a table of the same shape reuses the graph)
     auto launch_chunk = [&](int NE32, int NE64) -> cudaError_t {
         const bool same = L.gx && L.g_ne32 == NE32 && L.g_ne64 == NE64 && L.g_tab == L.d_tab.p && L.g_desc == L.d_desc.p &&
-                          L.g_state == L.d_state.p && L.g_win == win_b && L.g_stage == stage_cap && L.g_chunk == C;
+                          L.g_state == L.d_state.p && L.g_win == win_b && L.g_chunk == C;
         if (!same && !L.g_refused) {
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
@@ -2613,7 +2554,6 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
                 L.g_desc = L.d_desc.p;
                 L.g_state = L.d_state.p;
                 L.g_win = win_b;
-                L.g_stage = stage_cap;
                 L.g_chunk = C;
             }
         }

@@ -147,9 +147,8 @@ struct femd_pattern_s : femd::HandleBase {
     // largest column.  cl_state: 0 not built, 1 built, -1 unsuitable (a column offset over 32767)
     int cl_state = 0, cl_bw = 0;
     femd::DevBuf<int> cl_iperm, cl_indptr, cl_dst;
-    femd::DevBuf<short> cl_off;        // nnz + 8 (a bulk copy rounds its range out to 8 entries)
+    femd::DevBuf<short> cl_off;
     std::vector<int> cl_tile_lo, cl_tile_hi;
-    std::vector<int> cl_indptr_host;   // the reordered rows' pointers, on the host
     femd_pattern_s() : HandleBase(femd::KIND_PATTERN) {}
     ~femd_pattern_s() override { femd::ctx_release(ctx); }
 };
