@@ -36,6 +36,7 @@ def main():
     ap.add_argument("--kmin", type=int, default=2)
     ap.add_argument("--iters", type=int, default=100)
     ap.add_argument("--mixed", action="store_true")
+    ap.add_argument("--nnz-per-entry", type=int, default=0, help="lockstep: nonzeros per table entry (0: the default)")
     a = ap.parse_args()
     if a.kernel in ("batch", "lockstep"):
         return batch(a)
@@ -91,6 +92,8 @@ def batch(a):
     cache = W.SpaceCache()
     probs = [W.build_poisson(s, cache) for s in spec]
     B = fb.Batch([K for K, _ in probs])
+    if a.nnz_per_entry:
+        B.configure_lockstep(nnz_per_entry=a.nnz_per_entry)
     bs = [b for _, b in probs]
     engine = "lockstep" if a.kernel == "lockstep" else "persistent"
     for _ in range(a.reps):
