@@ -903,6 +903,21 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
 // memory over the entry's column window [c0, ...): TPR lanes per row, U value / offset loads in
 // flight per lane, the products read p from shared memory (no gathers from global memory).  Each
 // lane adds its entries in increasing position and the row's lanes combine by a fixed shuffle tree.
+// The loop is pipelined: a row group's first round of values and offsets is loaded while the
+// previous group is summed (its row pointers two groups ahead), so a warp keeps two rounds of
+// the matrix stream in flight.
+template <int U, int TPR>
+__device__ __forceinline__ void ls_round_c(const BProb &P, const float *__restrict__ A, int base, int hi, short (&o)[U],
+                                           float (&v)[U])
+{
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int q = base + u * TPR;
+        o[u] = q < hi ? __ldcs(&P.coff[q]) : (short)0;
+        v[u] = q < hi ? __ldcs(&A[q]) : 0.0f;
+    }
+}
+
 template <int TPR>
 __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restrict__ A, const float *win, int c0, int r0,
                                           int r1, float *__restrict__ Ap, double &dot)
@@ -912,42 +927,56 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
     const int sub = (int)(threadIdx.x & 31) / TPR;
     int i0 = r0 + (int)(threadIdx.x >> 5) * GPW;
     int i = i0 + sub;
-    int lo = 0, hi = 0;
+    int lo = 0, hi = 0, lo_n = 0, hi_n = 0;
     if (i < r1) {
         lo = P.cptr[i];
         hi = P.cptr[i + 1];
     }
+    if (i + STEP < r1) {
+        lo_n = P.cptr[i + STEP];
+        hi_n = P.cptr[i + STEP + 1];
+    }
+    short o[U];
+    float v[U];
+    ls_round_c<U, TPR>(P, A, lo + lane, hi, o, v);
     for (; i0 < r1; i0 += STEP) {
-        const int inext = i + STEP;
-        int lo_n = 0, hi_n = 0;
-        if (inext < r1) {
-            lo_n = P.cptr[inext];
-            hi_n = P.cptr[inext + 1];
+        const int i2 = i + 2 * STEP;
+        int lo_2 = 0, hi_2 = 0;
+        if (i2 < r1) {
+            lo_2 = P.cptr[i2];
+            hi_2 = P.cptr[i2 + 1];
         }
+        short on[U];
+        float vn[U];
+        ls_round_c<U, TPR>(P, A, lo_n + lane, hi_n, on, vn);
         const float *wrow = win + (i - c0);
         float s = 0.0f;
-        for (int base = lo + lane; base < hi; base += U * TPR) {
-            short o[U];
-            float v[U];
+        int base = lo + lane;
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int q = base + u * TPR;
-                o[u] = q < hi ? __ldcs(&P.coff[q]) : (short)0;
-                v[u] = q < hi ? __ldcs(&A[q]) : 0.0f;
-            }
+        for (int u = 0; u < U; ++u)
+            if (base + u * TPR < hi) s += v[u] * wrow[o[u]];
+        for (base += U * TPR; base < hi; base += U * TPR) {
+            ls_round_c<U, TPR>(P, A, base, hi, o, v);
 #pragma unroll
             for (int u = 0; u < U; ++u)
                 if (base + u * TPR < hi) s += v[u] * wrow[o[u]];
         }
 #pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, TPR);
+        for (int k = TPR / 2; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k, TPR);
         if (lane == 0 && i < r1) {
             Ap[i] = s;
             dot += (double)wrow[0] * (double)s;
         }
-        i = inext;
+        i += STEP;
         lo = lo_n;
         hi = hi_n;
+        lo_n = lo_2;
+        hi_n = hi_2;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            o[u] = on[u];
+            v[u] = vn[u];
+        }
     }
 }
 
