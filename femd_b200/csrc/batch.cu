@@ -82,8 +82,6 @@ struct BProb {
     // to its reordered one, cptr / coff are the reordered rows' pointers and 16-bit column offsets
     const int *iperm, *cptr;
     const short *coff;
-    // the low part of the split diagonal (compact layout, one per reordered row; null: none)
-    const float *dlo;
 };
 
 struct BQueue {
@@ -778,28 +776,6 @@ __global__ void k_ls_f32_perm(const double *__restrict__ a, const int *__restric
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv32[iperm[i]] = (float)inv[i];
 }
 
-// the compact layout's diagonal, split so that the FP32 matrix keeps the FP64 row sums: with the
-// off-diagonals rounded to FP32, d = a_ii + sum_{j != i} (a_ij - fl(a_ij)) (FP64) is stored as
-// hi = fl(d) at the diagonal position and lo = fl(d - hi) per row, and the SpMV adds lo p_i to the
-// FP32 row sum.  The represented matrix is then a graph Laplacian of the rounded off-diagonals
-// plus the exact row sums (to about eps_32^2), whose quadratic form is within O(eps_32) of the
-// FP64 one instead of O(eps_32 cond(A)); the FP32 recurrence needs fewer iterations.  One thread
-// per original row i (after k_ls_f32_perm wrote the entries).
-__global__ void k_ls_split_diag(const int *__restrict__ indptr, const int *__restrict__ diag_pos, const double *__restrict__ a,
-                                const int *__restrict__ dst, const int *__restrict__ iperm, float *__restrict__ a32,
-                                float *__restrict__ dlo, int n)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int lo = indptr[i], hi = indptr[i + 1], dp = diag_pos[i];
-        double d = a[dp];
-        for (int q = lo; q < hi; ++q)
-            if (q != dp) d += a[q] - (double)(float)a[q];
-        const float h = (float)d;
-        a32[dst[dp]] = h;
-        dlo[iperm[i]] = (float)(d - (double)h);
-    }
-}
-
 // chunk tables of one matrix: chunk k starts at the first row whose first nonzero is at or after
 // k * cp (cp = chunk capacity - longest row), so no chunk holds more than the capacity
 __global__ void k_chunk_table(const int *__restrict__ indptr, int n, int nnz, int cp, int nch, int *crow, int *cq)
@@ -929,8 +905,7 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
 // lane adds its entries in increasing position and the row's lanes combine by a fixed shuffle tree.
 // The loop is pipelined: a row group's first round of values and offsets is loaded while the
 // previous group is summed (its row pointers two groups ahead), so a warp keeps two rounds of
-// the matrix stream in flight.  With a split diagonal (dlo) the row's low part times p_i is added
-// to the FP32 row sum.
+// the matrix stream in flight.
 template <int U, int TPR>
 __device__ __forceinline__ void ls_round_c(const BProb &P, const float *__restrict__ A, int base, int hi, short (&o)[U],
                                            float (&v)[U])
@@ -964,8 +939,6 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
     short o[U];
     float v[U];
     ls_round_c<U, TPR>(P, A, lo + lane, hi, o, v);
-    const bool split = P.dlo != nullptr;
-    float dl = split && lane == 0 && i < r1 ? P.dlo[i] : 0.0f;
     for (; i0 < r1; i0 += STEP) {
         const int i2 = i + 2 * STEP;
         int lo_2 = 0, hi_2 = 0;
@@ -976,7 +949,6 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
         short on[U];
         float vn[U];
         ls_round_c<U, TPR>(P, A, lo_n + lane, hi_n, on, vn);
-        const float dln = split && lane == 0 && i + STEP < r1 ? P.dlo[i + STEP] : 0.0f;
         const float *wrow = win + (i - c0);
         float s = 0.0f;
         int base = lo + lane;
@@ -992,11 +964,9 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
 #pragma unroll
         for (int k = TPR / 2; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k, TPR);
         if (lane == 0 && i < r1) {
-            if (split) s = __fmaf_rn(dl, wrow[0], s);   // the low part of the split diagonal
             Ap[i] = s;
             dot += (double)wrow[0] * (double)s;
         }
-        dl = dln;
         i += STEP;
         lo = lo_n;
         hi = hi_n;
@@ -1665,7 +1635,7 @@ static int member_vectors(femd_batch_s *B, Member &M, bool mixed)
     cudaStream_t s = B->ctx->stream;
     const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
     if (mixed && !M.f32) {
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 8 * n + 32) * sizeof(float), s);
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 7 * n + 32) * sizeof(float), s);
         if (e != cudaSuccess) { M.f32 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
         if (reinterpret_cast<uintptr_t>(M.f32) & 15) {
             // the FP32 values are read by 16-byte bulk copies
@@ -1709,8 +1679,7 @@ static BProb describe(femd_batch_s *B, int id, bool mixed)
         P.pa32 = f; f += n;
         P.pb32 = f; f += n;
         P.Ap32 = f; f += n;
-        P.d32 = f; f += n;
-        P.dlo = nullptr;       // set by the compact layout's setup (the region follows d32)
+        P.d32 = f;
     } else {
         double *d = M.f64;
         P.r64 = d; d += n;
@@ -2136,7 +2105,6 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
         desc.iperm = P->cl_iperm.p;
         desc.cptr = P->cl_indptr.p;
         desc.coff = P->cl_off.p;
-        if (P->all_diag) desc.dlo = desc.d32 + M.n;   // the split diagonal (k_ls_split_diag)
     } else if (B->ls_windows && !M.ls_wrow.empty()) {
         desc.wrow = M.ls_tab.p;
         const int nw = (int)M.ls_wrow.size() - 1;
@@ -2152,14 +2120,10 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
     if (mx && (M.need_f32 || M.f32_compact != compact)) {
         cudaStream_t s = ctx->stream;
         const unsigned g = grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count);
-        if (compact) {
+        if (compact)
             k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, M.K->pattern->cl_dst.p, desc.A32, M.nnz, M.K->inv.p,
                                                      M.K->pattern->cl_iperm.p, desc.inv32, M.n);
-            if (desc.dlo)
-                k_ls_split_diag<<<grid_for((size_t)M.n, 128, 1u << 20), 128, 0, counted(s)>>>(
-                    M.K->pattern->indptr.p, M.K->pattern->diag_pos.p, M.K->data.p, M.K->pattern->cl_dst.p,
-                    M.K->pattern->cl_iperm.p, desc.A32, const_cast<float *>(desc.dlo), M.n);
-        } else
+        else
             k_batch_f32<<<g, 256, 0, counted(s)>>>(M.K->data.p, desc.A32, M.nnz, M.K->inv.p, desc.inv32, M.n);
         FEMD_TRY_CUDA(cudaGetLastError());
         M.need_f32 = false;
