@@ -900,41 +900,66 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
 }
 
 // y = A p on reordered rows [r0, r1) of the compact layout, the direction p staged in shared
-// memory over the entry's column window [c0, ...): TPR lanes per row, each lane reading 4
-// consecutive values and 16-bit offsets per load (rows are padded to multiples of 4 with zero
-// values at offset 0), the products reading p from shared memory (no gathers from global memory).
-// Each lane adds its entries in increasing position and the row's lanes combine by a fixed
-// shuffle tree.  The row pointers of the next row group are loaded one group ahead.
+// memory over the entry's column window [c0, ...): TPR lanes per row, U value / offset loads in
+// flight per lane, the products read p from shared memory (no gathers from global memory).  Each
+// lane adds its entries in increasing position and the row's lanes combine by a fixed shuffle tree.
+// The loop is pipelined: a row group's first round of values and offsets is loaded while the
+// previous group is summed (its row pointers two groups ahead), so a warp keeps two rounds of
+// the matrix stream in flight.
+template <int U, int TPR>
+__device__ __forceinline__ void ls_round_c(const BProb &P, const float *__restrict__ A, int base, int hi, short (&o)[U],
+                                           float (&v)[U])
+{
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int q = base + u * TPR;
+        o[u] = q < hi ? __ldcs(&P.coff[q]) : (short)0;
+        v[u] = q < hi ? __ldcs(&A[q]) : 0.0f;
+    }
+}
+
 template <int TPR>
 __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restrict__ A, const float *win, int c0, int r0,
                                           int r1, float *__restrict__ Ap, double &dot)
 {
-    constexpr int GPW = 32 / TPR, STEP = (LS_BB / 32) * GPW;
+    constexpr int U = 4, GPW = 32 / TPR, STEP = (LS_BB / 32) * GPW;
     const int lane = threadIdx.x % TPR;
     const int sub = (int)(threadIdx.x & 31) / TPR;
     int i0 = r0 + (int)(threadIdx.x >> 5) * GPW;
     int i = i0 + sub;
-    int lo = 0, hi = 0;
+    int lo = 0, hi = 0, lo_n = 0, hi_n = 0;
     if (i < r1) {
         lo = P.cptr[i];
         hi = P.cptr[i + 1];
     }
+    if (i + STEP < r1) {
+        lo_n = P.cptr[i + STEP];
+        hi_n = P.cptr[i + STEP + 1];
+    }
+    short o[U];
+    float v[U];
+    ls_round_c<U, TPR>(P, A, lo + lane, hi, o, v);
     for (; i0 < r1; i0 += STEP) {
-        const int inext = i + STEP;
-        int lo_n = 0, hi_n = 0;
-        if (inext < r1) {
-            lo_n = P.cptr[inext];
-            hi_n = P.cptr[inext + 1];
+        const int i2 = i + 2 * STEP;
+        int lo_2 = 0, hi_2 = 0;
+        if (i2 < r1) {
+            lo_2 = P.cptr[i2];
+            hi_2 = P.cptr[i2 + 1];
         }
+        short on[U];
+        float vn[U];
+        ls_round_c<U, TPR>(P, A, lo_n + lane, hi_n, on, vn);
         const float *wrow = win + (i - c0);
         float s = 0.0f;
-        for (int q = lo + 4 * lane; q < hi; q += 4 * TPR) {
-            const float4 v = __ldcs(reinterpret_cast<const float4 *>(A + q));
-            const short4 o = __ldcs(reinterpret_cast<const short4 *>(P.coff + q));
-            s += v.x * wrow[o.x];
-            s += v.y * wrow[o.y];
-            s += v.z * wrow[o.z];
-            s += v.w * wrow[o.w];
+        int base = lo + lane;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (base + u * TPR < hi) s += v[u] * wrow[o[u]];
+        for (base += U * TPR; base < hi; base += U * TPR) {
+            ls_round_c<U, TPR>(P, A, base, hi, o, v);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (base + u * TPR < hi) s += v[u] * wrow[o[u]];
         }
 #pragma unroll
         for (int k = TPR / 2; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k, TPR);
@@ -942,9 +967,16 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
             Ap[i] = s;
             dot += (double)wrow[0] * (double)s;
         }
-        i = inext;
+        i += STEP;
         lo = lo_n;
         hi = hi_n;
+        lo_n = lo_2;
+        hi_n = hi_2;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            o[u] = on[u];
+            v[u] = vn[u];
+        }
     }
 }
 
@@ -1603,7 +1635,7 @@ static int member_vectors(femd_batch_s *B, Member &M, bool mixed)
     cudaStream_t s = B->ctx->stream;
     const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
     if (mixed && !M.f32) {
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 3 * n + 7 * n + 32) * sizeof(float), s);
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 7 * n + 32) * sizeof(float), s);
         if (e != cudaSuccess) { M.f32 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
         if (reinterpret_cast<uintptr_t>(M.f32) & 15) {
             // the FP32 values are read by 16-byte bulk copies
@@ -1639,8 +1671,8 @@ static BProb describe(femd_batch_s *B, int id, bool mixed)
     const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
     if (mixed) {
         float *f = M.f32;
-        P.A32 = f;                          // nnz, or the compact layout's padded count (<= nnz + 3 n)
-        f = M.f32 + ((nnz + 3 * n + 7) & ~(size_t)7);
+        P.A32 = f; f += nnz;
+        f = M.f32 + ((nnz + 7) & ~(size_t)7);
         P.inv32 = f; f += n;
         P.r32 = f; f += n;
         P.z32 = f; f += n;
@@ -1962,17 +1994,10 @@ static int build_compact(femd_ctx ctx, femd_pattern P)
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));
     std::vector<int> order;
     rcm_order(n, ip, ix, order);
-    // every reordered row padded to a multiple of 4 entries (value 0, offset 0), so a lane reads
-    // 4 values and 4 offsets with one 16-byte and one 8-byte load
     std::vector<int> iperm((size_t)n), cptr((size_t)n + 1, 0), dst((size_t)std::max<long long>(nnz, 1));
+    std::vector<short> off((size_t)std::max<long long>(nnz, 1));
     for (int k = 0; k < n; ++k) iperm[order[k]] = k;
-    long long npad = 0;
-    for (int k = 0; k < n; ++k) {
-        npad += (ip[order[k] + 1] - ip[order[k]] + 3) & ~3;
-        if (npad >= INT_MAX / 2) { P->cl_state = -1; return FEMD_OK; }
-        cptr[k + 1] = (int)npad;
-    }
-    std::vector<short> off((size_t)std::max<long long>(npad, 1), (short)0);
+    for (int k = 0; k < n; ++k) cptr[k + 1] = cptr[k] + (ip[order[k] + 1] - ip[order[k]]);
     const int ntile = (n + CL_TILE - 1) / CL_TILE;
     std::vector<int> tlo((size_t)ntile, INT_MAX), thi((size_t)ntile, INT_MIN);
     std::vector<std::pair<int, int>> row;
@@ -2002,15 +2027,14 @@ static int build_compact(femd_ctx ctx, femd_pattern P)
     }
     int st;
     if ((st = P->cl_iperm.alloc((size_t)n)) || (st = P->cl_indptr.alloc((size_t)n + 1)) ||
-        (st = P->cl_dst.alloc((size_t)std::max<long long>(nnz, 1))) || (st = P->cl_off.alloc((size_t)npad + 8)))
+        (st = P->cl_dst.alloc((size_t)std::max<long long>(nnz, 1))) || (st = P->cl_off.alloc((size_t)std::max<long long>(nnz, 1))))
         return st;
     FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_iperm.p, iperm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
     FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_indptr.p, cptr.data(), ((size_t)n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
     if (nnz) {
         FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_dst.p, dst.data(), (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
-        FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_off.p, off.data(), (size_t)npad * sizeof(short), cudaMemcpyHostToDevice, s));
+        FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_off.p, off.data(), (size_t)nnz * sizeof(short), cudaMemcpyHostToDevice, s));
     }
-    P->cl_nnz = npad;
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // the host vectors are released on return
     P->cl_tile_lo.swap(tlo);
     P->cl_tile_hi.swap(thi);
@@ -2096,11 +2120,10 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
     if (mx && (M.need_f32 || M.f32_compact != compact)) {
         cudaStream_t s = ctx->stream;
         const unsigned g = grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count);
-        if (compact) {
-            FEMD_TRY_CUDA(cudaMemsetAsync(desc.A32, 0, (size_t)M.K->pattern->cl_nnz * sizeof(float), s));   // the padding
+        if (compact)
             k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, M.K->pattern->cl_dst.p, desc.A32, M.nnz, M.K->inv.p,
                                                      M.K->pattern->cl_iperm.p, desc.inv32, M.n);
-        } else
+        else
             k_batch_f32<<<g, 256, 0, counted(s)>>>(M.K->data.p, desc.A32, M.nnz, M.K->inv.p, desc.inv32, M.n);
         FEMD_TRY_CUDA(cudaGetLastError());
         M.need_f32 = false;

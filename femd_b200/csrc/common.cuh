@@ -146,7 +146,6 @@ struct femd_pattern_s : femd::HandleBase {
     // entry its position in the reordered layout; per tile of 32 reordered rows the smallest and
     // largest column.  cl_state: 0 not built, 1 built, -1 unsuitable (a column offset over 32767)
     int cl_state = 0, cl_bw = 0;
-    int cl_nnz = 0;                    // entries of the compact layout (rows padded to multiples of 4)
     femd::DevBuf<int> cl_iperm, cl_indptr, cl_dst;
     femd::DevBuf<short> cl_off;
     std::vector<int> cl_tile_lo, cl_tile_hi;
