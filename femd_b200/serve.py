@@ -184,8 +184,9 @@ class Server:
     device's free memory (free_memory(), default cudaMemGetInfo through torch) less
     reserve_bytes, and, when hbm_budget is given, that budget less what the requests in flight
     hold.  big_nnz: requests whose matrix has at least that many nonzeros are solved one at a time
-    on the whole GPU (femd_b200.cg_solve, the same precision) between batch launches -- a large
-    system streams HBM better with every block on it than as one team among many.  engine:
+    on the whole GPU between batch launches (femd_b200.cg_solve: the fused FP64 Jacobi-PCG, or
+    the single mixed solve when big_mixed) -- a large system streams HBM better through the
+    single-solve kernels than as many table entries among other members.  engine:
     "continuous" (the lockstep engine, resumable: requests join at the next chunk boundary
     after they are admitted, every request in flight advances by about iters iterations per
     step, finished ones leave), "persistent" (members join and leave between cooperative launches
@@ -194,7 +195,7 @@ class Server:
 
     def __init__(self, lib, sessions=(), *, mixed=True, iters=64, tol=1e-10, reserve_bytes=2 << 30, free_memory=None,
                  hbm_budget=None, max_members=1024, keep_solutions=False, shape=None, big_nnz=None,
-                 engine="continuous"):
+                 big_mixed=False, engine="continuous"):
         torch = _torch()
         if engine not in ("persistent", "lockstep", "continuous"):
             raise ValueError(f"serve: unknown engine {engine!r}")
@@ -207,6 +208,7 @@ class Server:
         self.max_members = int(max_members)
         self.keep = keep_solutions
         self.big_nnz = big_nnz
+        self.big_mixed = bool(big_mixed)
         self.batch = Batch()
         if shape:
             self.batch.configure(*shape)
@@ -272,7 +274,7 @@ class Server:
         """One request of the whole-GPU path."""
         r, S, K, b, x, _ = self.direct.popleft()
         x, conv, its, res, brk = fb.cg_solve(K, fb.JacobiPreconditioner(K), b, x, max(1000, 10 * K.nrows), self.tol,
-                                             mixed=self.mixed)
+                                             mixed=self.mixed and self.big_mixed)
         last = fb.cg_solve.last
         self._finish(r, S, x, dict(iterations=its, converged=conv, residual=res, status=0,
                                    reliable_updates=int(last.outer)), time.perf_counter() - t0)
