@@ -25,6 +25,7 @@
 #include <climits>
 #include <cmath>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -305,6 +306,9 @@ struct FastSpec {
     int psym[MAX_PAIRS];                      // pair k stands for (r, s) and (s, r) of a symmetric form
     int has_const, has_var, nf;               // factors per cell: npair (const) + nq npair (varying)
     int vector;
+    // the constant terms folded per pair onto the 15 monomials of degree <= 2 in J^-1 (1, Ji0..3,
+    // Ji_a Ji_b with a <= b): F_k = |det J| sum_m cm[k][m] mono_m (filled by fast_spec)
+    double cm[MAX_PAIRS][15];
 };
 
 __device__ __forceinline__ double amat(int m, int r, double Ji0, double Ji1, double Ji2, double Ji3)
@@ -355,14 +359,13 @@ __global__ void __launch_bounds__(256) k_elem_factors(const double *__restrict__
         double *F = factors + (size_t)e * fs.nf;
         int o = 0;
         if (fs.has_const) {
+            // the constant terms as a dot product with the monomials of J^-1 (no per-term branches)
+            const double mono[15] = {1.0, Ji0, Ji1, Ji2, Ji3, Ji0 * Ji0, Ji0 * Ji1, Ji0 * Ji2, Ji0 * Ji3,
+                                     Ji1 * Ji1, Ji1 * Ji2, Ji1 * Ji3, Ji2 * Ji2, Ji2 * Ji3, Ji3 * Ji3};
             for (int k = 0; k < fs.npair; ++k) {
                 double acc = 0.0;
-                for (int t = 0; t < fs.nterms; ++t) {
-                    if (fs.kind[t] != FEMD_COEF_CONST) continue;
-                    const double ar = amat(fs.a[t], fs.pr[k], Ji0, Ji1, Ji2, Ji3);
-                    const double bs = fs.vector ? 1.0 : amat(fs.b[t], fs.ps[k], Ji0, Ji1, Ji2, Ji3);
-                    acc += fs.cval[t] * ar * bs;
-                }
+#pragma unroll
+                for (int m = 0; m < 15; ++m) acc += fs.cm[k][m] * mono[m];
                 F[o++] = ad * acc;
             }
             if (!fs.has_var && (fs.npair & 1)) F[o++] = 0.0;
@@ -1000,6 +1003,27 @@ static void fast_spec(int nterms, const int *a, const int *b, const femd_coef *c
             fs.ps[fs.npair] = s;
             fs.psym[fs.npair] = symmetric && r != s && act[s][r];
             ++fs.npair;
+        }
+    // cm: amat(m, r) is 0, 1 or one entry of J^-1 (index 0 / 1 / 2 + entry); a product of two is a
+    // monomial: 0 = 1, 1-4 = Ji0..Ji3, then Ji_a Ji_b (a <= b) in row order
+    auto aidx = [](int m, int r) {
+        if (m == 0) return r == 0 ? 1 : 0;
+        if (r == 0) return 0;
+        if (m == 1) return r == 1 ? 2 : 4;    // Ji0 : Ji2
+        return r == 1 ? 3 : 5;                // Ji1 : Ji3
+    };
+    auto mono = [](int i, int j) {            // i, j in 1..5 (1 = the constant, 2..5 = Ji0..Ji3)
+        if (i > j) std::swap(i, j);
+        if (i == 1) return j - 1;             // 1 -> 0, Ji_x -> 1 + x
+        const int a = i - 2, b = j - 2;       // Ji_a Ji_b, a <= b
+        static const int base[4] = {5, 9, 12, 14};
+        return base[a] + (b - a);
+    };
+    for (int k = 0; k < fs.npair; ++k)
+        for (int t = 0; t < nterms; ++t) {
+            if (coef[t].kind != FEMD_COEF_CONST) continue;
+            const int i = aidx(a[t], fs.pr[k]), j = vector ? 1 : aidx(b[t], fs.ps[k]);
+            if (i && j) fs.cm[k][mono(i, j)] += coef[t].value;
         }
     fs.nf = (fs.has_const ? fs.npair : 0) + (fs.has_var ? nq * fs.npair : 0);
     // constant coefficients only: an even count per cell (one zero pad), so that a cell's factors
