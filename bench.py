@@ -702,7 +702,7 @@ def ours_c4(args, rank, world, dist):
 
 
 # ---- config 5: the serving sweep ---------------------------------------------------------------
-C5_BIG_NNZ = 2_000_000
+C5_BIG_NNZ = 1_000_000
 
 
 def c5_sweep(fb, torch, nreq=120, nsessions=16, seed=21, lambdas=LAMBDAS, big_nnz=C5_BIG_NNZ):
