@@ -153,3 +153,33 @@ def test_continuous_admits_mid_flight(sv, lib):
         xa, ra = Batch([K]).solve([b], mixed=True, engine="lockstep")
         assert ra[0]["converged"]
         assert np.array_equal(xa[0].cpu().numpy(), x.cpu().numpy())
+
+
+def test_large_requests_on_the_whole_gpu_path(sv, lib):
+    """big_nnz: requests whose matrix reaches it are solved one at a time by the fused FP64 CG
+    between batch steps -- the plain path's solve, so their solutions are the plain path's bits;
+    the batched ones stay within 1e-8 of plain FP64."""
+    sizes = [8, 12, 20, 24]
+    big = lib.get(20, 2)["nnz"]                       # every (20, 2) or larger request goes direct
+    sessions = sv.make_sessions(lib, 7, 2, sizes=sizes)
+    trace = sv.make_trace(13, 1e6, 16, len(sessions), sizes=sizes)
+    for S in sessions:
+        S.reset()
+    srv = sv.Server(lib, sessions, mixed=True, iters=16, keep_solutions=True, tol=1e-12, engine="continuous", big_nnz=big)
+    st = srv.run(trace, realtime=False)
+    assert st["completed"] == len(trace) and st["all_converged"]
+    served = {r.rid: r.x.clone() for r in trace}
+    for S in sessions:
+        S.reset()
+    trace2 = sv.make_trace(13, 1e6, 16, len(sessions), sizes=sizes)
+    sv.run_plain(lib, sessions, trace2, tol=1e-12, realtime=False, keep_solutions=True)
+    ndirect = 0
+    for r in trace2:
+        nnz = (sessions[r.session].A.nnz if r.kind == "heat" else lib.get(r.N, r.k)["nnz"])
+        a, b = served[r.rid].cpu().numpy(), r.x.cpu().numpy()
+        if nnz >= big:                                # a large session's every step is on the direct path
+            ndirect += 1
+            assert np.array_equal(a, b), r
+        else:
+            assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(b), r
+    assert ndirect > 0
