@@ -404,7 +404,7 @@ def kernel_rates(fb, torch, pr, hbm):
     reps = 20
     t, _ = event_time(torch, s, lambda: pr.assemble(jacobi=False), reps)
     alg3 = 16 * nv + 12 * ne + 4 * ne * nl * nl + 8 * nnz
-    out.append(("K3 assembly (k_elem_factors + k_assemble_nnz), FP64 values", t / reps, alg3,
+    out.append(("K3 assembly (k_elem_factors + k_assemble_rows_off), FP64 values", t / reps, alg3,
                 "16 nv (coordinates) + 12 ne (triangles) + 4 ne nloc^2 (map) + 8 nnz (values written)"))
     pr.assemble(jacobi=True)
     us = C.c_double()

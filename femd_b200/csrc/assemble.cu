@@ -368,7 +368,6 @@ __global__ void __launch_bounds__(256) k_elem_factors(const double *__restrict__
                 for (int m = 0; m < 15; ++m) acc += fs.cm[k][m] * mono[m];
                 F[o++] = ad * acc;
             }
-            if (!fs.has_var && (fs.npair & 1)) F[o++] = 0.0;
         }
         if (fs.has_var) {
             for (int q = 0; q < nq; ++q) {
@@ -598,299 +597,6 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows_off(
     }
 }
 
-// ---- K3e: one thread per nonzero over the inverted scatter map --------------------------------
-// Every matrix position p has the list of its element entries (cell nloc^2 + l nloc + j) in
-// increasing cell order (cptr / cent, built once per pattern by k_contrib_*).  A thread owns a
-// position: it forms each entry from the cell's factors and the reference tensors in shared memory
-// (the same contraction as K3d: sum over the active pairs k of F_k S^k(l, j), then the point terms)
-// and adds them in cell order in a register, then writes the value once -- consecutive threads
-// write consecutive positions.  No accumulator in shared memory and no atomics; the value is the
-// sum of its element contributions in increasing element order, as in the reference.
-//
-// The chain of loads per position (list bounds, then entry codes, then the cell's factors) is
-// latency-bound when a thread walks one position at a time, so with constant coefficients a
-// thread takes U positions of a tile (p = tile + u blockDim + tid, coalesced for every u) and
-// issues each level's loads for all of them, before the next level.  This pass adds the first two
-// entries of every position (most have one or two), read as one int2 per position (pcode, -1
-// for none), so a position needs one load before its cells' factors; the few positions with more
-// (a vertex's diagonal has one per cell around it) are listed once per pattern and finished by
-// k_assemble_nnz_long, which adds the rest to the stored value in the same cell order.
-template <int NLOC, int NPAIR>
-__device__ __forceinline__ double nnz_entry(int code, const double *__restrict__ F, const double *sS, const double *sR,
-                                            int nq, const FastSpec &fs)
-{
-    constexpr int NL2 = NLOC * NLOC;
-    const int e = code / NL2, lj = code - e * NL2, l = lj / NLOC, j = lj - l * NLOC;
-    F += (size_t)e * fs.nf;
-    double v = 0.0;
-    if (fs.has_const) {
-#pragma unroll
-        for (int k = 0; k < NPAIR; ++k) v += __ldg(&F[k]) * sS[k * NL2 + l * NLOC + j];
-    }
-    if (fs.has_var) {
-        const double *H = F + (fs.has_const ? NPAIR : 0);
-        for (int q = 0; q < nq; ++q) {
-            const double *R = sR + q * 3 * NLOC;
-#pragma unroll
-            for (int k = 0; k < NPAIR; ++k) v += (__ldg(&H[q * NPAIR + k]) * R[fs.pr[k] * NLOC + l]) * R[fs.ps[k] * NLOC + j];
-        }
-    }
-    return v;
-}
-
-// constant coefficients: the cell's factors as NP2 double2 (the count padded to even), the pair
-// tensors interleaved in shared memory as S2[l nloc + j][k] (k padded to 2 NP2), so an entry is
-// 2 NP2 vector loads; the products are added in pair order, as in nnz_entry
-template <int NPAIR>
-struct NnzPairs {
-    static constexpr int NP2 = (NPAIR + 1) / 2, NPP = 2 * NP2;
-};
-
-template <int NLOC, int NPAIR>
-__device__ __forceinline__ double nnz_const(int code, const double2 (&f)[NnzPairs<NPAIR>::NP2], const double *sS2)
-{
-    constexpr int NL2 = NLOC * NLOC, NP2 = NnzPairs<NPAIR>::NP2, NPP = NnzPairs<NPAIR>::NPP;
-    const int lj = code % NL2;
-    const double2 *s2 = reinterpret_cast<const double2 *>(sS2 + lj * NPP);
-    double v = 0.0;
-#pragma unroll
-    for (int h = 0; h < NP2; ++h) {
-        const double2 sv = s2[h];
-        v += f[h].x * sv.x;
-        if (2 * h + 1 < NPAIR) v += f[h].y * sv.y;
-    }
-    return v;
-}
-
-template <int NPAIR>
-__device__ __forceinline__ void nnz_factors(const double *factors, int nf, int code, int nl2, double2 (&f)[NnzPairs<NPAIR>::NP2])
-{
-    const double2 *F = reinterpret_cast<const double2 *>(factors + (size_t)(code < 0 ? 0 : code / nl2) * nf);
-#pragma unroll
-    for (int h = 0; h < NnzPairs<NPAIR>::NP2; ++h) f[h] = code >= 0 ? __ldg(&F[h]) : make_double2(0.0, 0.0);
-}
-
-template <int NLOC, int NPAIR, int U, bool VAR>
-__global__ void __launch_bounds__(256, 2) k_assemble_nnz(const int *__restrict__ cptr, const int *__restrict__ cent,
-                                                         const int2 *__restrict__ pcode,
-                                                         long long nnz, int nq, const double *__restrict__ factors,
-                                                         const double *__restrict__ g_S, const double *__restrict__ g_R,
-                                                         FastSpec fs, double *__restrict__ data)
-{
-    extern __shared__ __align__(16) double smem[];
-    constexpr int NL2 = NLOC * NLOC, NP2 = NnzPairs<NPAIR>::NP2, NPP = NnzPairs<NPAIR>::NPP;
-    double *sS = smem;
-    double *sR = sS + (fs.has_const ? NPAIR * NL2 : 0);
-    if (VAR) {
-        if (fs.has_const)
-            for (int t = threadIdx.x; t < NPAIR * NL2; t += blockDim.x) sS[t] = g_S[t];
-        for (int t = threadIdx.x; t < nq * 3 * NLOC; t += blockDim.x) sR[t] = g_R[t];
-    } else {
-        for (int t = threadIdx.x; t < NL2 * NPP; t += blockDim.x) {
-            const int lj = t / NPP, k = t - lj * NPP;
-            sS[t] = k < NPAIR ? g_S[k * NL2 + lj] : 0.0;
-        }
-    }
-    __syncthreads();
-    if (VAR) {
-        for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x) {
-            const int c0 = __ldcs(&cptr[p]), c1 = __ldcs(&cptr[p + 1]);
-            double acc = 0.0;
-            for (int c = c0; c < c1; ++c) acc += nnz_entry<NLOC, NPAIR>(__ldcs(&cent[c]), factors, sS, sR, nq, fs);
-            data[p] = acc;
-        }
-        return;
-    }
-    const int nf = fs.nf;
-    const long long tile = (long long)U * blockDim.x, stride = (long long)gridDim.x * tile;
-    // the codes of the next round are loaded before the current round's factors and sums, so the
-    // stream of codes waits on memory while the previous round computes
-    int2 nxt[U];
-    long long base = (long long)blockIdx.x * tile;
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-        const long long p = base + u * (long long)blockDim.x + threadIdx.x;
-        nxt[u] = p < nnz ? __ldcs(&pcode[p]) : make_int2(-1, -1);
-    }
-    for (; base < nnz; base += stride) {
-        int2 cur[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) cur[u] = nxt[u];
-        const long long nb = base + stride;
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const long long p = nb + u * (long long)blockDim.x + threadIdx.x;
-            nxt[u] = p < nnz ? __ldcs(&pcode[p]) : make_int2(-1, -1);
-        }
-        double2 f0[U][NP2], f1[U][NP2];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            nnz_factors<NPAIR>(factors, nf, cur[u].x, NL2, f0[u]);
-            nnz_factors<NPAIR>(factors, nf, cur[u].y, NL2, f1[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const long long p = base + u * (long long)blockDim.x + threadIdx.x;
-            double acc = 0.0;
-            if (cur[u].x >= 0) acc += nnz_const<NLOC, NPAIR>(cur[u].x, f0[u], sS);
-            if (cur[u].y >= 0) acc += nnz_const<NLOC, NPAIR>(cur[u].y, f1[u], sS);
-            if (p < nnz) data[p] = acc;
-        }
-    }
-}
-
-// the positions with more than two element entries: entries 2.. added to the stored sum of the
-// first two, in cell order; LU codes (and their factors) in flight per round
-template <int NLOC, int NPAIR>
-__global__ void __launch_bounds__(256) k_assemble_nnz_long(const int *__restrict__ lpos, int nlong, const int *__restrict__ cptr,
-                                                           const int *__restrict__ cent, const double *__restrict__ factors,
-                                                           const double *__restrict__ g_S, int nf, double *__restrict__ data)
-{
-    extern __shared__ __align__(16) double smem[];
-    constexpr int NL2 = NLOC * NLOC, NP2 = NnzPairs<NPAIR>::NP2, NPP = NnzPairs<NPAIR>::NPP, LU = 4;
-    double *sS = smem;
-    for (int t = threadIdx.x; t < NL2 * NPP; t += blockDim.x) {
-        const int lj = t / NPP, k = t - lj * NPP;
-        sS[t] = k < NPAIR ? g_S[k * NL2 + lj] : 0.0;
-    }
-    __syncthreads();
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nlong; t += gridDim.x * blockDim.x) {
-        const int p = lpos[t];
-        const int c1 = cptr[p + 1];
-        double acc = data[p];
-        for (int c = cptr[p] + 2; c < c1; c += LU) {
-            int code[LU];
-            double2 f[LU][NP2];
-#pragma unroll
-            for (int u = 0; u < LU; ++u) code[u] = c + u < c1 ? __ldcs(&cent[c + u]) : -1;
-#pragma unroll
-            for (int u = 0; u < LU; ++u) nnz_factors<NPAIR>(factors, nf, code[u], NL2, f[u]);
-#pragma unroll
-            for (int u = 0; u < LU; ++u)
-                if (code[u] >= 0) acc += nnz_const<NLOC, NPAIR>(code[u], f[u], sS);
-        }
-        data[p] = acc;
-    }
-}
-
-__global__ void k_pair_codes(const int *__restrict__ cptr, const int *__restrict__ cent, long long nnz, int2 *__restrict__ pcode)
-{
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x) {
-        const int c0 = cptr[p], c1 = cptr[p + 1];
-        pcode[p] = make_int2(c0 < c1 ? cent[c0] : -1, c0 + 1 < c1 ? cent[c0 + 1] : -1);
-    }
-}
-
-__global__ void k_long_flags(const int *__restrict__ cptr, long long nnz, int *__restrict__ flag)
-{
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x)
-        flag[p] = cptr[p + 1] - cptr[p] > 2 ? 1 : 0;
-}
-
-__global__ void k_long_fill(const int *__restrict__ flag, const int *__restrict__ idx, long long nnz, int *__restrict__ lpos)
-{
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (long long)gridDim.x * blockDim.x)
-        if (flag[p]) lpos[idx[p]] = (int)p;
-}
-
-// the inverse diagonal from the assembled values (JacobiPreconditioner, precond.hpp:82-102)
-__global__ void k_asm_inv(const int *__restrict__ diag_pos, const double *__restrict__ data, double *__restrict__ inv, int n,
-                          int *__restrict__ status)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int d = diag_pos[i];
-        const double a = d >= 0 ? data[d] : 0.0;
-        if (d < 0 || a == 0.0) { atomicOr(status, ST_ZERODIAG); atomicMin(status + 1, i); }
-        inv[i] = 1.0 / a;
-    }
-}
-
-// the inverted scatter map, pass 1: per position the number of element entries (one thread per
-// row walks its (cell, local) pairs and their row offsets; a row's positions are its own)
-__global__ void k_contrib_count(const int *__restrict__ rc_ptr, const int *__restrict__ indptr,
-                                const unsigned char *__restrict__ off, int nrows, int nloc, int offs, int *__restrict__ cnt)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x) {
-        const int rlo = indptr[i];
-        for (int c = rc_ptr[i]; c < rc_ptr[i + 1]; ++c)
-            for (int j = 0; j < nloc; ++j) {
-                const unsigned o = off[(size_t)c * offs + j];
-                if (o != 0xffu) cnt[rlo + o] += 1;
-            }
-    }
-}
-
-// pass 2: the entries, in the row's cell order (so each position's list is in increasing cell
-// order); cur starts as the exclusive prefix of the counts
-__global__ void k_contrib_fill(const int *__restrict__ rc_ptr, const int *__restrict__ rc_code,
-                               const int *__restrict__ indptr, const unsigned char *__restrict__ off, int nrows, int nloc,
-                               int offs, int *__restrict__ cur, int *__restrict__ cent)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nrows; i += gridDim.x * blockDim.x) {
-        const int rlo = indptr[i];
-        for (int c = rc_ptr[i]; c < rc_ptr[i + 1]; ++c) {
-            const int code = rc_code[c];
-            for (int j = 0; j < nloc; ++j) {
-                const unsigned o = off[(size_t)c * offs + j];
-                if (o != 0xffu) cent[cur[rlo + o]++] = code * nloc + j;
-            }
-        }
-    }
-}
-
-static int build_pair_offsets(femd_ctx ctx, femd_pattern p);
-
-// the inverted scatter map of a pattern (once): contrib_ptr (nnz + 1), contrib (every element entry)
-static int build_contrib(femd_ctx ctx, femd_pattern p)
-{
-    if (p->contrib_ptr.p) return FEMD_OK;
-    cudaStream_t s = ctx->stream;
-    FEMD_CHECK_ARG(p->max_row_len < 255, "assembly: a row is too long for the byte offsets of the inverted scatter map");
-    FEMD_TRY(build_pair_offsets(ctx, p));
-    const int offs = (p->nloc + 3) / 4 * 4, n = p->nrows;
-    const long long nnz = p->nnz;
-    FEMD_CHECK_ARG(nnz < INT_MAX && (long long)p->ncells * p->nloc * p->nloc < INT_MAX,
-                   "assembly: the pattern is too large for the inverted scatter map");
-    DevBuf<int> cnt, tmp;
-    FEMD_TRY(cnt.alloc((size_t)nnz + 1));
-    FEMD_TRY(tmp.alloc(scan_tmp_ints((size_t)nnz + 1)));
-    FEMD_TRY(p->contrib_ptr.alloc((size_t)nnz + 1));
-    FEMD_TRY_CUDA(cudaMemsetAsync(cnt.p, 0, ((size_t)nnz + 1) * sizeof(int), s));
-    const unsigned g = grid_for((size_t)n, 256, 1u << 20);
-    k_contrib_count<<<g, 256, 0, counted(s)>>>(p->rc_ptr.p, p->indptr.p, p->pair_off.p, n, p->nloc, offs, cnt.p);
-    FEMD_TRY_CUDA(cudaGetLastError());
-    FEMD_TRY(exclusive_scan_int(cnt.p, p->contrib_ptr.p, (size_t)nnz + 1, tmp.p, s));
-    int total = 0;
-    FEMD_TRY_CUDA(cudaMemcpyAsync(&total, p->contrib_ptr.p + nnz, sizeof(int), cudaMemcpyDeviceToHost, s));
-    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
-    int st = p->contrib.alloc((size_t)std::max(total, 1));
-    if (st) { p->contrib_ptr.release(); return st; }
-    FEMD_TRY_CUDA(cudaMemcpyAsync(cnt.p, p->contrib_ptr.p, ((size_t)nnz + 1) * sizeof(int), cudaMemcpyDeviceToDevice, s));
-    k_contrib_fill<<<g, 256, 0, counted(s)>>>(p->rc_ptr.p, p->rc_code.p, p->indptr.p, p->pair_off.p, n, p->nloc, offs, cnt.p,
-                                               p->contrib.p);
-    FEMD_TRY_CUDA(cudaGetLastError());
-    // the positions with more than two entries, in increasing order (flags, scan, fill)
-    DevBuf<int> idx;
-    if ((st = idx.alloc((size_t)nnz + 1))) { p->contrib_ptr.release(); p->contrib.release(); return st; }
-    const unsigned gz = grid_for((size_t)std::max<long long>(nnz, 1), 256, 1u << 20);
-    k_long_flags<<<gz, 256, 0, counted(s)>>>(p->contrib_ptr.p, nnz, cnt.p);
-    FEMD_TRY_CUDA(cudaMemsetAsync(cnt.p + nnz, 0, sizeof(int), s));
-    FEMD_TRY(exclusive_scan_int(cnt.p, idx.p, (size_t)nnz + 1, tmp.p, s));
-    int nlong = 0;
-    FEMD_TRY_CUDA(cudaMemcpyAsync(&nlong, idx.p + nnz, sizeof(int), cudaMemcpyDeviceToHost, s));
-    FEMD_TRY_CUDA(cudaStreamSynchronize(s));
-    if ((st = p->contrib_long.alloc((size_t)std::max(nlong, 1)))) { p->contrib_ptr.release(); p->contrib.release(); return st; }
-    p->n_long = nlong;
-    if (nlong) k_long_fill<<<gz, 256, 0, counted(s)>>>(cnt.p, idx.p, nnz, p->contrib_long.p);
-    if ((st = p->contrib_pair.alloc((size_t)nnz + 1))) {
-        p->contrib_ptr.release(); p->contrib.release(); p->contrib_long.release();
-        return st;
-    }
-    k_pair_codes<<<gz, 256, 0, counted(s)>>>(p->contrib_ptr.p, p->contrib.p, nnz, p->contrib_pair.p);
-    FEMD_TRY_CUDA(cudaGetLastError());
-    FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // cnt, idx and tmp are released on return
-    return FEMD_OK;
-}
 
 // The pair offsets: for rc index c (row i, cell entry code = cell nloc + l), byte j of
 // off[c * OFFS + j] = position of (i, dof(cell, j)) minus indptr[i], 255 where constrained.
@@ -1026,9 +732,6 @@ static void fast_spec(int nterms, const int *a, const int *b, const femd_coef *c
             if (i && j) fs.cm[k][mono(i, j)] += coef[t].value;
         }
     fs.nf = (fs.has_const ? fs.npair : 0) + (fs.has_var ? nq * fs.npair : 0);
-    // constant coefficients only: an even count per cell (one zero pad), so that a cell's factors
-    // start on a 16-byte boundary and load as double2
-    if (!fs.has_var && (fs.nf & 1)) fs.nf += 1;
 }
 
 static int check_common(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule *rule, femd_pattern p, int nterms,
@@ -1132,10 +835,6 @@ static int prepare_terms(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
 }
 
 static constexpr int FAST_MAX_ROW = 96;   // longest row the shared-memory accumulator holds
-#ifndef FEMD_NNZ_U
-#define FEMD_NNZ_U 1
-#endif
-static constexpr int NNZ_U = FEMD_NNZ_U;  // positions per thread in flight in k_assemble_nnz
 
 // FAST assembly of a matrix (K non-null) or a vector (f non-null).  Tables and factors live in
 // the pattern's workspace; no allocation once the workspace has its size.
@@ -1221,49 +920,6 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
         const size_t sho = ((fs.has_const ? (size_t)fs.npair * nl2 : 0) + (fs.has_var ? nref : 0) +
                             (size_t)maxlen * FAST_BLOCK) * sizeof(double) +
                            (FAST_BLOCK / 32) * 33 * sizeof(int) + (size_t)FAST_BLOCK * maxlen;
-#define FEMD_NNZ(NL, NP)                                                                                               \
-        if (!done && nl == NL && fs.npair == NP && p->nnz > 0 && B_NNZ) {                                             \
-            const size_t shn = (fs.has_var ? (fs.has_const ? (size_t)NP * NL * NL : 0) + nref                          \
-                                           : (size_t)NL * NL * NnzPairs<NP>::NPP) * sizeof(double);                    \
-            const unsigned gq = (unsigned)ctx->sm_count * 64;                                                         \
-            if (fs.has_var) {                                                                                          \
-                cudaFuncSetAttribute(k_assemble_nnz<NL, NP, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shn); \
-                k_assemble_nnz<NL, NP, 1, true><<<grid_for((size_t)p->nnz, 256, gq), 256, shn, counted(s)>>>(           \
-                    p->contrib_ptr.p, p->contrib.p, p->contrib_pair.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs,     \
-                    K->data.p);                                                                                        \
-            } else {                                                                                                   \
-                cudaFuncSetAttribute(k_assemble_nnz<NL, NP, NNZ_U, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                     (int)shn);                                                                        \
-                k_assemble_nnz<NL, NP, NNZ_U, false><<<grid_for((size_t)p->nnz, 256 * NNZ_U, gq), 256, shn, counted(s)>>>( \
-                    p->contrib_ptr.p, p->contrib.p, p->contrib_pair.p, p->nnz, nq, p->ws_factors.p, d_S, d_ref, fs,     \
-                    K->data.p);                                                                                        \
-                if (p->n_long) {                                                                                       \
-                    cudaFuncSetAttribute(k_assemble_nnz_long<NL, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                                         (int)shn);                                                                    \
-                    k_assemble_nnz_long<NL, NP><<<grid_for((size_t)p->n_long, 256, gq), 256, shn, counted(s)>>>(        \
-                        p->contrib_long.p, p->n_long, p->contrib_ptr.p, p->contrib.p, p->ws_factors.p, d_S, fs.nf,      \
-                        K->data.p);                                                                                    \
-                }                                                                                                      \
-            }                                                                                                          \
-            if (inv) k_asm_inv<<<grid_for((size_t)n, 256, 1u << 20), 256, 0, counted(s)>>>(p->diag_pos.p, K->data.p,   \
-                                                                                            inv, n, ctx->status_dev);  \
-            done = true;                                                                                               \
-        }
-        // the nonzero-parallel kernel where the inverted scatter map can be built
-        const bool B_NNZ = p->contrib_ptr.p || build_contrib(ctx, p) == FEMD_OK;
-        if (!B_NNZ) {
-            // no room (or a row too long): the row kernels below
-            p->contrib_ptr.release();
-            p->contrib.release();
-            p->contrib_long.release();
-            p->contrib_pair.release();
-            cudaGetLastError();
-            clear_error();
-        }
-        FEMD_NNZ(3, 1) FEMD_NNZ(3, 3) FEMD_NNZ(3, 4) FEMD_NNZ(3, 5)
-        FEMD_NNZ(6, 1) FEMD_NNZ(6, 3) FEMD_NNZ(6, 4) FEMD_NNZ(6, 5)
-        FEMD_NNZ(10, 1) FEMD_NNZ(10, 3) FEMD_NNZ(10, 4) FEMD_NNZ(10, 5)
-#undef FEMD_NNZ
 #define FEMD_ROWS_OFF(NL, NP)                                                                                          \
         if (!done && nl == NL && fs.npair == NP && maxlen < 255) {                                                     \
             FEMD_TRY(build_pair_offsets(ctx, p));                                                                      \

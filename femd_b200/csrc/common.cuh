@@ -130,12 +130,6 @@ struct femd_pattern_s : femd::HandleBase {
     static constexpr int TABLE_SLOTS = 4;
     TableSlot tables[TABLE_SLOTS];
     unsigned long long table_clock = 0;
-    // the scatter map inverted: for every matrix position, its element entries
-    // (cell nloc^2 + l nloc + j) in increasing cell order (built on the first FAST assembly)
-    femd::DevBuf<int> contrib_ptr, contrib;
-    femd::DevBuf<int> contrib_long;    // the positions with more than two entries, increasing
-    femd::DevBuf<int2> contrib_pair;   // per position its first two entries (-1: none)
-    int n_long = 0;
     // for every (row, cell) pair of the rc lists, the offsets within the row of the cell's nloc
     // columns (uint8, 255 = constrained): the scatter map in the rows' own order, a quarter of
     // its size (built on the first FAST assembly when every row is shorter than 255)
