@@ -706,9 +706,10 @@ C5_BIG_NNZ = 1_000_000
 
 
 def c5_sweep(fb, torch, nreq=120, nsessions=16, seed=21, lambdas=LAMBDAS, big_nnz=C5_BIG_NNZ):
-    """Served (mixed, continuous batching; requests of at least big_nnz nonzeros on the whole-GPU
-    FP64 path) and plain FP64 on the same seeded trace at each lambda: solves/s, p50 / p99
-    latency; the simulations are reset between the two paths."""
+    """Served (mixed precision: continuous batching, and requests of at least big_nnz nonzeros
+    one at a time on the whole GPU by the single mixed solve) and plain FP64 on the same seeded
+    trace at each lambda: solves/s, p50 / p99 latency; the simulations are reset between the two
+    paths."""
     from femd_b200 import serve
     lib = serve.SpaceLibrary()
     sessions = serve.make_sessions(lib, seed, nsessions)
@@ -722,7 +723,7 @@ def c5_sweep(fb, torch, nreq=120, nsessions=16, seed=21, lambdas=LAMBDAS, big_nn
             if path == "plain":
                 st = serve.run_plain(lib, sessions, trace, tol=TOL, realtime=True)
             else:
-                srv = serve.Server(lib, sessions, mixed=True, engine="continuous", big_nnz=big_nnz)
+                srv = serve.Server(lib, sessions, mixed=True, engine="continuous", big_nnz=big_nnz, big_mixed=True)
                 st = srv.run(trace, realtime=True)
                 del srv
             row[path] = {"solves_per_s": round(st["solves_per_s"], 3), "p50_ms": round(st["p50_ms"], 1),
@@ -731,8 +732,9 @@ def c5_sweep(fb, torch, nreq=120, nsessions=16, seed=21, lambdas=LAMBDAS, big_nn
     return {"workload": f"config 5: {nsessions} resident heat sessions (N log-uniform on a 2^(1/3) grid in [16, 1024], "
                         f"k in {{1, 2}}, dt log-uniform in [1e-4, 1e-1]), {nreq} requests per lambda (70% "
                         "backward-Euler steps, 30% fresh Poisson), Poisson arrivals in real time; served: "
-                        f"requests under {big_nnz} nonzeros batched (mixed precision, continuous lockstep engine), "
-                        "the others solved one at a time on the whole GPU (fused FP64 Jacobi-PCG) between batch steps",
+                        f"requests under {big_nnz} nonzeros batched (continuous lockstep engine), the others solved one "
+                        "at a time on the whole GPU (single-system PCG) between batch steps, all in FP32-inner / "
+                        "FP64-refined mixed precision",
             "sweep": rows}
 
 
