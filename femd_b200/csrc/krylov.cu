@@ -1600,6 +1600,13 @@ int femd_cuda_cg_jacobi_noalloc(femd_ctx ctx, femd_matrix K, int use_jacobi, con
     FEMD_CHECK_ARG(max_iter >= 0, "cg_jacobi_noalloc: max_iter must be >= 0");
     FEMD_CHECK_ARG(!use_jacobi || K->inv_valid, JACOBI_MISSING);
     FEMD_TRY_CUDA(cudaSetDevice(ctx->device));
+    // the solve reads its state back between chunks (a stream synchronization), which a stream
+    // capture does not allow
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    FEMD_TRY_CUDA(cudaStreamIsCapturing(ctx->stream, &cap));
+    FEMD_CHECK_ARG(cap == cudaStreamCaptureStatusNone,
+                   "cg_jacobi_noalloc: the context's stream is being captured; the solve synchronizes between chunks "
+                   "and cannot be captured");
     *res = femd_cg_result{1, 0, 0.0, 0, FEMD_OK, 0, 0.0};
     if (n == 0) return FEMD_OK;
     double *base = nullptr;

@@ -359,9 +359,11 @@ FEMD_API int femd_cuda_pcg_mixed(femd_ctx ctx, femd_matrix K, const double *b_de
  * static device array (about 25 MB, held by every GPU that loads the library until the process
  * exits) sized for at most 1,048,576 rows -- larger systems are rejected with FEMD_EINVAL.
  * The first call on a device (and the first after the device's CUDA context was made again, e.g.
- * after cudaDeviceReset) looks up that array's device address; make it before any stream
- * capture.  Every call shares the array: calls that overlap on the GPU (any stream or context
- * of the same device) race and must be serialized.  The solve updates x in place and reads b
+ * after cudaDeviceReset) looks up that array's device address.  The solve reads its state back
+ * between chunks (it synchronizes the context's stream), so it cannot be captured into a CUDA
+ * graph: called while that stream is capturing it returns FEMD_EINVAL.  Every call shares the
+ * array: calls that overlap on the GPU (any stream or context of the same device) race and must
+ * be serialized.  The solve updates x in place and reads b
  * throughout, so b and x must not overlap (FEMD_EINVAL).  Same kernels and iterates as
  * femd_cuda_cg_jacobi; res->seconds is not measured (0). */
 FEMD_API int femd_cuda_cg_jacobi_noalloc(femd_ctx ctx, femd_matrix K, int use_jacobi, const double *b_dev, double *x_dev,

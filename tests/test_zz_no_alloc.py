@@ -106,3 +106,36 @@ def test_noalloc_rejects_systems_beyond_its_scratch():
                                             C.byref(res))
     assert st == 1
     assert b"exceed the fixed scratch" in fb.lib.femd_cuda_last_error()
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """The solve synchronizes between chunks, so it cannot be captured: on a stream that is being
+    captured it returns FEMD_EINVAL before it enqueues anything (the capture is then ended)."""
+    import torch
+
+    import femd_b200 as fb
+    z, _ = golden("p2_varcoef_n16")
+    n = z["indptr"].size - 1
+    K = fb.CSRMatrix.from_arrays(n, n, z["indptr"], z["indices"], z["data"])
+    fb.JacobiPreconditioner(K)
+    b = torch.as_tensor(z["rhs"]).cuda()
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rt = C.CDLL("libcudart.so.12")                   # the runtime the library is linked against
+    s = C.c_void_p(fb.lib.femd_cuda_ctx_stream(K.ctx.h))
+    assert rt.cudaStreamBeginCapture(s, 1) == 0      # cudaStreamCaptureModeThreadLocal
+    res = fb._native.femd_cg_result()
+    try:
+        st = fb.lib.femd_cuda_cg_jacobi_noalloc(K.ctx.h, K.h, 1, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 100,
+                                                1e-10, C.byref(res))
+        err = fb.lib.femd_cuda_last_error()
+    finally:
+        g = C.c_void_p()
+        rt.cudaStreamEndCapture(s, C.byref(g))
+        if g.value:
+            rt.cudaGraphDestroy(g)
+    assert st == 1 and b"cannot be captured" in err
+    # the context still solves afterwards
+    st = fb.lib.femd_cuda_cg_jacobi_noalloc(K.ctx.h, K.h, 1, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 100000,
+                                            1e-10, C.byref(res))
+    assert st == 0 and res.converged
