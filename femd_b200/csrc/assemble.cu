@@ -485,21 +485,15 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows_off(
     const double *__restrict__ factors, const double *__restrict__ g_S, const double *__restrict__ g_R, FastSpec fs,
     int maxlen, double *__restrict__ data, double *__restrict__ inv, int *__restrict__ status)
 {
-    extern __shared__ __align__(16) double smem[];
+    extern __shared__ double smem[];
     constexpr int NL2 = NLOC * NLOC;
     constexpr int OFFS = (NLOC + 3) / 4 * 4;
     constexpr int NW = OFFS / 4;                             // 32-bit words of offsets per pair
-    // the pair tensors interleaved per entry, S2[(l nloc + j) NPP + k] (k padded to NPP = NPAIR
-    // rounded up to even), so an entry's NPAIR values load as double2
-    constexpr int NP2 = (NPAIR + 1) / 2, NPP = 2 * NP2;
     double *sS = smem;
-    double *sR = sS + (fs.has_const ? NPP * NL2 : 0);
+    double *sR = sS + (fs.has_const ? NPAIR * NL2 : 0);
     double *acc = sR + (fs.has_var ? nq * 3 * NLOC : 0);
     if (fs.has_const)
-        for (int t = threadIdx.x; t < NPP * NL2; t += blockDim.x) {
-            const int lj = t / NPP, k = t - lj * NPP;
-            sS[t] = k < NPAIR ? g_S[k * NL2 + lj] : 0.0;
-        }
+        for (int t = threadIdx.x; t < NPAIR * NL2; t += blockDim.x) sS[t] = g_S[t];
     if (fs.has_var)
         for (int t = threadIdx.x; t < nq * 3 * NLOC; t += blockDim.x) sR[t] = g_R[t];
     __syncthreads();
@@ -552,13 +546,8 @@ __global__ void __launch_bounds__(FAST_BLOCK) k_assemble_rows_off(
             for (int j = 0; j < NLOC; ++j) {
                 double s = 0.0;
                 if (fs.has_const) {
-                    const double2 *s2 = reinterpret_cast<const double2 *>(sS + (l * NLOC + j) * NPP);
 #pragma unroll
-                    for (int h = 0; h < NP2; ++h) {
-                        const double2 sv = s2[h];
-                        s += Fq[2 * h] * sv.x;
-                        if (2 * h + 1 < NPAIR) s += Fq[2 * h + 1] * sv.y;
-                    }
+                    for (int k = 0; k < NPAIR; ++k) s += Fq[k] * sS[k * NL2 + l * NLOC + j];
                 }
                 v[j] = s;
             }
@@ -928,7 +917,7 @@ static int fast_assemble(femd_ctx ctx, const femd_mesh2d *mesh, const femd_rule 
     if (n) {
         const unsigned grid = grid_for((size_t)n, FAST_BLOCK, 1u << 22);
         bool done = false;
-        const size_t sho = ((fs.has_const ? (size_t)((fs.npair + 1) / 2 * 2) * nl2 : 0) + (fs.has_var ? nref : 0) +
+        const size_t sho = ((fs.has_const ? (size_t)fs.npair * nl2 : 0) + (fs.has_var ? nref : 0) +
                             (size_t)maxlen * FAST_BLOCK) * sizeof(double) +
                            (FAST_BLOCK / 32) * 33 * sizeof(int) + (size_t)FAST_BLOCK * maxlen;
 #define FEMD_ROWS_OFF(NL, NP)                                                                                          \
