@@ -80,7 +80,10 @@ struct BProb {
     // lockstep engine, compact layout (mixed precision; null otherwise): the member's FP32 matrix
     // and its vectors are in the pattern's reverse Cuthill-McKee order; iperm maps an original row
     // to its reordered one, cptr / coff are the reordered rows' pointers and 16-bit column offsets
-    const int *iperm, *cptr;
+    // ctab: per reordered row its first position and the bits of the FP32 low part of its split
+    // diagonal (k_ls_split_rows), one table per member; row n holds the end
+    const int *iperm;
+    const int2 *ctab;
     const short *coff;
 };
 
@@ -776,6 +779,38 @@ __global__ void k_ls_f32_perm(const double *__restrict__ a, const int *__restric
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) inv32[iperm[i]] = (float)inv[i];
 }
 
+// The compact layout's row table of a member and its split diagonal.  With the off-diagonals
+// rounded to FP32, d = a_ii + sum_{j != i} (a_ij - fl(a_ij)) (FP64) keeps the FP64 row sum; it is
+// stored as hi = fl(d) at the diagonal position and lo = fl(d - hi) beside the row's first
+// position.  The represented matrix is then a graph Laplacian of the rounded off-diagonals plus
+// the row sums to about eps_32^2, whose quadratic form is within O(eps_32) of the FP64 one instead
+// of O(eps_32 cond(A)): the FP32 recurrence needs fewer iterations on large systems.  A pattern
+// without every diagonal position keeps the plain copy (lo = 0).  One thread per original row i
+// (after k_ls_f32_perm wrote the entries); thread n writes the end.
+__global__ void k_ls_split_rows(const int *__restrict__ indptr, const int *__restrict__ diag_pos, const double *__restrict__ a,
+                                const int *__restrict__ dst, const int *__restrict__ iperm, const int *__restrict__ cptr,
+                                int split, float *__restrict__ a32, int2 *__restrict__ ctab, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
+        if (i == n) {
+            ctab[n] = make_int2(cptr[n], 0);
+            continue;
+        }
+        const int r = iperm[i];
+        float lo = 0.0f;
+        if (split) {
+            const int q0 = indptr[i], q1 = indptr[i + 1], dp = diag_pos[i];
+            double d = a[dp];
+            for (int q = q0; q < q1; ++q)
+                if (q != dp) d += a[q] - (double)(float)a[q];
+            const float h = (float)d;
+            a32[dst[dp]] = h;
+            lo = (float)(d - (double)h);
+        }
+        ctab[r] = make_int2(cptr[r], __float_as_int(lo));
+    }
+}
+
 // chunk tables of one matrix: chunk k starts at the first row whose first nonzero is at or after
 // k * cp (cp = chunk capacity - longest row), so no chunk holds more than the capacity
 __global__ void k_chunk_table(const int *__restrict__ indptr, int n, int nnz, int cp, int nch, int *crow, int *cq)
@@ -904,8 +939,10 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
 // flight per lane, the products read p from shared memory (no gathers from global memory).  Each
 // lane adds its entries in increasing position and the row's lanes combine by a fixed shuffle tree.
 // The loop is pipelined: a row group's first round of values and offsets is loaded while the
-// previous group is summed (its row pointers two groups ahead), so a warp keeps two rounds of
-// the matrix stream in flight.
+// previous group is summed (its row table entries two groups ahead), so a warp keeps two rounds
+// of the matrix stream in flight.  The diagonal is split (k_ls_split_rows): its FP32 high part is
+// the row's diagonal entry, its low part comes with the row's table entry and is added to the
+// FP32 row sum, so the FP32 matrix keeps the FP64 matrix's row sums.
 template <int U, int TPR>
 __device__ __forceinline__ void ls_round_c(const BProb &P, const float *__restrict__ A, int base, int hi, short (&o)[U],
                                            float (&v)[U])
@@ -928,13 +965,18 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
     int i0 = r0 + (int)(threadIdx.x >> 5) * GPW;
     int i = i0 + sub;
     int lo = 0, hi = 0, lo_n = 0, hi_n = 0;
+    float dl = 0.0f, dl_n = 0.0f;                            // the rows' low diagonal parts
     if (i < r1) {
-        lo = P.cptr[i];
-        hi = P.cptr[i + 1];
+        const int2 c = P.ctab[i];
+        lo = c.x;
+        dl = __int_as_float(c.y);
+        hi = P.ctab[i + 1].x;
     }
     if (i + STEP < r1) {
-        lo_n = P.cptr[i + STEP];
-        hi_n = P.cptr[i + STEP + 1];
+        const int2 c = P.ctab[i + STEP];
+        lo_n = c.x;
+        dl_n = __int_as_float(c.y);
+        hi_n = P.ctab[i + STEP + 1].x;
     }
     short o[U];
     float v[U];
@@ -942,9 +984,12 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
     for (; i0 < r1; i0 += STEP) {
         const int i2 = i + 2 * STEP;
         int lo_2 = 0, hi_2 = 0;
+        float dl_2 = 0.0f;
         if (i2 < r1) {
-            lo_2 = P.cptr[i2];
-            hi_2 = P.cptr[i2 + 1];
+            const int2 c = P.ctab[i2];
+            lo_2 = c.x;
+            dl_2 = __int_as_float(c.y);
+            hi_2 = P.ctab[i2 + 1].x;
         }
         short on[U];
         float vn[U];
@@ -964,14 +1009,17 @@ __device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restric
 #pragma unroll
         for (int k = TPR / 2; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k, TPR);
         if (lane == 0 && i < r1) {
+            s = __fmaf_rn(dl, wrow[0], s);                    // the split diagonal's low part
             Ap[i] = s;
             dot += (double)wrow[0] * (double)s;
         }
         i += STEP;
         lo = lo_n;
         hi = hi_n;
+        dl = dl_n;
         lo_n = lo_2;
         hi_n = hi_2;
+        dl_n = dl_2;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             o[u] = on[u];
@@ -1635,7 +1683,7 @@ static int member_vectors(femd_batch_s *B, Member &M, bool mixed)
     cudaStream_t s = B->ctx->stream;
     const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
     if (mixed && !M.f32) {
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 7 * n + 32) * sizeof(float), s);
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 9 * n + 40) * sizeof(float), s);
         if (e != cudaSuccess) { M.f32 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
         if (reinterpret_cast<uintptr_t>(M.f32) & 15) {
             // the FP32 values are read by 16-byte bulk copies
@@ -1679,7 +1727,9 @@ static BProb describe(femd_batch_s *B, int id, bool mixed)
         P.pa32 = f; f += n;
         P.pb32 = f; f += n;
         P.Ap32 = f; f += n;
-        P.d32 = f;
+        P.d32 = f; f += n;
+        // the compact layout's row table (n + 1 int2), 8-byte aligned; set by ls_member_setup
+        P.ctab = nullptr;
     } else {
         double *d = M.f64;
         P.r64 = d; d += n;
@@ -2066,6 +2116,13 @@ struct PinnedBuf {
 // One lockstep solve of the members `ids` (armed, one precision).  The final states go to out.
 // One member's part of a lockstep launch: its descriptor (FP32 compact, FP32 plain or FP64 layout)
 // and its table entries (r0, r1, w0, w1); maxwin grows to its widest shared-memory window.
+// the compact layout's row table of a member: in its FP32 arena after d32, 8-byte aligned
+static const int2 *ls_ctab(const Member &M, const BProb &desc)
+{
+    const uintptr_t a = reinterpret_cast<uintptr_t>(desc.d32 + M.n);
+    return reinterpret_cast<const int2 *>((a + 7) & ~(uintptr_t)7);
+}
+
 static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb &desc, std::vector<std::array<int, 4>> &E,
                            bool &compact, int &maxwin)
 {
@@ -2074,7 +2131,8 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
     desc = describe(B, id, mx);
     desc.tpr = ls_tpr(M);
     desc.wrow = nullptr;
-    desc.iperm = desc.cptr = nullptr;
+    desc.iperm = nullptr;
+    desc.ctab = nullptr;
     desc.coff = nullptr;
     if (B->ls_windows && (st = ls_windows_of(B, M))) return st;
     E.clear();
@@ -2115,7 +2173,7 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
         femd_pattern P = M.K->pattern;
         desc.tpr = ls_tpr_compact(M);
         desc.iperm = P->cl_iperm.p;
-        desc.cptr = P->cl_indptr.p;
+        desc.ctab = ls_ctab(M, desc);
         desc.coff = P->cl_off.p;
     } else if (B->ls_windows && !M.ls_wrow.empty()) {
         desc.wrow = M.ls_tab.p;
@@ -2132,10 +2190,14 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
     if (mx && (M.need_f32 || M.f32_compact != compact)) {
         cudaStream_t s = ctx->stream;
         const unsigned g = grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count);
-        if (compact)
-            k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, M.K->pattern->cl_dst.p, desc.A32, M.nnz, M.K->inv.p,
-                                                     M.K->pattern->cl_iperm.p, desc.inv32, M.n);
-        else
+        if (compact) {
+            const femd_pattern P = M.K->pattern;
+            k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, P->cl_dst.p, desc.A32, M.nnz, M.K->inv.p, P->cl_iperm.p,
+                                                     desc.inv32, M.n);
+            k_ls_split_rows<<<grid_for((size_t)M.n + 1, 128, 1u << 20), 128, 0, counted(s)>>>(
+                P->indptr.p, P->diag_pos.p, M.K->data.p, P->cl_dst.p, P->cl_iperm.p, P->cl_indptr.p, P->all_diag ? 1 : 0,
+                desc.A32, const_cast<int2 *>(desc.ctab), M.n);
+        } else
             k_batch_f32<<<g, 256, 0, counted(s)>>>(M.K->data.p, desc.A32, M.nnz, M.K->inv.p, desc.inv32, M.n);
         FEMD_TRY_CUDA(cudaGetLastError());
         M.need_f32 = false;
