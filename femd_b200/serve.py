@@ -341,7 +341,10 @@ class Server:
 
 
 def run_plain(lib, sessions, trace, *, tol=1e-10, realtime=True, keep_solutions=False, mixed=False):
-    """The plain FP64 GPU path on the same trace: first come, first served, one cg_solve at a time."""
+    """The plain FP64 GPU path on the same trace: first come, first served, one cg_solve at a time.
+    A Poisson request re-assembles into its (N, k) space's matrix (one per space, kept across
+    requests, as a caller of cg_solve would), so the solver's workspace and captured graphs are
+    reused; a heat step solves with its simulation's resident matrix."""
     torch = _torch()
     for S in sessions:
         S.busy = False
@@ -349,6 +352,7 @@ def run_plain(lib, sessions, trace, *, tol=1e-10, realtime=True, keep_solutions=
         if r.kind == "poisson":
             lib.get(r.N, r.k)
     order = sorted(trace, key=lambda r: r.t)
+    mats = {}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for r in order:
@@ -364,7 +368,7 @@ def run_plain(lib, sessions, trace, *, tol=1e-10, realtime=True, keep_solutions=
                                                  mixed=mixed)
             S.u = x
         else:
-            K = stiffness(lib, r.N, r.k, r.c)
+            K = mats[(r.N, r.k)] = stiffness(lib, r.N, r.k, r.c, into=mats.get((r.N, r.k)))
             b = _rhs(r, K.nrows)
             x, conv, its, res, brk = fb.cg_solve(K, fb.JacobiPreconditioner(K), b, None, max(1000, 10 * K.nrows), tol,
                                                  mixed=mixed)
