@@ -6,6 +6,10 @@
     python -m femd_b200.profile_kernels batch --nmin 150 --nmax 256 --nprob 24 --iters 100 --mixed
     python -m femd_b200.profile_kernels lockstep --nmin 0 --kmin 1 --nprob 16 --iters 0 --reps 1
     python -m femd_b200.profile_kernels lockstep --nmin 0 --kmin 1 --nprob 16 --iters 120 --reps 1 --mixed
+    python -m femd_b200.profile_kernels numbering --n 512 --k 2 --reps 3
+    python -m femd_b200.profile_kernels forms --n 512 --k 2 --reps 3
+    python -m femd_b200.profile_kernels facets --n 512 --k 2 --reps 3
+    python -m femd_b200.profile_kernels precond --n 128 --k 2 --reps 3
 
 Workload: -Lap u + u = f on rectangle_mesh(0, 0, 1, 1, n, n), P_k, zero Dirichlet (the form of
 the config-2 benchmark at another size).  Prints the sizes and a CUDA-event time per launch.
@@ -13,7 +17,9 @@ batch: the problems of the config-4 stream (seed 0) with N in [nmin, nmax] and k
 first nprob of them, solved together by the batched PCG capped at iters iterations; prints the
 launch time and its algorithmic bytes (femd_b200.workloads.batch_bytes).  lockstep: the same
 problems solved by the lockstep engine (iters 0: to convergence); prints the solve time and its
-algorithmic bytes.
+algorithmic bytes.  numbering: the device dof numbering of the space; forms: a coefficient
+program on the cells' points and a P_k field with its derivatives there; facets: the ds matrix and
+load on every exterior facet of the free space; precond: ILU(0) and SSOR built and applied.
 """
 from __future__ import annotations
 
@@ -26,7 +32,7 @@ PI = math.pi
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("kernel", choices=["spmv", "assemble", "assemble_values", "rhs", "cg", "cg_mixed", "pattern", "batch",
-                                       "lockstep"])
+                                       "lockstep", "numbering", "forms", "facets", "precond"])
     ap.add_argument("--n", type=int, default=640)
     ap.add_argument("--k", type=int, default=2)
     ap.add_argument("--reps", type=int, default=3)
@@ -57,6 +63,17 @@ def main():
     s = ctx.stream
     x = torch.ones(V.dim, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
+    extra = {}
+    if a.kernel == "forms":
+        from femd_b200.forms import Integrand, eval_field
+        extra["prog"], extra["eval_field"] = Integrand.varcoef(2 * PI), eval_field
+        extra["c"] = torch.randn(V.dim, dtype=torch.float64, device="cuda")
+    elif a.kernel == "facets":
+        from femd_b200.lift import FacetCache2D, assemble_facet_matrix, assemble_facet_vector
+        Vf = fb.LagrangeSpace2D(m, a.k, bc="free")
+        Kf = fb.CSRMatrix(Vf.pattern())
+        extra.update(F=FacetCache2D(Vf, 2 * a.k), Kf=Kf, mat=assemble_facet_matrix, vec=assemble_facet_vector,
+                     bf=torch.zeros(Vf.dim, dtype=torch.float64, device="cuda"))
 
     def run():
         if a.kernel == "spmv":
@@ -72,6 +89,17 @@ def main():
         elif a.kernel in ("cg", "cg_mixed"):
             M = fb.JacobiPreconditioner(K)
             fb.cg_solve(K, M, b, None, 100000, 1e-10, mixed=a.kernel == "cg_mixed")
+        elif a.kernel == "numbering":
+            fb.LagrangeSpace2D(m, a.k, bc="dirichlet", numbering="device")
+        elif a.kernel == "forms":
+            extra["prog"].evaluate_cells(Qa, [], [1.0, 0.5, 2 * PI])
+            extra["eval_field"](Qa, extra["c"], [0, 1, 2])
+        elif a.kernel == "facets":
+            extra["mat"](extra["F"], [0], [0], [1.0], extra["Kf"])
+            extra["vec"](extra["F"], [0], [fb.Coef.const(1.0)], extra["bf"])
+        elif a.kernel == "precond":
+            for pc in (fb.ILU0Preconditioner(K), fb.SSORPreconditioner(K)):
+                pc.apply(b)
 
     run()
     torch.cuda.synchronize()
