@@ -1579,18 +1579,16 @@ static int grow_arrays(femd_batch_s *B, int cap)
     if ((st = B->d_probs.alloc(cap)) || (st = B->d_bar.alloc(cap)) || (st = B->d_claim.alloc(cap))) return st;
     {
         // members may be part-way through a resumable solve: keep their states
-        BState *ns = nullptr;
-        cudaError_t e = cudaMalloc(&ns, (size_t)cap * sizeof(BState));
-        if (e != cudaSuccess) { cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
+        DevBuf<BState> ns;
+        if ((st = ns.alloc(cap))) return st;
         cudaStream_t s = B->ctx->stream;
-        e = cudaMemsetAsync(ns, 0, (size_t)cap * sizeof(BState), s);
+        cudaError_t e = cudaMemsetAsync(ns.p, 0, (size_t)cap * sizeof(BState), s);
         if (e == cudaSuccess && B->d_state.p)
-            e = cudaMemcpyAsync(ns, B->d_state.p, B->d_state.n * sizeof(BState), cudaMemcpyDeviceToDevice, s);
+            e = cudaMemcpyAsync(ns.p, B->d_state.p, B->d_state.n * sizeof(BState), cudaMemcpyDeviceToDevice, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) { cudaFree(ns); set_error(std::string("batch: ") + cudaGetErrorString(e)); return FEMD_ECUDA; }
-        B->d_state.release();
-        B->d_state.p = ns;
-        B->d_state.n = (size_t)cap;
+        if (e != cudaSuccess) { set_error(std::string("batch: ") + cudaGetErrorString(e)); return FEMD_ECUDA; }
+        std::swap(B->d_state.p, ns.p);
+        std::swap(B->d_state.n, ns.n);
     }
     if (B->pinned) cudaFreeHost(B->pinned);
     B->pinned = nullptr;

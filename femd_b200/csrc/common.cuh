@@ -48,6 +48,13 @@ struct HandleBase {
     virtual ~HandleBase() {}
 };
 
+// Device memory of the library: a stream-ordered pool per device (core.cu). dev_alloc returns
+// memory that any stream may use as soon as it returns; dev_free first waits for the device, as
+// cudaFree does, then hands the block back to the pool, which keeps a bounded amount of freed
+// memory for the next allocation instead of unmapping it.
+cudaError_t dev_alloc(void **p, size_t bytes);
+void dev_free(void *p);
+
 // A device buffer owned by a handle.
 template <class T>
 struct DevBuf {
@@ -57,18 +64,20 @@ struct DevBuf {
     {
         release();
         if (count == 0) return FEMD_OK;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        void *q = nullptr;
+        cudaError_t e = dev_alloc(&q, count * sizeof(T));
         if (e != cudaSuccess) {
-            p = nullptr;
-            set_error(std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " + cudaGetErrorString(e));
+            set_error(std::string("device allocation of ") + std::to_string(count * sizeof(T)) + " bytes: " +
+                      cudaGetErrorString(e));
             return e == cudaErrorMemoryAllocation ? FEMD_ENOMEM : FEMD_ECUDA;
         }
+        p = static_cast<T *>(q);
         n = count;
         return FEMD_OK;
     }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         n = 0;
     }

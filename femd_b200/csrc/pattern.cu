@@ -10,6 +10,7 @@
 //   rc_code    sum of row cell counts  cell * nloc + local index, increasing cell order
 //   indptr     nrows + 1, indices nnz  the pattern (sorted, unique columns per row)
 //   map        ncells x nloc x nloc    position of (dof(e,i), dof(e,j)) in indices, or -1
+#include <algorithm>
 #include <climits>
 #include <string>
 
@@ -58,21 +59,88 @@ __global__ void k_sort_rows(const int *__restrict__ rc_ptr, int *__restrict__ rc
     atomicMax(maxcells, hi - lo);
 }
 
-// ---- K1: per row, gather the columns of its cells, bitonic sort in shared memory, unique ----
+// ---- K1, short rows: one thread per row -----------------------------------------------------
+// Each thread keeps its row's sorted unique columns in shared memory and inserts every candidate
+// column (the dofs of the row's cells, in increasing cell order) at its place, skipping the ones
+// already there. Entry s of thread t sits at s * PT_THREADS + t, so the 32 lanes of a warp hit 32
+// different banks whatever entry each one is at. A row with more than PT_CAP columns is put on a
+// list for the warp-per-row kernel below (counting pass); the filling pass skips it, since its
+// length (from indptr) is then known to be above PT_CAP.
+static constexpr int PT_THREADS = 128;
+static constexpr int PT_CAP = 40;   // P1..P3 rows of a 6-valent mesh have 7, 19, 37 columns
+
+template <bool FILL>
+__global__ void __launch_bounds__(PT_THREADS) k_pattern_rows_t(const int *__restrict__ dofs, int nloc,
+                                                               const int *__restrict__ rc_ptr,
+                                                               const int *__restrict__ rc_code, int nrows,
+                                                               int *__restrict__ rowlen, const int *__restrict__ indptr,
+                                                               int *__restrict__ indices, int *__restrict__ list,
+                                                               int *__restrict__ nlist, int *__restrict__ status)
+{
+    __shared__ int sbuf[PT_CAP * PT_THREADS];
+    int *buf = sbuf + threadIdx.x;
+    // every thread of a block takes the same number of turns, so the warp reduction below has all lanes
+    for (int base = blockIdx.x * PT_THREADS; base < nrows; base += gridDim.x * PT_THREADS) {
+        const int i = base + threadIdx.x;
+        int len = 0;
+        if (i < nrows && !(FILL && indptr[i + 1] - indptr[i] > PT_CAP)) {
+            const int lo = rc_ptr[i], hi = rc_ptr[i + 1];
+            bool over = false;
+            for (int a = lo; a < hi && !over; ++a) {
+                const int *cd = dofs + (size_t)(rc_code[a] / nloc) * nloc;
+                for (int j = 0; j < nloc; ++j) {
+                    const int d = cd[j];
+                    if (d < 0) continue;
+                    int b = len - 1, w = -1;   // b: the last entry <= d
+                    while (b >= 0) {
+                        w = buf[b * PT_THREADS];
+                        if (w <= d) break;
+                        --b;
+                    }
+                    if (b >= 0 && w == d) continue;
+                    if (len == PT_CAP) { over = true; break; }
+                    for (int c = len; c > b + 1; --c) buf[c * PT_THREADS] = buf[(c - 1) * PT_THREADS];
+                    buf[(b + 1) * PT_THREADS] = d;
+                    ++len;
+                }
+            }
+            if (over) {
+                // only the counting pass gets here: the warp kernel counts and later fills this row
+                if (!FILL) list[atomicAdd(nlist, 1)] = i;
+                len = 0;
+            } else if (FILL) {
+                int *out = indices + indptr[i];
+                for (int c = 0; c < len; ++c) out[c] = buf[c * PT_THREADS];
+            } else {
+                rowlen[i] = len;
+            }
+        }
+        if (!FILL) {
+            const int m = __reduce_max_sync(0xffffffffu, len);
+            if ((threadIdx.x & 31) == 0 && m) atomicMax(status + 2, m);
+        }
+    }
+}
+
+// ---- K1, long rows: one warp per listed row, bitonic sort in shared memory, unique ----------
 static constexpr int PAT_WARPS = 4;
 static constexpr int PAT_CAP = 1024;   // candidate columns per row (cells of the row x nloc, padded)
 
 template <bool FILL>
 __global__ void __launch_bounds__(PAT_WARPS * 32) k_pattern_rows(const int *__restrict__ dofs, int nloc,
                                                                   const int *__restrict__ rc_ptr,
-                                                                  const int *__restrict__ rc_code, int nrows,
+                                                                  const int *__restrict__ rc_code,
+                                                                  const int *__restrict__ list,
+                                                                  const int *__restrict__ nlist,
                                                                   int *__restrict__ rowlen, const int *__restrict__ indptr,
                                                                   int *__restrict__ indices, int *__restrict__ status)
 {
     __shared__ int sbuf[PAT_WARPS][PAT_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int *buf = sbuf[w];
-    for (int i = blockIdx.x * PAT_WARPS + w; i < nrows; i += gridDim.x * PAT_WARPS) {
+    const int nl = *nlist;
+    for (int j = blockIdx.x * PAT_WARPS + w; j < nl; j += gridDim.x * PAT_WARPS) {
+        const int i = list[j];
         const int lo = rc_ptr[i], ncell = rc_ptr[i + 1] - lo;
         const int m = ncell * nloc;
         int P = 32;
@@ -230,11 +298,12 @@ int femd_cuda_pattern_from_cells(femd_ctx ctx, int nrows, int ncells, int nloc, 
     DevBuf<int> maxc;
     if ((st = cnt.alloc((size_t)nrows + 1)) || (st = tmp.alloc(scan_tmp_ints((size_t)nrows + 1))) ||
         (st = p->rc_ptr.alloc((size_t)nrows + 1)) || (st = p->indptr.alloc((size_t)nrows + 1)) ||
-        (st = fill.alloc((size_t)nrows + 1)) || (st = rowlen.alloc((size_t)nrows + 1)) || (st = maxc.alloc(2)))
+        (st = fill.alloc((size_t)nrows + 1)) || (st = rowlen.alloc((size_t)nrows + 1)) || (st = maxc.alloc(3)))
         return fail(st);
     if ((st = reset_status(ctx))) return fail(st);
     cudaMemsetAsync(cnt.p, 0, ((size_t)nrows + 1) * sizeof(int), s);
-    cudaMemsetAsync(maxc.p, 0, 2 * sizeof(int), s);   // the most cells of a row, the rows without a diagonal
+    // the most cells of a row, the rows without a diagonal, the rows on the long-row list
+    cudaMemsetAsync(maxc.p, 0, 3 * sizeof(int), s);
     if (tot) k_count_rows<<<grid_for((size_t)tot, 256, 1u << 20), 256, 0, counted(s)>>>(p->cell_dofs.p, tot, nrows, cnt.p, ctx->status_dev);
     if ((st = exclusive_scan_int(cnt.p, p->rc_ptr.p, (size_t)nrows + 1, tmp.p, s))) return fail(st);
     int flags = 0;
@@ -249,12 +318,20 @@ int femd_cuda_pattern_from_cells(femd_ctx ctx, int nrows, int ncells, int nloc, 
     cudaMemcpyAsync(fill.p, p->rc_ptr.p, ((size_t)nrows + 1) * sizeof(int), cudaMemcpyDeviceToDevice, s);
     if (tot) k_fill_rows<<<grid_for((size_t)tot, 256, 1u << 20), 256, 0, counted(s)>>>(p->cell_dofs.p, tot, nrows, nloc, fill.p, p->rc_code.p);
     if (nrows) k_sort_rows<<<grid_for((size_t)nrows, 256), 256, 0, counted(s)>>>(p->rc_ptr.p, p->rc_code.p, nrows, maxc.p);
-    // K1: row lengths, scan, fill
+    // K1: row lengths, scan, fill. Rows of up to PT_CAP columns take a thread each; the longer
+    // ones go on a list (in `fill`, free again by now) that a warp per row takes.
     cudaMemsetAsync(rowlen.p + nrows, 0, sizeof(int), s);
-    const unsigned pgrid = grid_for((size_t)nrows, PAT_WARPS, 1u << 20);
-    if (nrows)
-        k_pattern_rows<false><<<pgrid, PAT_WARPS * 32, 0, counted(s)>>>(p->cell_dofs.p, nloc, p->rc_ptr.p, p->rc_code.p, nrows,
-                                                                rowlen.p, nullptr, nullptr, ctx->status_dev);
+    const unsigned tgrid = grid_for((size_t)nrows, PT_THREADS, 1u << 20);
+    const unsigned lgrid = std::min(grid_for((size_t)nrows, PAT_WARPS, 1u << 20), 1184u);
+    int *const long_rows = fill.p, *const nlong = maxc.p + 2;
+    if (nrows) {
+        k_pattern_rows_t<false><<<tgrid, PT_THREADS, 0, counted(s)>>>(p->cell_dofs.p, nloc, p->rc_ptr.p, p->rc_code.p, nrows,
+                                                                     rowlen.p, nullptr, nullptr, long_rows, nlong,
+                                                                     ctx->status_dev);
+        k_pattern_rows<false><<<lgrid, PAT_WARPS * 32, 0, counted(s)>>>(p->cell_dofs.p, nloc, p->rc_ptr.p, p->rc_code.p,
+                                                                long_rows, nlong, rowlen.p, nullptr, nullptr,
+                                                                ctx->status_dev);
+    }
     if ((st = exclusive_scan_int(rowlen.p, p->indptr.p, (size_t)nrows + 1, tmp.p, s))) return fail(st);
     int nnz = 0;
     e = cudaMemcpyAsync(&ctx->status_host[2], p->indptr.p + nrows, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -271,9 +348,14 @@ int femd_cuda_pattern_from_cells(femd_ctx ctx, int nrows, int ncells, int nloc, 
     }
     p->nnz = nnz;
     if ((st = p->indices.alloc((size_t)nnz + 1))) return fail(st);
-    if (nrows)
-        k_pattern_rows<true><<<pgrid, PAT_WARPS * 32, 0, counted(s)>>>(p->cell_dofs.p, nloc, p->rc_ptr.p, p->rc_code.p, nrows,
-                                                               nullptr, p->indptr.p, p->indices.p, ctx->status_dev);
+    if (nrows) {
+        k_pattern_rows_t<true><<<tgrid, PT_THREADS, 0, counted(s)>>>(p->cell_dofs.p, nloc, p->rc_ptr.p, p->rc_code.p, nrows,
+                                                                    nullptr, p->indptr.p, p->indices.p, nullptr, nullptr,
+                                                                    ctx->status_dev);
+        k_pattern_rows<true><<<lgrid, PAT_WARPS * 32, 0, counted(s)>>>(p->cell_dofs.p, nloc, p->rc_ptr.p, p->rc_code.p,
+                                                               long_rows, nlong, nullptr, p->indptr.p, p->indices.p,
+                                                               ctx->status_dev);
+    }
     if ((st = p->diag_pos.alloc((size_t)nrows + 1))) return fail(st);
     if (nrows)
         k_diag_pos<<<grid_for((size_t)nrows, 256), 256, 0, counted(s)>>>(p->indptr.p, p->indices.p, nrows, nrows, p->diag_pos.p,

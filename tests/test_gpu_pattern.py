@@ -90,3 +90,46 @@ def test_config2_pattern_counts(fb):
     ip, ix = P.to_host()
     ip0, ix0 = O.from_cells(V.dim, V.cell_dofs)
     assert np.array_equal(ip, ip0) and np.array_equal(ix, ix0)
+
+
+def _pattern_of_cells(fb, nrows, dofs_np):
+    import ctypes as C
+    import torch
+    dofs = torch.as_tensor(np.ascontiguousarray(dofs_np, dtype=np.int32)).cuda()
+    h = C.c_void_p()
+    ctx = fb.context()
+    st = fb.lib.femd_cuda_pattern_from_cells(ctx.h, nrows, dofs.shape[0], dofs.shape[1], C.c_void_p(dofs.data_ptr()),
+                                             C.byref(h))
+    assert st == 0, fb.lib.femd_cuda_last_error()
+    P = fb.SparsityPattern(h, ctx)
+    P.ncells, P.nloc = dofs.shape   # what cell_pattern records for scatter_map_2d
+    return P
+
+
+@pytest.mark.parametrize("ncells,nloc,nrows,seed", [(5000, 6, 3000, 1), (20000, 3, 1500, 2), (600, 10, 200, 3),
+                                                    (40, 6, 1000, 4)])
+def test_pattern_of_random_cells(fb, ncells, nloc, nrows, seed):
+    """Random cell maps with constrained (-1) entries: rows from empty to a few hundred columns,
+    so both the thread-per-row path (up to 40 columns) and the warp-per-row path for the longer
+    rows run; pattern, diagonal flag and scatter map against the oracle bit for bit."""
+    rng = np.random.default_rng(seed)
+    dofs = rng.integers(-1, nrows, size=(ncells, nloc)).astype(np.int32)
+    P = _pattern_of_cells(fb, nrows, dofs)
+    ip0, ix0 = O.from_cells(nrows, dofs)
+    ip, ix = P.to_host()
+    assert np.array_equal(ip, ip0) and np.array_equal(ix, ix0)
+    lens = np.diff(ip0)
+    assert lens.max() > 40 or nrows > ncells   # the long-row path ran (the last case: mostly empty rows)
+    assert np.array_equal(fb.scatter_map_2d(P).cpu().numpy(), O.scatter_map(dofs, ip0, ix0))
+
+
+@pytest.mark.parametrize("N,k", [(20, 4), (12, 5)])
+def test_pattern_of_high_degree(fb, N, k):
+    """P4 / P5: the vertex rows (61 / 91 columns on a 6-valent mesh) take the warp-per-row path,
+    the edge and interior rows the thread-per-row path."""
+    m = fb.rectangle_mesh(0, 0, 1, 1, N, N)
+    V = fb.LagrangeSpace2D(m, k, bc="free")
+    ip0, ix0 = O.from_cells(V.dim, V.cell_dofs)
+    ip, ix = V.pattern().to_host()
+    assert np.diff(ip0).max() > 40
+    assert np.array_equal(ip, ip0) and np.array_equal(ix, ix0)
