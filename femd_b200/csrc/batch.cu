@@ -934,97 +934,89 @@ __device__ __forceinline__ void ls_rows(const BProb &P, const V *A, int r0, int 
     }
 }
 
-// y = A p on reordered rows [r0, r1) of the compact layout, the direction p staged in shared
-// memory over the entry's column window [c0, ...): TPR lanes per row, U value / offset loads in
-// flight per lane, the products read p from shared memory (no gathers from global memory).  Each
-// lane adds its entries in increasing position and the row's lanes combine by a fixed shuffle tree.
-// The loop is pipelined: a row group's first round of values and offsets is loaded while the
-// previous group is summed (its row table entries two groups ahead), so a warp keeps two rounds
-// of the matrix stream in flight.  The diagonal is split (k_ls_split_rows): its FP32 high part is
-// the row's diagonal entry, its low part comes with the row's table entry and is added to the
-// FP32 row sum, so the FP32 matrix keeps the FP64 matrix's row sums.
-template <int U, int TPR>
-__device__ __forceinline__ void ls_round_c(const BProb &P, const float *__restrict__ A, int base, int hi, short (&o)[U],
-                                           float (&v)[U])
+// y = A p on reordered rows [r0, r1) of the compact layout (r0 a multiple of 32), the direction
+// p staged in shared memory over the entry's column window [c0, ...). One warp per slice of 32
+// rows, one lane per row: entry j of the lane's row is at its first position + 32 j, so each
+// load of the warp reads 32 consecutive offsets (64 B) and values (128 B), and no lane idles at
+// a row's end (the slice's rows have nearly the same length; the padding entries, offset 0 and
+// value 0, add nothing). The slice's width comes from the next slice's first position. Each lane
+// sums its row in increasing column order. The diagonal is split (k_ls_split_rows): its FP32
+// high part is the row's diagonal entry, its low part comes with the row's table entry and is
+// added last, so the FP32 matrix keeps the FP64 matrix's row sums.
+//
+// The warp is latency-bound (a chain of dependent loads per slice), so: SELL_U entries per round,
+// the next slice's table entries loaded one slice ahead, and the first slice's table entries and
+// first round loaded by sell_prime before the block's window is staged (they do not need it).
+static constexpr int SELL_U = 12;
+struct SellCursor {
+    int base, width, base1, end1;   // this slice's first position and width; the next slice's bounds
+    float dl, dl1;                  // this lane's row's low diagonal part, this slice's and the next's
+    short o[SELL_U];
+    float v[SELL_U];                // the current round of this slice
+};
+
+__device__ __forceinline__ void sell_header(const BProb &P, int s0, int r1, int &base, int &end, float &dl)
 {
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-        const int q = base + u * TPR;
-        o[u] = q < hi ? __ldcs(&P.coff[q]) : (short)0;
-        v[u] = q < hi ? __ldcs(&A[q]) : 0.0f;
+    base = end = 0;
+    dl = 0.0f;
+    if (s0 < r1) {
+        const int i = s0 + (int)(threadIdx.x & 31);
+        base = P.ctab[s0].x;
+        end = P.ctab[min(s0 + 32, P.n)].x;
+        if (i < r1) dl = __int_as_float(P.ctab[i].y);
     }
 }
 
-template <int TPR>
-__device__ __forceinline__ void ls_rows_c(const BProb &P, const float *__restrict__ A, const float *win, int c0, int r0,
-                                          int r1, float *__restrict__ Ap, double &dot)
+__device__ __forceinline__ void sell_round(const BProb &P, const float *__restrict__ A, int base, int width, int j,
+                                           short (&o)[SELL_U], float (&v)[SELL_U])
 {
-    constexpr int U = 4, GPW = 32 / TPR, STEP = (LS_BB / 32) * GPW;
-    const int lane = threadIdx.x % TPR;
-    const int sub = (int)(threadIdx.x & 31) / TPR;
-    int i0 = r0 + (int)(threadIdx.x >> 5) * GPW;
-    int i = i0 + sub;
-    int lo = 0, hi = 0, lo_n = 0, hi_n = 0;
-    float dl = 0.0f, dl_n = 0.0f;                            // the rows' low diagonal parts
-    if (i < r1) {
-        const int2 c = P.ctab[i];
-        lo = c.x;
-        dl = __int_as_float(c.y);
-        hi = P.ctab[i + 1].x;
+    const int q0 = base + (int)(threadIdx.x & 31);
+#pragma unroll
+    for (int u = 0; u < SELL_U; ++u) {
+        const bool in = j + u < width;
+        const int q = q0 + (j + u) * 32;
+        o[u] = in ? __ldcs(&P.coff[q]) : (short)0;
+        v[u] = in ? __ldcs(&A[q]) : 0.0f;
     }
-    if (i + STEP < r1) {
-        const int2 c = P.ctab[i + STEP];
-        lo_n = c.x;
-        dl_n = __int_as_float(c.y);
-        hi_n = P.ctab[i + STEP + 1].x;
-    }
-    short o[U];
-    float v[U];
-    ls_round_c<U, TPR>(P, A, lo + lane, hi, o, v);
-    for (; i0 < r1; i0 += STEP) {
-        const int i2 = i + 2 * STEP;
-        int lo_2 = 0, hi_2 = 0;
-        float dl_2 = 0.0f;
-        if (i2 < r1) {
-            const int2 c = P.ctab[i2];
-            lo_2 = c.x;
-            dl_2 = __int_as_float(c.y);
-            hi_2 = P.ctab[i2 + 1].x;
-        }
-        short on[U];
-        float vn[U];
-        ls_round_c<U, TPR>(P, A, lo_n + lane, hi_n, on, vn);
-        const float *wrow = win + (i - c0);
+}
+
+__device__ __forceinline__ void sell_prime(const BProb &P, const float *__restrict__ A, int r0, int r1, SellCursor &c)
+{
+    const int s0 = r0 + (int)(threadIdx.x >> 5) * 32;
+    int end;
+    sell_header(P, s0, r1, c.base, end, c.dl);
+    c.width = (end - c.base) >> 5;
+    sell_header(P, s0 + LS_BB, r1, c.base1, c.end1, c.dl1);
+    sell_round(P, A, c.base, c.width, 0, c.o, c.v);
+}
+
+__device__ __forceinline__ void ls_rows_sell(const BProb &P, const float *__restrict__ A, const float *win, int c0, int r0,
+                                             int r1, float *__restrict__ Ap, double &dot, SellCursor &c)
+{
+    const int lane = threadIdx.x & 31;
+    for (int s0 = r0 + (int)(threadIdx.x >> 5) * 32; s0 < r1; s0 += LS_BB) {
+        const int i = s0 + lane;
+        const bool ok = i < r1;                                  // lanes past the member's last row: padding
+        const float *wrow = win + (ok ? i - c0 : 0);
         float s = 0.0f;
-        int base = lo + lane;
+        for (int j = 0;; j += SELL_U) {
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-            if (base + u * TPR < hi) s += v[u] * wrow[o[u]];
-        for (base += U * TPR; base < hi; base += U * TPR) {
-            ls_round_c<U, TPR>(P, A, base, hi, o, v);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (base + u * TPR < hi) s += v[u] * wrow[o[u]];
+            for (int u = 0; u < SELL_U; ++u) s += c.v[u] * wrow[c.o[u]];
+            if (j + SELL_U >= c.width) break;
+            sell_round(P, A, c.base, c.width, j + SELL_U, c.o, c.v);
         }
-#pragma unroll
-        for (int k = TPR / 2; k > 0; k >>= 1) s += __shfl_xor_sync(0xffffffffu, s, k, TPR);
-        if (lane == 0 && i < r1) {
-            s = __fmaf_rn(dl, wrow[0], s);                    // the split diagonal's low part
+        if (ok) {
+            s = __fmaf_rn(c.dl, wrow[0], s);                     // the split diagonal's low part
             Ap[i] = s;
             dot += (double)wrow[0] * (double)s;
         }
-        i += STEP;
-        lo = lo_n;
-        hi = hi_n;
-        dl = dl_n;
-        lo_n = lo_2;
-        hi_n = hi_2;
-        dl_n = dl_2;
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            o[u] = on[u];
-            v[u] = vn[u];
-        }
+        // the next slice: its bounds were loaded a slice ago; load its first round and the
+        // bounds of the slice after it
+        c.base = c.base1;
+        c.width = (c.end1 - c.base1) >> 5;
+        c.dl = c.dl1;
+        sell_header(P, s0 + 2 * LS_BB, r1, c.base1, c.end1, c.dl1);
+        if (s0 + LS_BB < r1) sell_round(P, A, c.base, c.width, 0, c.o, c.v);
     }
 }
 
@@ -1148,10 +1140,12 @@ __device__ __forceinline__ void ls_finish(LState &S, int *active)
 }
 
 // SpMV with the direction formed on the fly: p = z + beta pold (pold = 0 at the start); p.Ap.
-// Block 0 also empties the reliable-update list of the iteration.  At most 51 registers: 5
-// blocks per SM (with the loads issued ahead, 60 registers and 4 blocks ran 14 % slower).
+// Block 0 also empties the reliable-update list of the iteration.  Mixed precision: at most 64
+// registers, 4 blocks per SM. The sliced rows' 12 entries per round need them: at 5 blocks (51
+// registers) the rounds spilled and ran 33 % slower than at 4 (64 config-4 problems x 120
+// iterations). FP64: at most 51 registers, 5 blocks per SM.
 template <bool MIXED>
-__global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
+__global__ void __launch_bounds__(LS_BB, MIXED ? 4 : 5) k_ls_spmv(const BProb *__restrict__ probs, const LBlock *__restrict__ blks, int NE,
                                                    LState *st, double *part, int *active, int *ru_count)
 {
     using F = typename std::conditional<MIXED, float, double>::type;
@@ -1182,6 +1176,8 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ 
         const float *zf = (const float *)z, *pf = (const float *)pold;
         float *pn = (float *)pnew;
         const float bf = (float)beta;
+        SellCursor cur;
+        sell_prime(P, (const float *)A, L.r0, L.r1, cur);
         for (int w0 = c0 + (int)threadIdx.x; w0 < c1; w0 += WU * LS_BB) {
             float zv[WU], pv[WU];
 #pragma unroll
@@ -1201,13 +1197,7 @@ __global__ void __launch_bounds__(LS_BB, 5) k_ls_spmv(const BProb *__restrict__ 
             }
         }
         __syncthreads();
-        switch (P.tpr) {
-        case 2: ls_rows_c<2>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
-        case 4: ls_rows_c<4>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
-        case 8: ls_rows_c<8>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
-        case 16: ls_rows_c<16>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
-        default: ls_rows_c<32>(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot); break;
-        }
+        ls_rows_sell(P, (const float *)A, ls_win, c0, L.r0, L.r1, (float *)Ap, dot, cur);
     } else {
         ls_spmv_entry<F, F>(
             P, A, L, [&](int j) { return pdir(z, pold, beta, j); }, [&](int i) { return pdir(z, pold, beta, i); },
@@ -1453,6 +1443,7 @@ struct Member {
     DevBuf<int> tables;                         // crow (nch+1), cq (nch+1)
     DevBuf<double> cpart;                       // per-chunk sums of the SpMV passes (6 x nch)
     float *f32 = nullptr;                       // A32, inv32, r, z, p, p', Ap, d
+    long long a32_cap = 0;                      // room for A32 in f32: nnz, or the sliced layout's size
     double *f64 = nullptr;                      // r, z, p, p', Ap
     const double *b = nullptr;
     double *x = nullptr;
@@ -1675,14 +1666,32 @@ static int add_member(femd_batch_s *B, femd_matrix K, int *id_out)
     return FEMD_OK;
 }
 
-// the member's vectors of one precision (stream-ordered allocation on the first use)
-static int member_vectors(femd_batch_s *B, Member &M, bool mixed)
+static int build_compact(femd_ctx ctx, femd_pattern P);
+
+// the member's vectors of one precision (stream-ordered allocation on the first use). With
+// `sliced` (a mixed lockstep solve that may use the compact layout) the pattern's compact layout
+// is built first and A32 gets room for its padded slices; a smaller arena is replaced (its FP32
+// copy is made again).
+static int member_vectors(femd_batch_s *B, Member &M, bool mixed, bool sliced = false)
 {
     cudaStream_t s = B->ctx->stream;
     const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
+    size_t cap = nnz;
+    if (mixed && sliced) {
+        femd_pattern P = M.K->pattern;
+        int st;
+        if ((st = build_compact(B->ctx, P))) return st;
+        if (P->cl_state == 1) cap = std::max(cap, (size_t)P->cl_nsell);
+    }
+    if (mixed && M.f32 && (size_t)M.a32_cap < cap) {
+        cudaFreeAsync(M.f32, s);
+        M.f32 = nullptr;
+        M.need_f32 = true;
+    }
     if (mixed && !M.f32) {
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (nnz + 9 * n + 40) * sizeof(float), s);
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&M.f32), (cap + 9 * n + 40) * sizeof(float), s);
         if (e != cudaSuccess) { M.f32 = nullptr; cudaGetLastError(); set_error("batch: out of device memory"); return FEMD_ENOMEM; }
+        M.a32_cap = (long long)cap;
         if (reinterpret_cast<uintptr_t>(M.f32) & 15) {
             // the FP32 values are read by 16-byte bulk copies
             cudaFreeAsync(M.f32, s);
@@ -1717,8 +1726,8 @@ static BProb describe(femd_batch_s *B, int id, bool mixed)
     const size_t n = (size_t)M.n, nnz = (size_t)M.nnz;
     if (mixed) {
         float *f = M.f32;
-        P.A32 = f; f += nnz;
-        f = M.f32 + ((nnz + 7) & ~(size_t)7);
+        P.A32 = f;
+        f = M.f32 + (((size_t)M.a32_cap + 7) & ~(size_t)7);
         P.inv32 = f; f += n;
         P.r32 = f; f += n;
         P.z32 = f; f += n;
@@ -1991,17 +2000,6 @@ static int ls_tpr(const Member &M)
     return tpr;
 }
 
-// lanes per row of the compact SpMV (p from shared memory): the fewest whose 8 entries per lane
-// cover the mean row.  Measured on 64 config-4 problems x 120 iterations: 47.4 ms, against 51.2
-// with 4 entries per lane (the plain layout's rule), 49.6 with 16 and 63.2 with one lane per row.
-static int ls_tpr_compact(const Member &M)
-{
-    const double avg = (double)M.nnz / (double)M.n;
-    int tpr = 2;
-    while (tpr * 8 < avg && tpr < 32) tpr <<= 1;
-    return tpr;
-}
-
 // rows of one table entry of a member: about nnz_per_entry nonzeros
 static int ls_rows_per_entry(const femd_batch_s *B, const Member &M)
 {
@@ -2037,7 +2035,8 @@ namespace femd {
 void rcm_order(int n, const std::vector<int> &ip, const std::vector<int> &ix, std::vector<int> &order);
 }
 
-static constexpr int CL_TILE = 32;          // rows per tile of the column-window bounds
+static constexpr int CL_TILE = 32;          // rows per tile of the column-window bounds = rows per SELL slice
+static constexpr int CL_SORT = 256;         // rows per window of the sort by row length
 static constexpr int CL_WIN_MAX = 12288;    // largest column window of an entry (FP32: 48 KB of shared memory)
 
 // Build the pattern's compact layout once (cl_state 1), or mark it unsuitable (-1).
@@ -2053,11 +2052,34 @@ static int build_compact(femd_ctx ctx, femd_pattern P)
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));
     std::vector<int> order;
     rcm_order(n, ip, ix, order);
-    std::vector<int> iperm((size_t)n), cptr((size_t)n + 1, 0), dst((size_t)std::max<long long>(nnz, 1));
-    std::vector<short> off((size_t)std::max<long long>(nnz, 1));
+    // rows by length, longest first, within windows of CL_SORT rows of the RCM order, so that
+    // the 32 rows of a slice have nearly the same length (P2 / P3 rows of a 6-valent mesh have
+    // 7 to 37 entries; unsorted, the slices would be padded by 66 % / 121 %, sorted by 1-5 %)
+    auto rlen = [&](int i) { return ip[i + 1] - ip[i]; };
+    for (int a = 0; a < n; a += CL_SORT)
+        std::stable_sort(order.begin() + a, order.begin() + std::min(n, a + CL_SORT),
+                         [&](int u, int v) { return rlen(u) > rlen(v); });
+    // SELL-32 positions: slice t holds reordered rows 32t .. 32t + 31 column-major (entry j of row
+    // k at cptr[k] + 32 j, cptr[k] = the slice's base + k % 32), each slice as wide as its
+    // longest row; the padding entries have offset 0 and value 0
+    const int nslice = (n + CL_TILE - 1) / CL_TILE;
+    std::vector<int> iperm((size_t)n), cptr((size_t)n + 1, 0);
+    long long nsell = 0;
+    for (int t = 0; t < nslice; ++t) {
+        int w = 0;
+        for (int k = t * CL_TILE; k < std::min(n, (t + 1) * CL_TILE); ++k) w = std::max(w, rlen(order[k]));
+        for (int k = t * CL_TILE; k < std::min(n, (t + 1) * CL_TILE); ++k) cptr[k] = (int)(nsell + (k - t * CL_TILE));
+        nsell += (long long)CL_TILE * w;
+    }
+    if (nsell > INT_MAX - 64) {
+        P->cl_state = -1;
+        return FEMD_OK;
+    }
+    cptr[n] = (int)nsell;
+    std::vector<int> dst((size_t)std::max<long long>(nnz, 1));
+    std::vector<short> off((size_t)std::max<long long>(nsell, 1), (short)0);
     for (int k = 0; k < n; ++k) iperm[order[k]] = k;
-    for (int k = 0; k < n; ++k) cptr[k + 1] = cptr[k] + (ip[order[k] + 1] - ip[order[k]]);
-    const int ntile = (n + CL_TILE - 1) / CL_TILE;
+    const int ntile = nslice;
     std::vector<int> tlo((size_t)ntile, INT_MAX), thi((size_t)ntile, INT_MIN);
     std::vector<std::pair<int, int>> row;
     int bw = 0;
@@ -2074,7 +2096,8 @@ static int build_compact(femd_ctx ctx, femd_pattern P)
             const int d = e.first - k;
             bw = std::max(bw, std::abs(d));
             off[pos] = (short)std::max(-32768, std::min(32767, d));
-            dst[e.second] = pos++;
+            dst[e.second] = pos;
+            pos += CL_TILE;
             lo = std::min(lo, e.first);
             hi = std::max(hi, e.first);
         }
@@ -2086,14 +2109,13 @@ static int build_compact(femd_ctx ctx, femd_pattern P)
     }
     int st;
     if ((st = P->cl_iperm.alloc((size_t)n)) || (st = P->cl_indptr.alloc((size_t)n + 1)) ||
-        (st = P->cl_dst.alloc((size_t)std::max<long long>(nnz, 1))) || (st = P->cl_off.alloc((size_t)std::max<long long>(nnz, 1))))
+        (st = P->cl_dst.alloc((size_t)std::max<long long>(nnz, 1))) || (st = P->cl_off.alloc((size_t)std::max<long long>(nsell, 1))))
         return st;
     FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_iperm.p, iperm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
     FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_indptr.p, cptr.data(), ((size_t)n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
-    if (nnz) {
-        FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_dst.p, dst.data(), (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
-        FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_off.p, off.data(), (size_t)nnz * sizeof(short), cudaMemcpyHostToDevice, s));
-    }
+    if (nnz) FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_dst.p, dst.data(), (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (nsell) FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_off.p, off.data(), (size_t)nsell * sizeof(short), cudaMemcpyHostToDevice, s));
+    P->cl_nsell = nsell;
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // the host vectors are released on return
     P->cl_tile_lo.swap(tlo);
     P->cl_tile_hi.swap(thi);
@@ -2169,7 +2191,6 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
     }
     if (compact) {
         femd_pattern P = M.K->pattern;
-        desc.tpr = ls_tpr_compact(M);
         desc.iperm = P->cl_iperm.p;
         desc.ctab = ls_ctab(M, desc);
         desc.coff = P->cl_off.p;
@@ -2190,6 +2211,8 @@ static int ls_member_setup(femd_ctx ctx, femd_batch_s *B, int id, bool mx, BProb
         const unsigned g = grid_for((size_t)M.nnz, 256, 4 * (unsigned)ctx->sm_count);
         if (compact) {
             const femd_pattern P = M.K->pattern;
+            // the padding entries of the slices stay 0
+            FEMD_TRY_CUDA(cudaMemsetAsync(desc.A32, 0, (size_t)P->cl_nsell * sizeof(float), s));
             k_ls_f32_perm<<<g, 256, 0, counted(s)>>>(M.K->data.p, P->cl_dst.p, desc.A32, M.nnz, M.K->inv.p, P->cl_iperm.p,
                                                      desc.inv32, M.n);
             k_ls_split_rows<<<grid_for((size_t)M.n + 1, 128, 1u << 20), 128, 0, counted(s)>>>(
@@ -2213,7 +2236,7 @@ static int ls_run(femd_ctx ctx, femd_batch_s *B, const std::vector<int> &ids, bo
     out.assign(nm, LState{});
     if (nm == 0) return FEMD_OK;
     for (int id : ids)
-        if ((st = member_vectors(B, *B->mem[id], mx))) return st;
+        if ((st = member_vectors(B, *B->mem[id], mx, B->ls_compact && !B->ls_windows))) return st;
     std::vector<BProb> desc(nm);
     std::vector<std::vector<std::array<int, 4>>> ents(nm);   // per member: r0, r1, w0, w1 of its entries
     std::vector<int> nent(nm);
@@ -2526,7 +2549,7 @@ static int ls_advance(femd_ctx ctx, femd_batch_s *B, bool mx, int chunks, int *n
     for (int id : fresh) {
         Member &M = *B->mem[id];
         const bool m32 = mx && !M.force_fp64;
-        if ((st = member_vectors(B, M, m32))) return st;
+        if ((st = member_vectors(B, M, m32, B->ls_compact && !B->ls_windows))) return st;
         BProb d{};
         bool compact = false;
         if ((st = ls_member_setup(ctx, B, id, m32, d, L.ents[id], compact, L.maxwin))) return st;

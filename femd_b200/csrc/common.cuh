@@ -144,11 +144,14 @@ struct femd_pattern_s : femd::HandleBase {
     // its size (built on the first FAST assembly when every row is shorter than 255)
     femd::DevBuf<unsigned char> pair_off;
     // the batched engine's compact layout of the pattern, built on first use: a reverse
-    // Cuthill-McKee order (iperm: original row -> reordered row), the reordered rows' pointers,
-    // every entry's column as a 16-bit offset from its (reordered) row, and for every original
-    // entry its position in the reordered layout; per tile of 32 reordered rows the smallest and
+    // Cuthill-McKee order with the rows of every 256 sorted by length (iperm: original row ->
+    // reordered row); the entries in slices of 32 reordered rows, column-major within a slice
+    // and padded to its longest row (cl_indptr: each reordered row's first position, entry j at
+    // + 32 j; row n: the total); every entry's column as a 16-bit offset from its (reordered)
+    // row (padding: 0), and for every original entry its position; per slice the smallest and
     // largest column.  cl_state: 0 not built, 1 built, -1 unsuitable (a column offset over 32767)
     int cl_state = 0, cl_bw = 0;
+    long long cl_nsell = 0;            // entries of the sliced layout, padding included
     femd::DevBuf<int> cl_iperm, cl_indptr, cl_dst;
     femd::DevBuf<short> cl_off;
     std::vector<int> cl_tile_lo, cl_tile_hi;
