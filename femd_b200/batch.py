@@ -68,8 +68,10 @@ class Batch:
     def configure_lockstep(self, nnz_per_entry=0, chunk=0, windows=None, compact=None):
         """Shape of the lockstep engine (femd_cuda_batch_lockstep_configure; 0 / None keep a
         value).  windows: SpMV by windows of whole rows (True) or by row groups (False); compact:
-        in mixed precision, the reordered layout with 16-bit column offsets and the direction
-        read from shared memory (True, the default) or the plain layout (False)."""
+        in mixed precision, the reordered layout (SELL-32 slices of length-sorted RCM rows, one
+        lane per row, 16-bit column offsets, the direction read from shared memory; True, the
+        default) or the plain layout (False).  Row groups and windows are the FP64 and plain FP32
+        layouts' SpMV forms."""
         w = -1 if windows is None else int(bool(windows))
         cp = -1 if compact is None else int(bool(compact))
         check(lib.femd_cuda_batch_lockstep_configure(self.h, int(nnz_per_entry), int(chunk), w, cp))
@@ -127,6 +129,26 @@ class Batch:
         self.ctx.leave()
         check(st)
         return self.params(), sec.value
+
+    def tune_lockstep(self, bs, *, candidates=(8192, 16384, 32768, 65536), iters=48, reps=2, mixed=True):
+        """Autotune the lockstep engine's launch shape: the nonzeros per table entry, that is the
+        rows one block of 256 threads takes (8 warps, each a slice of 32 rows in the compact
+        layout). Each candidate runs `iters` iterations of every member on these right-hand
+        sides (on scratch solutions, no member stops early), `reps` times; the fastest device
+        time wins and stays configured. Returns (best, {candidate: seconds})."""
+        if not candidates or iters < 1 or reps < 1:
+            raise ValueError("tune_lockstep: needs candidates, iters >= 1 and reps >= 1")
+        times = {}
+        for c in candidates:
+            self.configure_lockstep(nnz_per_entry=int(c))
+            best = float("inf")
+            for _ in range(reps):
+                _, res = self.solve(bs, None, tol=1e-300, max_iter=int(iters), mixed=mixed, engine="lockstep")
+                best = min(best, max(r["seconds"] for r in res))
+            times[int(c)] = best
+        pick = min(times, key=times.get)
+        self.configure_lockstep(nnz_per_entry=pick)
+        return pick, times
 
     def solve(self, bs, xs=None, *, tol=1e-10, max_iter=0, mixed=True, engine="persistent"):
         """Solve every member (in id order) to completion.  bs: right-hand sides; xs: initial

@@ -139,3 +139,22 @@ def test_pattern_batch_layout(fb, problems):
     R = fb.SparsityPattern.from_arrays(2, 3, np.array([0, 1, 2]), np.array([0, 2]))
     with pytest.raises(ValueError, match="square"):
         R.batch_layout()
+
+
+def test_tune_lockstep(fb, problems):
+    """The lockstep autotuner: each candidate entry size timed on the members, the fastest kept
+    configured, and a solve with it within 1e-8 of the direct solutions."""
+    mats = [K for _, K, _ in problems]
+    bs = [b for _, _, b in problems]
+    B = fb.Batch(mats)
+    best, times = B.tune_lockstep(bs, candidates=(2048, 8192), iters=6, reps=1)
+    assert set(times) == {2048, 8192} and all(t > 0 for t in times.values())
+    assert best in times and times[best] == min(times.values())
+    assert B._ls_shape["nnz_per_entry"] == best
+    xs, res = B.solve(bs, tol=1e-10, mixed=True, engine="lockstep")
+    for (s, K, b), x, r in zip(problems, xs, res):
+        assert r["converged"], (s, r)
+        xd = direct(K, b)
+        assert np.linalg.norm(x.cpu().numpy() - xd) / np.linalg.norm(xd) <= 1e-8, (s, r)
+    with pytest.raises(ValueError):
+        B.tune_lockstep(bs, candidates=())
