@@ -419,11 +419,13 @@ FEMD_API int femd_cuda_batch_advance_lockstep(femd_ctx ctx, femd_batch B, int mi
  * SpMV by windows of whole rows read by coalesced loads (windows = 1) or by row groups of a few
  * lanes per row (0, the default), and in mixed precision the compact layout (compact = 1, the
  * default): each member's FP32 matrix and vectors in a reverse Cuthill-McKee order of its
- * pattern (built once per pattern on the host, kept with the pattern), column indices as 16-bit
- * offsets from the row (6 bytes per nonzero instead of 8), and the SpMV reading the search
- * direction from a shared-memory window of each row range instead of gathering it from global
- * memory; a pattern whose reordered bandwidth exceeds 32767 or whose windows exceed 12288 columns
- * keeps the plain layout.  0 (-1 for windows and compact) keeps the current value.  No reference
+ * pattern with the rows of every 256 sorted by length (built once per pattern on the host, kept
+ * with the pattern), the entries in slices of 32 rows stored column-major and padded to the
+ * slice's longest row (one warp per slice, one lane per row), column indices as 16-bit offsets
+ * from the row (6 bytes per nonzero instead of 8), and the SpMV reading the search direction
+ * from a shared-memory window of each row range instead of gathering it from global memory; a
+ * pattern whose reordered bandwidth exceeds 32767 or whose windows exceed 12288 columns keeps
+ * the plain layout.  0 (-1 for windows and compact) keeps the current value.  No reference
  * counterpart. */
 FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry, int chunk, int windows, int compact);
 /* The last lockstep solve's layout (out: 4 entries): [0] members in the compact layout, [1] members
@@ -431,7 +433,8 @@ FEMD_API int femd_cuda_batch_lockstep_configure(femd_batch B, int nnz_per_entry,
  * Instrumentation with no reference counterpart. */
 FEMD_API int femd_cuda_batch_lockstep_stats(femd_batch B, long long *out);
 /* Build (once per pattern) the lockstep engine's compact layout of a square pattern: the reverse
- * Cuthill-McKee order, 16-bit column offsets, the column window of every 32-row tile.  Mixed-
+ * Cuthill-McKee order with the rows of every 256 sorted by length, the 32-row slices, 16-bit
+ * column offsets, the column window of every slice.  Mixed-
  * precision members on the pattern use it; without this call it is built by the first lockstep
  * solve that meets the pattern (host work, seconds for millions of rows), so a server calls it
  * while it sets its meshes up.  *bandwidth: the reordered bandwidth, -1 when over 32,767 (the
