@@ -131,6 +131,7 @@ SIGNATURES = {
     "femd_host_triangle_quadrature": (_I, [_I, _P, _P, _P]),
     "femd_host_tabulate": (_I, [_I, _I, _P, _P, _P]),
     "femd_host_rcm_order": (_I, [_I, _P, _P, _P]),
+    "femd_host_compact_layout": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "femd_host_lagrange_raw": (_I, [_I, _I, _P, _I, _P, _PI]),
     "femd_host_lagrange_nodes": (_I, [_I, _P, _P]),
     "femd_host_exterior_facets": (_I, [_I, _I, _P, _P, _D, _D, _D, _D, _P, _P, _P, _P]),

@@ -43,6 +43,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "compact_host.h"
 
 namespace femd {
 
@@ -2030,13 +2031,7 @@ static int ls_windows_of(femd_batch_s *B, Member &M)
 
 // ---- the compact layout (lockstep engine, mixed precision) -------------------------------------
 
-// a reverse Cuthill-McKee order of a square host CSR pattern, order[new] = old (setup_host.cpp)
-namespace femd {
-void rcm_order(int n, const std::vector<int> &ip, const std::vector<int> &ix, std::vector<int> &order);
-}
-
-static constexpr int CL_TILE = 32;          // rows per tile of the column-window bounds = rows per SELL slice
-static constexpr int CL_SORT = 256;         // rows per window of the sort by row length
+// (the host part -- order, slices, offsets -- is femd::compact_layout, setup_host.cpp)
 static constexpr int CL_WIN_MAX = 12288;    // largest column window of an entry (FP32: 48 KB of shared memory)
 
 // Build the pattern's compact layout once (cl_state 1), or mark it unsuitable (-1).
@@ -2050,75 +2045,26 @@ static int build_compact(femd_ctx ctx, femd_pattern P)
     FEMD_TRY_CUDA(cudaMemcpyAsync(ip.data(), P->indptr.p, ((size_t)n + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (nnz) FEMD_TRY_CUDA(cudaMemcpyAsync(ix.data(), P->indices.p, (size_t)nnz * sizeof(int), cudaMemcpyDeviceToHost, s));
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));
-    std::vector<int> order;
-    rcm_order(n, ip, ix, order);
-    // rows by length, longest first, within windows of CL_SORT rows of the RCM order, so that
-    // the 32 rows of a slice have nearly the same length (P2 / P3 rows of a 6-valent mesh have
-    // 7 to 37 entries; unsorted, the slices would be padded by 66 % / 121 %, sorted by 1-5 %)
-    auto rlen = [&](int i) { return ip[i + 1] - ip[i]; };
-    for (int a = 0; a < n; a += CL_SORT)
-        std::stable_sort(order.begin() + a, order.begin() + std::min(n, a + CL_SORT),
-                         [&](int u, int v) { return rlen(u) > rlen(v); });
-    // SELL-32 positions: slice t holds reordered rows 32t .. 32t + 31 column-major (entry j of row
-    // k at cptr[k] + 32 j, cptr[k] = the slice's base + k % 32), each slice as wide as its
-    // longest row; the padding entries have offset 0 and value 0
-    const int nslice = (n + CL_TILE - 1) / CL_TILE;
-    std::vector<int> iperm((size_t)n), cptr((size_t)n + 1, 0);
-    long long nsell = 0;
-    for (int t = 0; t < nslice; ++t) {
-        int w = 0;
-        for (int k = t * CL_TILE; k < std::min(n, (t + 1) * CL_TILE); ++k) w = std::max(w, rlen(order[k]));
-        for (int k = t * CL_TILE; k < std::min(n, (t + 1) * CL_TILE); ++k) cptr[k] = (int)(nsell + (k - t * CL_TILE));
-        nsell += (long long)CL_TILE * w;
-    }
-    if (nsell > INT_MAX - 64) {
+    CompactLayout L;
+    compact_layout(n, ip, ix, L);
+    P->cl_bw = L.bw;
+    if (!L.ok) {
         P->cl_state = -1;
         return FEMD_OK;
     }
-    cptr[n] = (int)nsell;
-    std::vector<int> dst((size_t)std::max<long long>(nnz, 1));
-    std::vector<short> off((size_t)std::max<long long>(nsell, 1), (short)0);
-    for (int k = 0; k < n; ++k) iperm[order[k]] = k;
-    const int ntile = nslice;
-    std::vector<int> tlo((size_t)ntile, INT_MAX), thi((size_t)ntile, INT_MIN);
-    std::vector<std::pair<int, int>> row;
-    int bw = 0;
-    for (int k = 0; k < n; ++k) {
-        const int i = order[k];
-        row.clear();
-        for (int q = ip[i]; q < ip[i + 1]; ++q) row.emplace_back(iperm[ix[q]], q);
-        std::sort(row.begin(), row.end());
-        int pos = cptr[k];
-        int &lo = tlo[k / CL_TILE], &hi = thi[k / CL_TILE];
-        lo = std::min(lo, k);
-        hi = std::max(hi, k);
-        for (const auto &e : row) {
-            const int d = e.first - k;
-            bw = std::max(bw, std::abs(d));
-            off[pos] = (short)std::max(-32768, std::min(32767, d));
-            dst[e.second] = pos;
-            pos += CL_TILE;
-            lo = std::min(lo, e.first);
-            hi = std::max(hi, e.first);
-        }
-    }
-    P->cl_bw = bw;
-    if (bw > 32767) {
-        P->cl_state = -1;
-        return FEMD_OK;
-    }
+    const long long nsell = L.nsell;
     int st;
     if ((st = P->cl_iperm.alloc((size_t)n)) || (st = P->cl_indptr.alloc((size_t)n + 1)) ||
         (st = P->cl_dst.alloc((size_t)std::max<long long>(nnz, 1))) || (st = P->cl_off.alloc((size_t)std::max<long long>(nsell, 1))))
         return st;
-    FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_iperm.p, iperm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
-    FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_indptr.p, cptr.data(), ((size_t)n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
-    if (nnz) FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_dst.p, dst.data(), (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
-    if (nsell) FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_off.p, off.data(), (size_t)nsell * sizeof(short), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_iperm.p, L.iperm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
+    FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_indptr.p, L.rstart.data(), ((size_t)n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (nnz) FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_dst.p, L.dst.data(), (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (nsell) FEMD_TRY_CUDA(cudaMemcpyAsync(P->cl_off.p, L.off.data(), (size_t)nsell * sizeof(short), cudaMemcpyHostToDevice, s));
     P->cl_nsell = nsell;
     FEMD_TRY_CUDA(cudaStreamSynchronize(s));   // the host vectors are released on return
-    P->cl_tile_lo.swap(tlo);
-    P->cl_tile_hi.swap(thi);
+    P->cl_tile_lo.swap(L.tlo);
+    P->cl_tile_hi.swap(L.thi);
     P->cl_state = 1;
     return FEMD_OK;
 }

@@ -2,12 +2,15 @@
 // the dof numbering, the quadrature rule and the reference tabulation.  These run once per
 // mesh and degree (the reference runs them on the host too) and feed the device kernels.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
 #include "../../include/femd_cuda.h"
+#include "compact_host.h"
 
 namespace femd {
 void set_error(const std::string &msg);
@@ -87,6 +90,67 @@ void rcm_order(int n, const std::vector<int> &ip, const std::vector<int> &ix, st
         }
     }
     std::reverse(order.begin(), order.end());
+}
+
+
+void compact_layout(int n, const std::vector<int> &ip, const std::vector<int> &ix, CompactLayout &L)
+{
+    L = CompactLayout();
+    std::vector<int> order;
+    rcm_order(n, ip, ix, order);
+    // rows by length, longest first, within windows of CL_SORT rows of the RCM order, so that
+    // the 32 rows of a slice have nearly the same length (P2 / P3 rows of a 6-valent mesh have
+    // 7 to 37 entries; unsorted, the slices would be padded by 66 % / 121 %, sorted by 1-5 %)
+    auto rlen = [&](int i) { return ip[i + 1] - ip[i]; };
+    for (int a = 0; a < n; a += CL_SORT)
+        std::stable_sort(order.begin() + a, order.begin() + std::min(n, a + CL_SORT),
+                         [&](int u, int v) { return rlen(u) > rlen(v); });
+    const int nslice = (n + CL_TILE - 1) / CL_TILE;
+    L.iperm.assign((size_t)n, 0);
+    L.rstart.assign((size_t)n + 1, 0);
+    long long nsell = 0;
+    for (int t = 0; t < nslice; ++t) {
+        const int k0 = t * CL_TILE, k1 = std::min(n, (t + 1) * CL_TILE);
+        int w = 0;
+        for (int k = k0; k < k1; ++k) w = std::max(w, rlen(order[k]));
+        for (int k = k0; k < k1; ++k) L.rstart[k] = (int)std::min<long long>(nsell + (k - k0), INT_MAX);
+        nsell += (long long)CL_TILE * w;
+    }
+    L.nsell = nsell;
+    if (nsell > INT_MAX - 64) {
+        L.bw = -1;
+        return;
+    }
+    L.rstart[n] = (int)nsell;
+    for (int k = 0; k < n; ++k) L.iperm[order[k]] = k;
+    const long long nnz = n ? ip[n] : 0;
+    L.dst.assign((size_t)std::max<long long>(nnz, 1), 0);
+    L.off.assign((size_t)std::max<long long>(nsell, 1), (short)0);
+    L.tlo.assign((size_t)nslice, INT_MAX);
+    L.thi.assign((size_t)nslice, INT_MIN);
+    std::vector<std::pair<int, int>> row;
+    int bw = 0;
+    for (int k = 0; k < n; ++k) {
+        const int i = order[k];
+        row.clear();
+        for (int q = ip[i]; q < ip[i + 1]; ++q) row.emplace_back(L.iperm[ix[q]], q);
+        std::sort(row.begin(), row.end());
+        int pos = L.rstart[k];
+        int &lo = L.tlo[k / CL_TILE], &hi = L.thi[k / CL_TILE];
+        lo = std::min(lo, k);
+        hi = std::max(hi, k);
+        for (const auto &e : row) {
+            const int d = e.first - k;
+            bw = std::max(bw, std::abs(d));
+            L.off[pos] = (short)std::max(-32768, std::min(32767, d));
+            L.dst[e.second] = pos;
+            pos += CL_TILE;
+            lo = std::min(lo, e.first);
+            hi = std::max(hi, e.first);
+        }
+    }
+    L.bw = bw;
+    L.ok = bw <= 32767;
 }
 
 }  // namespace femd
@@ -371,6 +435,38 @@ int femd_host_rcm_order(int n, const int *indptr, const int *indices, int *order
     std::vector<int> ip(indptr, indptr + n + 1), ix(indices, indices + nnz), out;
     femd::rcm_order(n, ip, ix, out);
     std::copy(out.begin(), out.end(), order);
+    return FEMD_OK;
+}
+
+// The lockstep engine's compact layout of a square CSR pattern (femd::compact_layout), what
+// femd_cuda_pattern_batch_layout builds and uploads.  Called with off == NULL it reports the sizes
+// only (*nsell, *bandwidth); with the arrays it fills them.
+int femd_host_compact_layout(int n, const int *indptr, const int *indices, long long *nsell, int *bandwidth, int *iperm,
+                             int *rstart, int *dst, short *off, int *tile_lo, int *tile_hi)
+{
+    femd::clear_error();
+    if (n < 0 || !indptr || !nsell || !bandwidth || (n > 0 && indptr[n] > 0 && !indices)) {
+        set_error("compact_layout: bad arguments");
+        return FEMD_EINVAL;
+    }
+    for (int i = 0; i < n; ++i)
+        if (indptr[i + 1] < indptr[i]) { set_error("compact_layout: indptr is not increasing"); return FEMD_EINVAL; }
+    const long long nnz = n ? indptr[n] : 0;
+    for (long long q = 0; q < nnz; ++q)
+        if (indices[q] < 0 || indices[q] >= n) { set_error("compact_layout: column out of range"); return FEMD_EINVAL; }
+    std::vector<int> ip(indptr, indptr + n + 1), ix(indices, indices + nnz);
+    femd::CompactLayout L;
+    femd::compact_layout(n, ip, ix, L);
+    *nsell = L.nsell;
+    *bandwidth = L.ok ? L.bw : -1;
+    if (!off || !L.ok) return FEMD_OK;
+    if (!iperm || !rstart || (nnz && !dst) || !tile_lo || !tile_hi) { set_error("compact_layout: NULL array"); return FEMD_EINVAL; }
+    std::copy(L.iperm.begin(), L.iperm.end(), iperm);
+    std::copy(L.rstart.begin(), L.rstart.end(), rstart);
+    std::copy(L.dst.begin(), L.dst.begin() + nnz, dst);
+    std::copy(L.off.begin(), L.off.begin() + L.nsell, off);
+    std::copy(L.tlo.begin(), L.tlo.end(), tile_lo);
+    std::copy(L.thi.begin(), L.thi.end(), tile_hi);
     return FEMD_OK;
 }
 

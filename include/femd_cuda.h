@@ -529,6 +529,19 @@ FEMD_API int femd_host_triangle_quadrature(int degree, double *xi, double *eta, 
  * pseudo-peripheral start per connected component, neighbours by increasing degree, reversed) --
  * the order of the batched engine's compact layout.  No reference counterpart. */
 FEMD_API int femd_host_rcm_order(int n, const int *indptr, const int *indices, int *order);
+/* The lockstep engine's compact layout of a square CSR pattern, computed on the host: what
+ * femd_cuda_pattern_batch_layout builds and keeps with a pattern, here for inspection and tests.
+ * The reverse Cuthill-McKee order with the rows of every 256 sorted by length (iperm: original
+ * row -> reordered row); the entries in slices of 32 reordered rows, column-major, each padded to
+ * its longest row: entry j of reordered row k at slot rstart[k] + 32 j (rstart[n] = *nsell, the
+ * slots with padding); off[slot] = the entry's reordered column minus k (0 in the padding);
+ * dst[q] = the slot of entry q; tile_lo / tile_hi = per slice the smallest and largest column,
+ * the slice's own rows included.  With off == NULL only *nsell and *bandwidth are set; else
+ * iperm (n), rstart (n + 1), dst (nnz), off (*nsell), tile_lo and tile_hi ((n + 31) / 32) are
+ * filled.  *bandwidth: the reordered bandwidth, -1 when the layout does not apply (over 32,767);
+ * then nothing is filled.  No reference counterpart. */
+FEMD_API int femd_host_compact_layout(int n, const int *indptr, const int *indices, long long *nsell, int *bandwidth,
+                                      int *iperm, int *rstart, int *dst, short *off, int *tile_lo, int *tile_hi);
 /* The equispaced P_k basis and its reference derivatives at points: out[q][3][nloc]. */
 FEMD_API int femd_host_tabulate(int k, int nq, const double *xi, const double *eta, double *out);
 
