@@ -152,3 +152,34 @@ def test_compact_layout_rejects_bad_input():
     st = lib.femd_host_compact_layout(2, ip.ctypes.data, ix.ctypes.data, C.byref(nsell), C.byref(bw), None, None, None,
                                       None, None, None)
     assert st == 1 and b"out of range" in lib.femd_cuda_last_error()
+
+
+def test_tune_lockstep_picks_the_fastest_candidate():
+    """Batch.tune_lockstep's host logic with the solve stood in for: every candidate configured
+    and timed `reps` times (best of them), the fastest kept configured, ties to the first, and no
+    candidates refused."""
+    from femd_b200.batch import Batch
+    B = object.__new__(Batch)
+    B._ls_shape = dict(nnz_per_entry=16384, chunk=8, spmv="row groups", compact=True)
+    cost = {8192: [3.0, 2.0], 16384: [1.5, 1.0], 32768: [1.0, 1.2], 65536: [4.0, 4.0]}
+    seen, configured = [], []
+
+    def configure_lockstep(nnz_per_entry=0, chunk=0, windows=None, compact=None):
+        configured.append(nnz_per_entry)
+        B._ls_shape["nnz_per_entry"] = nnz_per_entry
+
+    def solve(bs, xs=None, *, tol, max_iter, mixed, engine):
+        c = B._ls_shape["nnz_per_entry"]
+        seen.append((c, max_iter, engine, tol))
+        t = cost[c].pop(0)
+        return None, [{"seconds": t}, {"seconds": t / 2}]
+
+    B.configure_lockstep, B.solve = configure_lockstep, solve
+    best, times = B.tune_lockstep([None], iters=7, reps=2)
+    assert times == {8192: 2.0, 16384: 1.0, 32768: 1.0, 65536: 4.0}
+    assert best == 16384 and configured[-1] == 16384 and B._ls_shape["nnz_per_entry"] == 16384
+    assert len(seen) == 8 and all(m == 7 and e == "lockstep" and tol < 1e-200 for _, m, e, tol in seen)
+    with pytest.raises(ValueError):
+        B.tune_lockstep([None], candidates=())
+    with pytest.raises(ValueError):
+        B.tune_lockstep([None], iters=0)
